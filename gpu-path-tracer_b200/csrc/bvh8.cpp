@@ -1,0 +1,545 @@
+// Host construction of the 8-wide, 8-bit-quantised BVH.
+//
+// Replaces the reference's median-split binary BVH (Core/Source/Graphics/Cuda/Bvh/HostBvh.cpp:22-100)
+// and its DFS flattening to 40-byte nodes (Core/Source/Graphics/Cuda/Bvh/DeviceBvh.cpp:7-52).
+//  1. Binary BVH by binned SAH (16 bins, all three axes), leaves of at most 4 triangles.
+//  2. Collapse to 8-wide: a wide node takes the two binary children of its binary node and keeps
+//     opening the child of largest surface area until it has 8 children.
+//  3. Child slots are assigned by octant (greedy on dot(child centre - node centre, octant
+//     direction)) so a ray visiting slot i ^ octant(ray) goes roughly front to back.
+//  4. Child boxes are padded (1e-5 of their largest extent, plus a relative 1e-7 of their
+//     coordinates) and quantised to 8 bits per axis against the node origin with a power-of-two
+//     scale, rounding outward; every quantised box is checked in exact arithmetic to contain the
+//     padded child box.
+#include "bvh8.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <numeric>
+#include <stdexcept>
+
+namespace pt
+{
+    namespace
+    {
+        struct Box
+        {
+            float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+            float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+            void grow(const Box& b)
+            {
+                for (int k = 0; k < 3; k++)
+                {
+                    lo[k] = std::min(lo[k], b.lo[k]);
+                    hi[k] = std::max(hi[k], b.hi[k]);
+                }
+            }
+            void grow(const float* p)
+            {
+                for (int k = 0; k < 3; k++)
+                {
+                    lo[k] = std::min(lo[k], p[k]);
+                    hi[k] = std::max(hi[k], p[k]);
+                }
+            }
+            float area() const
+            {
+                float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+                if (dx < 0 || dy < 0 || dz < 0) return 0.0f;
+                return 2.0f * (dx * dy + dy * dz + dz * dx);
+            }
+        };
+
+        struct BNode
+        {
+            Box box;
+            uint32_t left = kInvalid, right = kInvalid;
+            uint32_t first = 0, count = 0;
+            bool leaf() const { return left == kInvalid; }
+        };
+
+        constexpr int kBins = 16;
+        constexpr uint32_t kMaxLeaf = 4;
+        constexpr float kTraversalCost = 1.2f;
+
+        struct BinaryBuilder
+        {
+            const float* pos;
+            uint32_t n;
+            std::vector<Box> triBox;
+            std::vector<float> cent;  // 3 per triangle
+            std::vector<uint32_t> idx;
+            std::vector<BNode> nodes;
+            std::atomic<uint32_t> nodeCount{0};
+            std::atomic<int> spawned{0};
+            int maxThreads = 1;
+
+            uint32_t alloc()
+            {
+                uint32_t i = nodeCount.fetch_add(1);
+                if (i >= nodes.size()) throw std::runtime_error("BVH node pool exhausted");
+                return i;
+            }
+
+            uint32_t build(uint32_t first, uint32_t count, int depth)
+            {
+                const uint32_t me = alloc();
+                Box box, cbox;
+                for (uint32_t i = first; i < first + count; i++)
+                {
+                    const uint32_t t = idx[i];
+                    box.grow(triBox[t]);
+                    cbox.grow(&cent[static_cast<size_t>(t) * 3]);
+                }
+                BNode node;
+                node.box = box;
+                node.first = first;
+                node.count = count;
+                if (count <= 1 || depth >= 60)
+                {
+                    nodes[me] = node;
+                    return me;
+                }
+                // binned SAH over the three axes
+                float bestCost = FLT_MAX;
+                int bestAxis = -1, bestBin = -1;
+                const float parentArea = std::max(box.area(), 1e-30f);
+                for (int k = 0; k < 3; k++)
+                {
+                    const float ext = cbox.hi[k] - cbox.lo[k];
+                    if (!(ext > 0.0f)) continue;
+                    uint32_t cnt[kBins] = {};
+                    Box bb[kBins];
+                    const float scale = kBins / ext;
+                    for (uint32_t i = first; i < first + count; i++)
+                    {
+                        const uint32_t t = idx[i];
+                        int b = static_cast<int>((cent[static_cast<size_t>(t) * 3 + k] - cbox.lo[k]) * scale);
+                        b = std::min(std::max(b, 0), kBins - 1);
+                        cnt[b]++;
+                        bb[b].grow(triBox[t]);
+                    }
+                    float areaL[kBins], areaR[kBins];
+                    uint32_t cntL[kBins], cntR[kBins];
+                    Box acc;
+                    uint32_t c = 0;
+                    for (int b = 0; b < kBins; b++)
+                    {
+                        acc.grow(bb[b]);
+                        c += cnt[b];
+                        areaL[b] = acc.area();
+                        cntL[b] = c;
+                    }
+                    acc = Box();
+                    c = 0;
+                    for (int b = kBins - 1; b >= 0; b--)
+                    {
+                        acc.grow(bb[b]);
+                        c += cnt[b];
+                        areaR[b] = acc.area();
+                        cntR[b] = c;
+                    }
+                    for (int b = 0; b < kBins - 1; b++)
+                    {
+                        if (cntL[b] == 0 || cntR[b + 1] == 0) continue;
+                        float cost = kTraversalCost + (areaL[b] * cntL[b] + areaR[b + 1] * cntR[b + 1]) / parentArea;
+                        if (cost < bestCost)
+                        {
+                            bestCost = cost;
+                            bestAxis = k;
+                            bestBin = b;
+                        }
+                    }
+                }
+                if (count <= kMaxLeaf && static_cast<float>(count) <= bestCost)
+                {
+                    nodes[me] = node;
+                    return me;
+                }
+                uint32_t mid;
+                if (bestAxis < 0)
+                {
+                    if (count <= kMaxLeaf)
+                    {
+                        nodes[me] = node;
+                        return me;
+                    }
+                    mid = first + count / 2;  // identical centroids: split the range
+                }
+                else
+                {
+                    const float lo = cbox.lo[bestAxis];
+                    const float scale = kBins / (cbox.hi[bestAxis] - lo);
+                    auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t)
+                    {
+                        int b = static_cast<int>((cent[static_cast<size_t>(t) * 3 + bestAxis] - lo) * scale);
+                        b = std::min(std::max(b, 0), kBins - 1);
+                        return b <= bestBin;
+                    });
+                    mid = static_cast<uint32_t>(it - idx.begin());
+                    if (mid == first || mid == first + count) mid = first + count / 2;
+                }
+                uint32_t l, r;
+                if (count > 65536 && spawned.fetch_add(1) < maxThreads)
+                {
+                    auto fut = std::async(std::launch::async, [&, first, mid, depth]() { return build(first, mid - first, depth + 1); });
+                    r = build(mid, first + count - mid, depth + 1);
+                    l = fut.get();
+                }
+                else
+                {
+                    l = build(first, mid - first, depth + 1);
+                    r = build(mid, first + count - mid, depth + 1);
+                }
+                node.left = l;
+                node.right = r;
+                nodes[me] = node;
+                return me;
+            }
+        };
+
+        struct WideBuilder
+        {
+            const BinaryBuilder& bin;
+            std::vector<Node8> out;
+            uint32_t maxDepth = 0;
+
+            static void padBox(const Box& in, double lo[3], double hi[3])
+            {
+                float ext = 0.0f, mag = 0.0f;
+                for (int k = 0; k < 3; k++)
+                {
+                    ext = std::max(ext, in.hi[k] - in.lo[k]);
+                    mag = std::max(mag, std::max(std::fabs(in.lo[k]), std::fabs(in.hi[k])));
+                }
+                const double pad = 1e-5 * ext + 1e-7 * mag + 1e-30;
+                for (int k = 0; k < 3; k++)
+                {
+                    lo[k] = static_cast<double>(in.lo[k]) - pad;
+                    hi[k] = static_cast<double>(in.hi[k]) + pad;
+                }
+            }
+
+            uint32_t emit(uint32_t bnode, uint32_t depth)
+            {
+                maxDepth = std::max(maxDepth, depth + 1);
+                const uint32_t me = static_cast<uint32_t>(out.size());
+                out.push_back(Node8{});
+                // children list
+                std::vector<uint32_t> kids;
+                const BNode& root = bin.nodes[bnode];
+                if (root.leaf())
+                    kids.push_back(bnode);
+                else
+                {
+                    kids.push_back(root.left);
+                    kids.push_back(root.right);
+                    while (kids.size() < 8)
+                    {
+                        int best = -1;
+                        float bestArea = -1.0f;
+                        for (size_t i = 0; i < kids.size(); i++)
+                        {
+                            const BNode& c = bin.nodes[kids[i]];
+                            if (c.leaf()) continue;
+                            float a = c.box.area();
+                            if (a > bestArea)
+                            {
+                                bestArea = a;
+                                best = static_cast<int>(i);
+                            }
+                        }
+                        if (best < 0) break;
+                        const BNode& c = bin.nodes[kids[best]];
+                        kids[best] = c.left;
+                        kids.push_back(c.right);
+                    }
+                }
+                // slot assignment by octant
+                Box nodeBox;
+                for (uint32_t k : kids) nodeBox.grow(bin.nodes[k].box);
+                float center[3];
+                for (int a = 0; a < 3; a++) center[a] = 0.5f * (nodeBox.lo[a] + nodeBox.hi[a]);
+                int slotOf[8];
+                bool slotUsed[8] = {};
+                bool kidUsed[8] = {};
+                for (size_t round = 0; round < kids.size(); round++)
+                {
+                    float bestScore = -FLT_MAX;
+                    int bk = -1, bs = -1;
+                    for (size_t i = 0; i < kids.size(); i++)
+                    {
+                        if (kidUsed[i]) continue;
+                        const Box& b = bin.nodes[kids[i]].box;
+                        float v[3];
+                        for (int a = 0; a < 3; a++) v[a] = 0.5f * (b.lo[a] + b.hi[a]) - center[a];
+                        for (int s = 0; s < 8; s++)
+                        {
+                            if (slotUsed[s]) continue;
+                            float score = ((s & 1) ? v[0] : -v[0]) + ((s & 2) ? v[1] : -v[1]) + ((s & 4) ? v[2] : -v[2]);
+                            if (score > bestScore)
+                            {
+                                bestScore = score;
+                                bk = static_cast<int>(i);
+                                bs = s;
+                            }
+                        }
+                    }
+                    kidUsed[bk] = true;
+                    slotUsed[bs] = true;
+                    slotOf[bk] = bs;
+                }
+                // child references (recursion first: indices of internal children)
+                uint32_t childRef[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                uint8_t counts[8] = {};
+                uint8_t innerMask = 0, leafMask = 0;
+                for (size_t i = 0; i < kids.size(); i++)
+                {
+                    const BNode& c = bin.nodes[kids[i]];
+                    const int s = slotOf[i];
+                    if (c.leaf())
+                    {
+                        if (c.count > 255) throw std::runtime_error("BVH leaf larger than 255 triangles");
+                        childRef[s] = c.first;
+                        counts[s] = static_cast<uint8_t>(c.count);
+                        leafMask |= static_cast<uint8_t>(1u << s);
+                    }
+                    else
+                    {
+                        childRef[s] = emit(kids[i], depth + 1);
+                        innerMask |= static_cast<uint8_t>(1u << s);
+                    }
+                }
+                // quantisation
+                double clo[8][3], chi[8][3];
+                bool valid[8] = {};
+                double plo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, phi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+                for (size_t i = 0; i < kids.size(); i++)
+                {
+                    const int s = slotOf[i];
+                    padBox(bin.nodes[kids[i]].box, clo[s], chi[s]);
+                    valid[s] = true;
+                    for (int a = 0; a < 3; a++)
+                    {
+                        plo[a] = std::min(plo[a], clo[s][a]);
+                        phi[a] = std::max(phi[a], chi[s][a]);
+                    }
+                }
+                float p[3];
+                int expo[3];
+                uint8_t qlo[3][8], qhi[3][8];
+                for (int a = 0; a < 3; a++)
+                {
+                    // origin rounded down to float
+                    float pf = static_cast<float>(plo[a]);
+                    if (static_cast<double>(pf) > plo[a]) pf = std::nextafter(pf, -FLT_MAX);
+                    p[a] = pf;
+                    const double ext = phi[a] - static_cast<double>(pf);
+                    int e = -126;
+                    if (ext > 0.0)
+                    {
+                        int fe;
+                        std::frexp(ext / 255.0, &fe);  // ext/255 = m * 2^fe, m in [0.5, 1)
+                        e = std::max(-126, std::min(127, fe));
+                    }
+                    for (;;)
+                    {
+                        const double scale = std::ldexp(1.0, e);
+                        bool ok = true;
+                        for (int s = 0; s < 8 && ok; s++)
+                        {
+                            if (!valid[s])
+                            {
+                                qlo[a][s] = 255;
+                                qhi[a][s] = 0;
+                                continue;
+                            }
+                            double ql = std::floor((clo[s][a] - pf) / scale);
+                            double qh = std::ceil((chi[s][a] - pf) / scale);
+                            ql = std::max(0.0, ql);
+                            while (ql > 0 && static_cast<double>(pf) + ql * scale > clo[s][a]) ql -= 1.0;
+                            while (static_cast<double>(pf) + qh * scale < chi[s][a]) qh += 1.0;
+                            if (qh > 255.0 || static_cast<double>(pf) + ql * scale > clo[s][a])
+                            {
+                                ok = false;
+                                break;
+                            }
+                            qlo[a][s] = static_cast<uint8_t>(ql);
+                            qhi[a][s] = static_cast<uint8_t>(qh);
+                        }
+                        if (ok) break;
+                        e++;
+                        if (e > 127) throw std::runtime_error("BVH quantisation exponent overflow");
+                    }
+                    expo[a] = e;
+                }
+                Node8 node{};
+                uint32_t header = static_cast<uint32_t>(expo[0] + 127) | (static_cast<uint32_t>(expo[1] + 127) << 8) |
+                                  (static_cast<uint32_t>(expo[2] + 127) << 16) | (static_cast<uint32_t>(innerMask) << 24);
+                uint32_t pb[3];
+                std::memcpy(pb, p, sizeof(pb));
+                node.w[0] = make_uint4(pb[0], pb[1], pb[2], header);
+                auto pack8 = [](const uint8_t* q, uint32_t& lo, uint32_t& hi)
+                {
+                    lo = static_cast<uint32_t>(q[0]) | (static_cast<uint32_t>(q[1]) << 8) | (static_cast<uint32_t>(q[2]) << 16) | (static_cast<uint32_t>(q[3]) << 24);
+                    hi = static_cast<uint32_t>(q[4]) | (static_cast<uint32_t>(q[5]) << 8) | (static_cast<uint32_t>(q[6]) << 16) | (static_cast<uint32_t>(q[7]) << 24);
+                };
+                uint32_t a0, a1, b0, b1;
+                pack8(qlo[0], a0, a1);
+                pack8(qlo[1], b0, b1);
+                node.w[1] = make_uint4(a0, a1, b0, b1);
+                pack8(qlo[2], a0, a1);
+                pack8(qhi[0], b0, b1);
+                node.w[2] = make_uint4(a0, a1, b0, b1);
+                pack8(qhi[1], a0, a1);
+                pack8(qhi[2], b0, b1);
+                node.w[3] = make_uint4(a0, a1, b0, b1);
+                node.w[4] = make_uint4(childRef[0], childRef[1], childRef[2], childRef[3]);
+                node.w[5] = make_uint4(childRef[4], childRef[5], childRef[6], childRef[7]);
+                pack8(counts, a0, a1);
+                node.w[6] = make_uint4(a0, a1, leafMask, 0);
+                node.w[7] = make_uint4(0, 0, 0, 0);
+                out[me] = node;
+                return me;
+            }
+        };
+    }
+
+    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads)
+    {
+        if (n == 0) throw std::runtime_error("scene has no triangles");
+        BinaryBuilder b;
+        b.pos = positions;
+        b.n = n;
+        b.maxThreads = std::max(1, threads);
+        b.triBox.resize(n);
+        b.cent.resize(static_cast<size_t>(n) * 3);
+        for (uint32_t t = 0; t < n; t++)
+        {
+            Box box;
+            for (int k = 0; k < 3; k++) box.grow(positions + (static_cast<size_t>(t) * 3 + k) * 3);
+            b.triBox[t] = box;
+            for (int a = 0; a < 3; a++) b.cent[static_cast<size_t>(t) * 3 + a] = 0.5f * (box.lo[a] + box.hi[a]);
+        }
+        b.idx.resize(n);
+        std::iota(b.idx.begin(), b.idx.end(), 0u);
+        b.nodes.resize(static_cast<size_t>(n) * 2);
+        const uint32_t root = b.build(0, n, 0);
+        WideBuilder w{b, {}, 0};
+        w.out.reserve(static_cast<size_t>(n) / 3 + 8);
+        if (root != 0) throw std::runtime_error("BVH root index");
+        w.emit(root, 0);
+        Bvh8 result;
+        result.nodes = std::move(w.out);
+        result.depth = w.maxDepth;
+        result.order = b.idx;
+        result.tris.resize(static_cast<size_t>(n) * 3);
+        for (uint32_t j = 0; j < n; j++)
+        {
+            const uint32_t t = b.idx[j];
+            const float* p0 = positions + (static_cast<size_t>(t) * 3 + 0) * 3;
+            const float* p1 = positions + (static_cast<size_t>(t) * 3 + 1) * 3;
+            const float* p2 = positions + (static_cast<size_t>(t) * 3 + 2) * 3;
+            uint32_t ob = t, mb = models[t];
+            float of, mf;
+            std::memcpy(&of, &ob, 4);
+            std::memcpy(&mf, &mb, 4);
+            result.tris[static_cast<size_t>(j) * 3 + 0] = make_float4(p0[0], p0[1], p0[2], of);
+            result.tris[static_cast<size_t>(j) * 3 + 1] = make_float4(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2], mf);
+            result.tris[static_cast<size_t>(j) * 3 + 2] = make_float4(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2], 0.0f);
+        }
+        return result;
+    }
+}
+
+namespace pt
+{
+    namespace
+    {
+        struct CheckState
+        {
+            const Bvh8& b;
+            const float* positions;
+            std::vector<uint32_t> seen;
+            uint64_t violations = 0;
+            uint64_t leafTriangles = 0;
+        };
+
+        // Exact bounds of a subtree; checks each quantised child box against its subtree.
+        void check_node(CheckState& cs, uint32_t node, double lo[3], double hi[3])
+        {
+            const Node8& n = cs.b.nodes[node];
+            float p[3];
+            std::memcpy(p, &n.w[0], 12);
+            const uint32_t header = n.w[0].w;
+            const uint32_t innerMask = header >> 24;
+            const uint32_t leafMask = n.w[6].z & 0xFFu;
+            const uint32_t* child = reinterpret_cast<const uint32_t*>(&n.w[4]);
+            const uint8_t* counts = reinterpret_cast<const uint8_t*>(&n.w[6]);
+            const uint8_t* q = reinterpret_cast<const uint8_t*>(&n.w[1]);  // qlo x,y,z then qhi x,y,z, 8 each
+            for (int k = 0; k < 3; k++)
+            {
+                lo[k] = DBL_MAX;
+                hi[k] = -DBL_MAX;
+            }
+            for (int s = 0; s < 8; s++)
+            {
+                const bool isInner = (innerMask >> s) & 1u, isLeaf = (leafMask >> s) & 1u;
+                if (!isInner && !isLeaf) continue;
+                double clo[3], chi[3];
+                if (isInner)
+                    check_node(cs, child[s], clo, chi);
+                else
+                {
+                    for (int k = 0; k < 3; k++)
+                    {
+                        clo[k] = DBL_MAX;
+                        chi[k] = -DBL_MAX;
+                    }
+                    for (uint32_t j = 0; j < counts[s]; j++)
+                    {
+                        const uint32_t t = cs.b.order[child[s] + j];
+                        cs.seen[t]++;
+                        cs.leafTriangles++;
+                        for (int v = 0; v < 3; v++)
+                            for (int k = 0; k < 3; k++)
+                            {
+                                const double c = cs.positions[(static_cast<size_t>(t) * 3 + v) * 3 + k];
+                                clo[k] = std::min(clo[k], c);
+                                chi[k] = std::max(chi[k], c);
+                            }
+                    }
+                }
+                for (int k = 0; k < 3; k++)
+                {
+                    const int e = static_cast<int>((header >> (8 * k)) & 0xFFu) - 127;
+                    const double scale = std::ldexp(1.0, e);
+                    const double qlo = q[k * 8 + s], qhi = q[24 + k * 8 + s];
+                    const double blo = static_cast<double>(p[k]) + qlo * scale;
+                    const double bhi = static_cast<double>(p[k]) + qhi * scale;
+                    if (!(blo <= clo[k] && bhi >= chi[k])) cs.violations++;
+                    lo[k] = std::min(lo[k], clo[k]);
+                    hi[k] = std::max(hi[k], chi[k]);
+                }
+            }
+        }
+    }
+
+    Bvh8Check CheckBvh8(const Bvh8& b, const float* positions, uint32_t n)
+    {
+        CheckState cs{b, positions, std::vector<uint32_t>(n, 0)};
+        double lo[3], hi[3];
+        check_node(cs, 0, lo, hi);
+        Bvh8Check r;
+        r.containmentViolations = cs.violations;
+        r.leafTriangles = cs.leafTriangles;
+        r.trianglesNotExactlyOnce = 0;
+        for (uint32_t t = 0; t < n; t++)
+            if (cs.seen[t] != 1) r.trianglesNotExactlyOnce++;
+        return r;
+    }
+}

@@ -1,0 +1,30 @@
+// Host construction of the BVH8 (see bvh8.cpp).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "pt_internal.h"
+
+namespace pt
+{
+    struct Bvh8
+    {
+        std::vector<Node8> nodes;
+        std::vector<float4> tris;      // 3 per triangle, leaf order: (v0, orig), (e1, model), (e2, 0)
+        std::vector<uint32_t> order;   // leaf position -> input triangle index
+        uint32_t depth = 0;            // levels of the wide tree
+    };
+
+    // positions: [n][3][3] world positions; models: shading model per triangle.
+    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads);
+
+    struct Bvh8Check
+    {
+        uint64_t containmentViolations;  // quantised child boxes not containing their subtree (exact arithmetic)
+        uint64_t trianglesNotExactlyOnce;
+        uint64_t leafTriangles;
+    };
+
+    // Structural validation of a built BVH8 on the host.
+    Bvh8Check CheckBvh8(const Bvh8& bvh, const float* positions, uint32_t n);
+}

@@ -1,0 +1,1372 @@
+// sm_100a kernels of the wavefront path tracer.
+//
+// Per wavefront iteration (one CUDA-graph body, no host round trip):
+//   trace_kernel<closest>  BVH8 closest hit for the current ray queue -> hit records, per-model queues
+//   shade_kernel<model>    one launch per shading model present (MaterialEval.cu:194-912)
+//   trace_kernel<any>      NEE shadow rays, any hit; unoccluded radiance added to the path slot
+//   regen_kernel           finished paths -> per-sample radiance; new samples -> next ray queue
+//   advance_kernel         one thread: queue bookkeeping, log, loop condition (Renderer.cpp:573-619)
+// All arithmetic that reaches a result uses IEEE operators in the reference's order; the
+// library is compiled with -fmad=false.
+#include <curand_kernel.h>
+
+#include "kernels.h"
+#include "traverse.cuh"
+
+namespace pt
+{
+    // ------------------------------------------------------------------ warp helpers
+    __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+    // Warp-aggregated queue slot reservation: one atomic per converged group of lanes.
+    __device__ __forceinline__ uint32_t agg_push(uint32_t* counter)
+    {
+        const unsigned mask = __activemask();
+        const int leader = __ffs(mask) - 1;
+        const uint32_t lane = lane_id();
+        uint32_t base = 0;
+        if (static_cast<int>(lane) == leader) base = atomicAdd(counter, static_cast<uint32_t>(__popc(mask)));
+        base = __shfl_sync(mask, base, leader);
+        return base + static_cast<uint32_t>(__popc(mask & ((1u << lane) - 1u)));
+    }
+
+    // Same, grouping lanes by key (queue id); counters[key] is the queue's size.
+    __device__ __forceinline__ uint32_t agg_push_keyed(uint32_t* counters, uint32_t key)
+    {
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, key);
+        const int leader = __ffs(peers) - 1;
+        const uint32_t lane = lane_id();
+        uint32_t base = 0;
+        if (static_cast<int>(lane) == leader) base = atomicAdd(&counters[key], static_cast<uint32_t>(__popc(peers)));
+        base = __shfl_sync(peers, base, leader);
+        return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
+    }
+
+    __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+    __device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
+
+    // ------------------------------------------------------------------ traversal
+    struct TraversalState
+    {
+        RayPre ray;
+        HitRecord hit;
+        uint32_t pending;  // node to visit next, kInvalid when the stack decides
+        int sp;
+    };
+
+    // Visit one node or pop the next child group. Returns false when traversal is over.
+    // ANY: stops at the first triangle with tmin <= t < tmax.
+    template <bool ANY>
+    __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, uint32_t* stack, uint32_t stride,
+                                                  int stackCap, bool& occluded, uint32_t* errorFlags)
+    {
+        uint32_t node;
+        if (st.pending != kInvalid)
+        {
+            node = st.pending;
+            st.pending = kInvalid;
+        }
+        else
+        {
+            if (st.sp == 0) return false;
+            uint32_t* top = stack + static_cast<uint32_t>(st.sp - 1) * stride;
+            const uint32_t entry = *top;
+            uint32_t m = entry & 0xFFu;
+            const uint32_t i = static_cast<uint32_t>(__ffs(m) - 1);
+            m &= m - 1u;
+            if (m == 0) st.sp--;
+            else *top = (entry & ~0xFFu) | m;
+            const uint32_t parent = entry >> 8;
+            const uint32_t* childRefs = reinterpret_cast<const uint32_t*>(&sc.nodes[parent].w[4]);
+            node = __ldg(childRefs + (i ^ st.ray.oct));
+        }
+        const uint4* nw = sc.nodes[node].w;
+        const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3), w6 = ldg4(nw + 6);
+        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, w6, st.ray, st.hit.t);
+        const uint32_t innerSlots = hitSlots & (w0.w >> 24);
+        uint32_t leafOrder = permute_mask(hitSlots & w6.z, st.ray.oct);
+        while (leafOrder)
+        {
+            const uint32_t i = static_cast<uint32_t>(__ffs(leafOrder) - 1);
+            leafOrder &= leafOrder - 1u;
+            const uint32_t slot = i ^ st.ray.oct;
+            const uint32_t first = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
+            const uint32_t count = __ldg(reinterpret_cast<const unsigned char*>(&nw[6]) + slot);
+            for (uint32_t k = 0; k < count; k++)
+            {
+                const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
+                const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+                float t, u, v;
+                if (!intersect_triangle(a, b, c, st.ray, t, u, v)) continue;
+                if (ANY)
+                {
+                    if (t >= st.ray.tmin && t < st.hit.t)
+                    {
+                        occluded = true;
+                        return false;
+                    }
+                }
+                else
+                {
+                    const uint32_t orig = __float_as_uint(a.w);
+                    if (better_hit(t, orig, st.ray.tmin, st.hit))
+                    {
+                        st.hit.t = t;
+                        st.hit.tri = orig;
+                        st.hit.u = u;
+                        st.hit.v = v;
+                        st.hit.model = __float_as_uint(b.w);
+                    }
+                }
+            }
+        }
+        if (innerSlots)
+        {
+            if (st.sp >= stackCap)
+            {
+                atomicOr(errorFlags, static_cast<uint32_t>(kErrStackOverflow));
+                return false;
+            }
+            stack[static_cast<uint32_t>(st.sp) * stride] = (node << 8) | permute_mask(innerSlots, st.ray.oct);
+            st.sp++;
+        }
+        return true;
+    }
+
+    // Work sources of the persistent traversal kernel.
+    struct WavefrontClosest
+    {
+        SceneView sc;
+        Wavefront wf;
+        __device__ uint32_t count() const { return wf.ctr->rayCount[wf.ctr->cur]; }
+        __device__ uint32_t* cursor() const { return &wf.ctr->traceCursor; }
+        __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
+        {
+            const uint32_t cur = wf.ctr->cur;
+            const float4 a = wf.rayO[cur][i], b = wf.rayD[cur][i];
+            o = make_float3(a.x, a.y, a.z);
+            d = make_float3(b.x, b.y, b.z);
+            tmin = kMinT;
+            tmax = b.w;
+            tag = __float_as_uint(a.w);
+        }
+        __device__ void finish(uint32_t i, uint32_t slot, const HitRecord& h, bool) const
+        {
+            wf.hit[i] = make_float4(__uint_as_float(h.tri), h.u, h.v, h.t);
+            if (h.tri != kInvalid)
+            {
+                const uint32_t pos = agg_push_keyed(wf.ctr->matCount, h.model);
+                wf.matQ[h.model][pos] = i;
+            }
+            else
+            {
+                const uint32_t pos = agg_push(&wf.ctr->regenCount);
+                wf.regen[pos] = slot;
+            }
+        }
+    };
+
+    // Shadow radiance clamp, Intersect.cu:125-134.
+    __device__ __forceinline__ float3 clamp_radiance(float3 radiance, float maxLength)
+    {
+        const float lengthSquared = dot(radiance, radiance);
+        const float maxLengthSquared = maxLength * maxLength;
+        if (lengthSquared > maxLengthSquared) radiance = radiance * (maxLength * rsqrt_ieee(lengthSquared));
+        return radiance;
+    }
+
+    struct WavefrontShadow
+    {
+        SceneView sc;
+        Wavefront wf;
+        __device__ uint32_t count() const { return wf.ctr->shadowCount; }
+        __device__ uint32_t* cursor() const { return &wf.ctr->shadowCursor; }
+        __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
+        {
+            const float4 a = wf.shO[i], b = wf.shD[i];
+            o = make_float3(a.x, a.y, a.z);
+            d = make_float3(b.x, b.y, b.z);
+            tmin = kMinT;
+            tmax = b.w;
+            tag = __float_as_uint(a.w);
+        }
+        __device__ void finish(uint32_t i, uint32_t slot, const HitRecord&, bool occluded) const
+        {
+            if (occluded) return;
+            const float4 l = wf.shL[i];
+            const float3 add = clamp_radiance(make_float3(l.x, l.y, l.z), 20.0f);
+            float4 acc = wf.slotL[slot];
+            acc.x = acc.x + add.x;
+            acc.y = acc.y + add.y;
+            acc.z = acc.z + add.z;
+            wf.slotL[slot] = acc;
+        }
+    };
+
+    struct BatchRays
+    {
+        SceneView sc;
+        const float* rays;
+        uint32_t n;
+        uint32_t* cursorPtr;
+        uint32_t* triOut;
+        float* uvtOut;
+        uint8_t* occOut;
+        __device__ uint32_t count() const { return n; }
+        __device__ uint32_t* cursor() const { return cursorPtr; }
+        __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
+        {
+            const float* r = rays + static_cast<size_t>(i) * 8;
+            o = make_float3(r[0], r[1], r[2]);
+            d = make_float3(r[3], r[4], r[5]);
+            tmin = r[6];
+            tmax = r[7];
+            tag = i;
+        }
+        __device__ void finish(uint32_t i, uint32_t, const HitRecord& h, bool occluded) const
+        {
+            if (occOut)
+            {
+                occOut[i] = occluded ? 1 : 0;
+                return;
+            }
+            triOut[i] = h.tri;
+            uvtOut[static_cast<size_t>(i) * 3 + 0] = h.tri != kInvalid ? h.u : 0.0f;
+            uvtOut[static_cast<size_t>(i) * 3 + 1] = h.tri != kInvalid ? h.v : 0.0f;
+            uvtOut[static_cast<size_t>(i) * 3 + 2] = h.tri != kInvalid ? h.t : 0.0f;
+        }
+    };
+
+    // Persistent traversal: each warp keeps 32 rays in flight; when at least `refill` lanes are
+    // idle the warp takes that many new rays with one atomic (ballot + popc + shuffle), so lanes
+    // that finished early are refilled instead of idling until the slowest ray of the warp ends.
+    // Traversal stack: STACK entries per thread in shared memory, entry = node << 8 | child mask.
+    template <int STACK, bool ANY, class Work>
+    __global__ void __launch_bounds__(128) trace_kernel(Work work, uint32_t refill, uint32_t* errorFlags)
+    {
+        extern __shared__ uint32_t smem[];
+        uint32_t* stack = smem + threadIdx.x;
+        const uint32_t stride = blockDim.x;
+        const uint32_t n = work.count();
+        const uint32_t lane = lane_id();
+        const unsigned laneMaskLt = (1u << lane) - 1u;
+        TraversalState st;
+        uint32_t index = 0, tag = 0;
+        bool active = false;
+        bool exhausted = false;
+        for (;;)
+        {
+            const unsigned idle = __ballot_sync(0xFFFFFFFFu, !active);
+            if (!exhausted && static_cast<uint32_t>(__popc(idle)) >= refill)
+            {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(work.cursor(), static_cast<uint32_t>(__popc(idle)));
+                base = __shfl_sync(0xFFFFFFFFu, base, 0);
+                if (base >= n) exhausted = true;
+                if (!active)
+                {
+                    const uint32_t i = base + static_cast<uint32_t>(__popc(idle & laneMaskLt));
+                    if (i < n)
+                    {
+                        float3 o, d;
+                        float tmin, tmax;
+                        work.load(i, o, d, tmin, tmax, tag);
+                        index = i;
+                        st.ray = make_ray(o, d, tmin);
+                        st.hit.t = tmax;
+                        st.hit.tri = kInvalid;
+                        st.hit.u = 0.0f;
+                        st.hit.v = 0.0f;
+                        st.hit.model = 0;
+                        st.pending = 0;
+                        st.sp = 0;
+                        active = true;
+                    }
+                }
+            }
+            if (__ballot_sync(0xFFFFFFFFu, active) == 0)
+            {
+                if (exhausted) break;
+                continue;
+            }
+            if (active)
+            {
+                bool occluded = false;
+                bool more = true;
+#pragma unroll 1
+                for (int k = 0; k < 4 && more; k++) more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags);
+                if (!more)
+                {
+                    work.finish(index, tag, st.hit, occluded);
+                    active = false;
+                }
+            }
+        }
+    }
+
+    // ------------------------------------------------------------------ paths
+    __device__ __forceinline__ uint32_t pack_meta(uint32_t depth, bool delta) { return depth | (delta ? 0x100u : 0u); }
+
+    // ComputePathSample + GenerateCameraRay (PathGeneration.cu:15-54).
+    __device__ __forceinline__ void camera_ray(const JobView& job, uint64_t sampleIndex, float2 jitter, float3& o, float3& d)
+    {
+        const uint64_t spp = job.spp;
+        const uint64_t pixelQ = sampleIndex / spp;
+        const uint32_t pixelIndex = static_cast<uint32_t>(pixelQ);
+        const uint32_t sampleGridIndex = static_cast<uint32_t>(sampleIndex - pixelQ * spp);
+        const uint32_t yq = pixelIndex / job.width;
+        const uint32_t x = pixelIndex - yq * job.width;
+        const uint32_t y = yq;
+        const uint32_t sgq = sampleGridIndex / job.spa;
+        const uint32_t sgx = sampleGridIndex - sgq * job.spa;
+        const uint32_t sgy = sgq;
+        const float u = (static_cast<float>(x) + (static_cast<float>(sgx) + jitter.x) / static_cast<float>(job.spa)) / static_cast<float>(job.width);
+        const float v = (static_cast<float>(y) + (static_cast<float>(sgy) + jitter.y) / static_cast<float>(job.spa)) / static_cast<float>(job.height);
+        const float3 origin = make_float3(job.camera[0], job.camera[1], job.camera[2]);
+        const float3 llc = make_float3(job.camera[3], job.camera[4], job.camera[5]);
+        const float3 hor = make_float3(job.camera[6], job.camera[7], job.camera[8]);
+        const float3 ver = make_float3(job.camera[9], job.camera[10], job.camera[11]);
+        d = normalize(llc + u * hor + v * ver - origin);
+        o = origin;
+    }
+
+    // New path for a sample in a slot: Philox stream (seed 1234, subsequence = sample), jitter from
+    // the first uniform4, throughput 1, depth 0, delta flag set (PathGeneration.cu:56-102).
+    __device__ __forceinline__ void start_path(const JobView& job, const Wavefront& wf, uint32_t slot, uint32_t sample,
+                                               uint32_t queue, uint32_t position)
+    {
+        curandStatePhilox4_32_10_t rng;
+        curand_init(kRandomSeed, static_cast<unsigned long long>(sample), 0ull, &rng);
+        const float4 r = curand_uniform4(&rng);
+        float3 o, d;
+        camera_ray(job, sample, make_float2(r.x, r.y), o, d);
+        wf.slotT[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pack_meta(0, true)));
+        wf.slotL[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(4u));
+        wf.slotSample[slot] = sample;
+        wf.rayO[queue][position] = make_float4(o.x, o.y, o.z, __uint_as_float(slot));
+        wf.rayD[queue][position] = make_float4(d.x, d.y, d.z, kMaxT);
+    }
+
+    __global__ void frame_init_kernel(Wavefront wf, const JobView* job, uint32_t pool)
+    {
+        Counters* c = wf.ctr;
+        const uint64_t total = job->totalSamples;
+        const uint32_t gen = static_cast<uint32_t>(total < pool ? total : pool);
+        c->rayCount[0] = gen;
+        c->rayCount[1] = 0;
+        c->cur = 0;
+        for (uint32_t m = 0; m < kModelCount; m++) c->matCount[m] = 0;
+        c->shadowCount = 0;
+        c->regenCount = 0;
+        c->traceCursor = 0;
+        c->shadowCursor = 0;
+        c->iteration = 0;
+        c->done = gen == 0 ? 1u : 0u;
+        c->errorFlags = 0;
+        c->launched = gen;
+        c->raysTraced = 0;
+        c->shadowRaysTraced = 0;
+    }
+
+    __global__ void generate_kernel(Wavefront wf, const JobView* jobPtr)
+    {
+        const JobView job = *jobPtr;
+        const uint32_t n = wf.ctr->rayCount[0];
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+            start_path(job, wf, i, i, 0, i);
+    }
+
+    // ------------------------------------------------------------------ shading (MaterialEval.cu)
+    struct Frame
+    {
+        float3 tangent, bitangent, normal;
+        __device__ float3 to_local(float3 v) const { return make_float3(dot(v, tangent), dot(v, bitangent), dot(v, normal)); }
+        __device__ float3 from_local(float3 v) const { return v.x * tangent + v.y * bitangent + v.z * normal; }
+    };
+
+    __device__ __forceinline__ float3 safe_normalize(float3 v, float3 fallback)
+    {
+        const float l2 = dot(v, v);
+        if (l2 > 1e-16f) return v * rsqrt_ieee(l2);
+        return fallback;
+    }
+
+    __device__ __forceinline__ Frame frame_from_normal(float3 n)  // Math.hpp:120-134
+    {
+        float3 t;
+        if (fabsf(n.x) > fabsf(n.z)) t = normalize(make_float3(n.y, -n.x, 0.0f));
+        else t = normalize(make_float3(0.0f, n.z, -n.y));
+        return Frame{t, cross(n, t), n};
+    }
+
+    __device__ __forceinline__ Frame frame_from(float3 n, float3 t, float sign)  // Math.hpp:136-148
+    {
+        n = safe_normalize(n, make_float3(0.0f, 0.0f, 1.0f));
+        t = t - n * dot(n, t);
+        const float l2 = dot(t, t);
+        if (l2 > 1e-16f) t = t * rsqrt_ieee(l2);
+        else t = frame_from_normal(n).tangent;
+        return Frame{t, cross(n, t) * sign, n};
+    }
+
+    struct Surface
+    {
+        float3 position, gN, normal;
+        float4 tangent;
+        uint32_t material;
+    };
+
+    // LoadResolvedHit (MaterialEval.cu:54-87), without the uv (constant materials).
+    __device__ __forceinline__ Surface resolve_hit(const SceneView& sc, float3 o, float3 d, float tHit, uint32_t tri, float u, float v)
+    {
+        const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
+        const float b0 = 1.0f - u - v;
+        const float b1 = u;
+        const float b2 = v;
+        Surface s;
+        s.position = o + d * tHit;
+        const float4 g = ldg4(rec + 6);
+        float3 gn = make_float3(g.x, g.y, g.z);
+        if (dot(gn, d) > 0.0f) gn = -gn;
+        s.gN = gn;
+        s.material = __float_as_uint(g.w);
+        const float4 n0 = ldg4(rec + 0), n1 = ldg4(rec + 1), n2 = ldg4(rec + 2);
+        s.normal = b0 * f3(n0) + b1 * f3(n1) + b2 * f3(n2);
+        const float4 t0 = ldg4(rec + 3), t1 = ldg4(rec + 4), t2 = ldg4(rec + 5);
+        s.tangent = b0 * t0 + b1 * t1 + b2 * t2;
+        return s;
+    }
+
+    __device__ __forceinline__ float3 mat3(const float* v) { return make_float3(__ldg(v), __ldg(v + 1), __ldg(v + 2)); }
+
+    // GetShadingFrame (MaterialEval.cu:89-115) with a constant normal-map texel.
+    __device__ __forceinline__ Frame shading_frame(const Surface& s, const MaterialDev& m)
+    {
+        const float3 bt = make_float3(s.tangent.x, s.tangent.y, s.tangent.z);
+        const float sign = s.tangent.w < 0.0f ? -1.0f : 1.0f;
+        const Frame base = frame_from(s.normal, bt, sign);
+        const float3 ts = normalize(mat3(m.normal) * 2.0f - 1.0f);
+        const float3 sn = ts.x * base.tangent + ts.y * base.bitangent + ts.z * base.normal;
+        return frame_from(sn, bt, sign);
+    }
+
+    __device__ __forceinline__ float luminance(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
+
+    struct Continuation
+    {
+        bool terminated;
+        uint32_t depth;
+        float3 throughput;
+    };
+
+    // ComputePathContinuation (MaterialEval.cu:129-146).
+    __device__ __forceinline__ Continuation continue_path(uint32_t depth, float3 T, uint32_t limit, float3 w, float rr)
+    {
+        const uint32_t next = depth + 1;
+        if (next >= limit) return {true, next, f3(0.0f)};
+        const float3 nt = T * w;
+        if (next < kRussianRouletteStartDepth) return {false, next, nt};
+        const float p = clampf(max3(nt), 0.0f, 1.0f);
+        if (rr > p) return {true, next, f3(0.0f)};
+        return {false, next, nt / p};
+    }
+
+    __device__ __forceinline__ float3 cosine_hemisphere(float2 u)  // :222-229
+    {
+        const float phi = 2.0f * kPi * u.x;
+        const float cosTheta = sqrtf(u.y);
+        const float sinTheta = sqrtf(1.0f - u.y);
+        float s, c;
+        sincos_det(phi, &s, &c);
+        return make_float3(sinTheta * c, sinTheta * s, cosTheta);
+    }
+
+    struct LightHit
+    {
+        float3 position, gN, wi, emission;
+        float distanceSquared, pdf;
+    };
+
+    // SampleLightTriangle (MaterialEval.cu:171-192) with the alias table (AliasTableView.hpp:32-60).
+    __device__ __forceinline__ LightHit sample_light(const SceneView& sc, float uSel, float2 xi, float3 hitPoint)
+    {
+        const uint32_t n = sc.lightCount;
+        const float scaledU = uSel * static_cast<float>(n);
+        uint32_t bin = static_cast<uint32_t>(scaledU);
+        bin = bin < n - 1u ? bin : n - 1u;
+        const float up = fminf(scaledU - static_cast<float>(bin), kOneMinusEpsilon);
+        const uint4 b = ldg4(sc.bins + bin);
+        uint32_t index = bin;
+        float pmf = __uint_as_float(b.y);
+        if (!(up < __uint_as_float(b.x)))
+        {
+            index = b.z;
+            pmf = __uint_as_float(__ldg(&sc.bins[index].y));
+        }
+        const float4* L = sc.lights + static_cast<size_t>(index) * 5;
+        const float4 l0 = ldg4(L), l1 = ldg4(L + 1), l2 = ldg4(L + 2), l3 = ldg4(L + 3), l4 = ldg4(L + 4);
+        const float s0 = sqrtf(xi.x);
+        const float b1 = s0 * (1.0f - xi.y);
+        const float b2 = s0 * xi.y;
+        LightHit h;
+        h.position = f3(l0) + b1 * f3(l1) + b2 * f3(l2);
+        const float3 toLight = h.position - hitPoint;
+        h.distanceSquared = dot(toLight, toLight);
+        h.wi = normalize(toLight);
+        float3 gn = f3(l3);
+        if (dot(gn, h.wi) > 0.0f) gn = -gn;
+        h.gN = gn;
+        h.emission = f3(l4);
+        h.pdf = pmf / l1.w;
+        return h;
+    }
+
+    struct ShadowOut
+    {
+        bool valid;
+        float3 origin, direction, radiance;
+        float tMax;
+    };
+
+    __device__ __forceinline__ ShadowOut shadow_ray(float3 hitPosition, float3 gN, const LightHit& lh, float3 radiance)  // :261-267
+    {
+        ShadowOut s;
+        s.valid = true;
+        s.origin = hitPosition + gN * 1e-4f;
+        const float3 v = lh.position - s.origin;
+        const float dist = length(v);
+        s.direction = v / dist;
+        s.tMax = dist - 1e-4f;
+        s.radiance = radiance;
+        return s;
+    }
+
+    // Lambert NEE, EvaluateDiffuseDirect (:231-268); Phong NEE adds the lobe (:410-455).
+    __device__ __forceinline__ ShadowOut direct_lambert_phong(const SceneView& sc, float3 T, float3 dir, const Surface& s, const Frame& f,
+                                                              float3 rs, float3 albedo, bool phong, float3 specular, float shininess)
+    {
+        ShadowOut none;
+        none.valid = false;
+        const LightHit lh = sample_light(sc, rs.x, make_float2(rs.y, rs.z), s.position);
+        if (lh.distanceSquared < 1e-6f) return none;
+        const float cosThetaI = fmaxf(dot(f.normal, lh.wi), 0.0f);
+        const float gCos = fmaxf(dot(s.gN, lh.wi), 0.0f);
+        if (cosThetaI <= 0.0f || gCos <= 0.0f) return none;
+        const float cosThetaLight = fmaxf(dot(lh.gN, f3(0.0f) - lh.wi), 0.0f);
+        if (cosThetaLight <= 0.0f) return none;
+        float3 brdf;
+        if (phong)
+        {
+            const float3 refl = normalize(reflect(dir, f.normal));
+            const float cosThetaR = fmaxf(dot(refl, lh.wi), 0.0f);
+            const float3 diffuseBrdf = albedo / kPi;
+            const float3 specularBrdf = specular * (shininess + 2.0f) * kInvTwoPi * pow_det(cosThetaR, shininess);
+            brdf = diffuseBrdf + specularBrdf;
+        }
+        else
+            brdf = albedo / kPi;
+        const float geometryTerm = cosThetaI * cosThetaLight / lh.distanceSquared;
+        const float3 radiance = lh.emission * T * brdf * geometryTerm / lh.pdf;
+        return shadow_ray(s.position, s.gN, lh, radiance);
+    }
+
+    // GGX helpers (MaterialEval.cu:587-650) and Math.hpp:217-262.
+    __device__ __forceinline__ float cos2_theta(float3 w) { return w.z * w.z; }
+    __device__ __forceinline__ float sin2_theta(float3 w) { return fmaxf(0.0f, 1.0f - cos2_theta(w)); }
+    __device__ __forceinline__ float sin_theta(float3 w) { return sqrtf(sin2_theta(w)); }
+    __device__ __forceinline__ float tan2_theta(float3 w) { return sin2_theta(w) / cos2_theta(w); }
+    __device__ __forceinline__ float cos_phi(float3 w)
+    {
+        const float st = sin_theta(w);
+        return (st == 0) ? 1 : clampf(w.x / st, -1.f, 1.f);
+    }
+    __device__ __forceinline__ float sin_phi(float3 w)
+    {
+        const float st = sin_theta(w);
+        return (st == 0) ? 0 : clampf(w.y / st, -1.f, 1.f);
+    }
+    __device__ __forceinline__ float ggx_lambda(float3 w, float alpha)
+    {
+        const float t2 = tan2_theta(w);
+        if (t2 == INFINITY) return 0.0f;
+        const float a2 = sqr(cos_phi(w) * alpha) + sqr(sin_phi(w) * alpha);
+        return (sqrtf(1.0f + a2 * t2) - 1.0f) * 0.5f;
+    }
+    __device__ __forceinline__ float ggx_g1(float3 w, float alpha) { return 1.0f / (1.0f + ggx_lambda(w, alpha)); }
+    __device__ __forceinline__ float ggx_g(float3 wo, float3 wi, float alpha) { return 1 / (1 + ggx_lambda(wo, alpha) + ggx_lambda(wi, alpha)); }
+    __device__ __forceinline__ float ggx_d(float3 wm, float alpha)
+    {
+        const float t2 = tan2_theta(wm);
+        if (t2 == INFINITY) return 0.0f;
+        const float cos4 = sqr(cos2_theta(wm));
+        if (cos4 < 1e-16f) return 0.0f;
+        const float e = t2 * (sqr(cos_phi(wm) / alpha) + sqr(sin_phi(wm) / alpha));
+        return 1 / (kPi * sqr(alpha) * cos4 * sqr(1 + e));
+    }
+    __device__ __forceinline__ float ggx_dv(float3 w, float3 wm, float alpha)
+    {
+        return ggx_g1(w, alpha) / fabsf(w.z) * ggx_d(wm, alpha) * fabsf(dot(w, wm));
+    }
+    __device__ __forceinline__ float3 fresnel_schlick(float3 f0, float c) { return f0 + (1.0f - f0) * pow5_det(1.0f - c); }
+
+    __device__ __forceinline__ float3 trowbridge_sample(float3 w, float alpha, float2 u)
+    {
+        float3 wh = normalize(make_float3(alpha * w.x, alpha * w.y, w.z));
+        if (wh.z < 0) wh = -wh;
+        const float3 t = (wh.z < 0.999f) ? normalize(cross(wh, make_float3(0.0f, 0.0f, 1.0f))) : make_float3(1.0f, 0.0f, 0.0f);
+        const float3 b = cross(wh, t);
+        const float r = sqrtf(u.x);
+        const float theta = 2.0f * kPi * u.y;
+        float sn, cs;
+        sincos_det(theta, &sn, &cs);
+        float2 disk = make_float2(r * cs, r * sn);
+        const float h = sqrtf(1.0f - disk.x * disk.x);
+        disk.y = lerpf(h, disk.y, (1 + wh.z) * 0.5f);
+        const float pz = sqrtf(fmaxf(0.0f, 1.0f - dot(disk, disk)));
+        const float3 nh = disk.x * t + disk.y * b + pz * wh;
+        return normalize(make_float3(alpha * nh.x, alpha * nh.y, fmaxf(1e-6f, nh.z)));
+    }
+
+    // EvaluateGgxDirect (:652-718)
+    __device__ __forceinline__ ShadowOut direct_ggx(const SceneView& sc, float3 T, float3 dir, const Surface& s, const Frame& f, float3 rs,
+                                                    float3 base, float alpha, float metallic, float ior)
+    {
+        ShadowOut none;
+        none.valid = false;
+        const LightHit lh = sample_light(sc, rs.x, make_float2(rs.y, rs.z), s.position);
+        if (lh.distanceSquared < 1e-6f || lh.pdf <= 0.0f) return none;
+        if (dot(s.gN, lh.wi) <= 0.0f) return none;
+        const float cosThetaLight = fmaxf(dot(lh.gN, f3(0.0f) - lh.wi), 0.0f);
+        if (cosThetaLight <= 0.0f) return none;
+        const float3 wo = f.to_local(f3(0.0f) - dir);
+        const float3 wi = f.to_local(lh.wi);
+        const float cosThetaI = wi.z;
+        const float cosThetaO = wo.z;
+        if (cosThetaI <= 0.0f || cosThetaO <= 0.0f) return none;
+        const float3 wm = normalize(wo + wi);
+        if (wm.z <= 0.0f) return none;
+        const float woDotWm = dot(wo, wm);
+        const float wiDotWm = dot(wi, wm);
+        if (woDotWm <= 1e-6f || wiDotWm <= 1e-6f) return none;
+        const float dielectricF0 = sqr((1.0f - ior) / (1.0f + ior));
+        const float3 f0 = lerp3(f3(dielectricF0), base, metallic);
+        const float3 diffuseColor = base * (1.0f - metallic);
+        const float3 F = fresnel_schlick(f0, clampf(woDotWm, 0.0f, 1.0f));
+        const float3 diffuseBsdf = (1.0f - F) * diffuseColor * kInvPi;
+        const float3 ggxBsdf = F * ggx_d(wm, alpha) * ggx_g(wo, wi, alpha) / (4.0f * cosThetaI * cosThetaO);
+        const float3 bsdf = diffuseBsdf + ggxBsdf;
+        const float geometryTerm = cosThetaI * cosThetaLight / lh.distanceSquared;
+        const float3 radiance = lh.emission * T * bsdf * geometryTerm / lh.pdf;
+        return shadow_ray(s.position, s.gN, lh, radiance);
+    }
+
+    struct Scatter
+    {
+        bool terminated;
+        Continuation c;
+        float3 direction;
+    };
+
+    __device__ __forceinline__ Scatter scatter_terminated()
+    {
+        Scatter s;
+        s.terminated = true;
+        return s;
+    }
+
+    // EvaluateGgxIndirect (:720-836)
+    __device__ __forceinline__ Scatter indirect_ggx(uint32_t depth, float3 T, uint32_t limit, float3 dir, const Surface& s, const Frame& f,
+                                                    float4 rs, float3 base, float alpha, float metallic, float ior)
+    {
+        const float3 wo = f.to_local(f3(0.0f) - dir);
+        if (wo.z <= 0.0f) return scatter_terminated();
+        const float dielectricF0 = sqr((1.0f - ior) / (1.0f + ior));
+        const float3 f0 = lerp3(f3(dielectricF0), base, metallic);
+        const float3 diffuseColor = base * (1.0f - metallic);
+        const float dw = luminance(diffuseColor);
+        const float sw = luminance(f0);
+        const float ws = dw + sw;
+        if (ws <= 1e-6f) return scatter_terminated();
+        const float dsp = dw / ws;
+        const float ssp = sw / ws;
+        float3 wi;
+        if (rs.z < dsp) wi = cosine_hemisphere(make_float2(rs.x, rs.y));
+        else wi = reflect(-wo, trowbridge_sample(wo, alpha, make_float2(rs.x, rs.y)));
+        const float cosThetaI = wi.z;
+        const float cosThetaO = wo.z;
+        if (cosThetaI <= 0.0f) return scatter_terminated();
+        const float3 wm = normalize(wi + wo);
+        if (wm.z <= 0.0f) return scatter_terminated();
+        const float woDotWm = dot(wo, wm);
+        if (woDotWm <= 1e-6f) return scatter_terminated();
+        const float3 F = fresnel_schlick(f0, clampf(woDotWm, 0.0f, 1.0f));
+        const float3 diffuseBsdf = (1.0f - F) * diffuseColor * kInvPi;
+        const float3 ggxBsdf = F * ggx_d(wm, alpha) * ggx_g(wo, wi, alpha) / (4.0f * cosThetaI * cosThetaO);
+        const float diffusePdf = cosThetaI * kInvPi;
+        const float ggxPdf = ggx_dv(wo, wm, alpha) / (4.0f * woDotWm);
+        const float pdf = dsp * diffusePdf + ssp * ggxPdf;
+        if (pdf <= 1e-8f) return scatter_terminated();
+        const float3 worldWi = f.from_local(wi);
+        if (dot(worldWi, s.gN) <= 0.0f) return scatter_terminated();
+        Scatter out;
+        out.c = continue_path(depth, T, limit, (diffuseBsdf + ggxBsdf) * (cosThetaI / pdf), rs.w);
+        out.terminated = out.c.terminated;
+        out.direction = worldWi;
+        return out;
+    }
+
+    // EvaluatePhongIndirect (:457-542)
+    __device__ __forceinline__ Scatter indirect_phong(uint32_t depth, float3 T, uint32_t limit, float3 dir, const Surface& s, const Frame& f,
+                                                      float4 rs, float3 albedo, float3 specular, float shininess)
+    {
+        const float dw = luminance(albedo);
+        const float sw = luminance(specular);
+        const float ws = dw + sw;
+        if (ws <= 0.0f) return scatter_terminated();
+        const float dsp = dw / ws;
+        const float ssp = 1.0f - dsp;
+        const float3 refl = normalize(reflect(dir, f.normal));
+        float3 wi;
+        if (rs.z < dsp)
+            wi = f.from_local(cosine_hemisphere(make_float2(rs.x, rs.y)));
+        else
+        {
+            const float phi = 2.0f * kPi * rs.x;
+            const float cosTheta = pow_det(rs.y, 1.0f / (shininess + 1.0f));
+            const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
+            float sn, cs;
+            sincos_det(phi, &sn, &cs);
+            wi = frame_from_normal(refl).from_local(make_float3(sinTheta * cs, sinTheta * sn, cosTheta));
+        }
+        const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
+        const float gCos = fmaxf(dot(s.gN, wi), 0.0f);
+        if (cosThetaI <= 0.0f || gCos <= 0.0f) return scatter_terminated();
+        const float cosThetaR = fmaxf(dot(refl, wi), 0.0f);
+        const float lobe = kInvTwoPi * pow_det(cosThetaR, shininess);
+        const float diffusePdf = cosThetaI * kInvPi;
+        const float specularPdf = (shininess + 1.0f) * lobe;
+        const float pdf = dsp * diffusePdf + ssp * specularPdf;
+        if (pdf <= 0.0f) return scatter_terminated();
+        const float3 diffuseBrdf = albedo * kInvPi;
+        const float3 specularBrdf = specular * (shininess + 2.0f) * lobe;
+        Scatter out;
+        out.c = continue_path(depth, T, limit, (diffuseBrdf + specularBrdf) * (cosThetaI / pdf), rs.w);
+        out.terminated = out.c.terminated;
+        out.direction = wi;
+        return out;
+    }
+
+    // One kernel per shading model; grid-stride over the model's queue.
+    template <uint32_t MODEL>
+    __global__ void __launch_bounds__(128) shade_kernel(SceneView sc, Wavefront wf, const JobView* jobPtr)
+    {
+        Counters* ctr = wf.ctr;
+        const uint32_t n = ctr->matCount[MODEL];
+        const uint32_t cur = ctr->cur;
+        const uint32_t nxt = cur ^ 1u;
+        const uint32_t limit = jobPtr->depthLimit;
+        const bool nee = jobPtr->nee != 0;
+        const uint32_t* queue = wf.matQ[MODEL];
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        {
+            const uint32_t r = queue[k];
+            const float4 o4 = wf.rayO[cur][r];
+            const float4 d4 = wf.rayD[cur][r];
+            const float4 h4 = wf.hit[r];
+            const uint32_t slot = __float_as_uint(o4.w);
+            const float3 o = f3(o4), d = f3(d4);
+            const float tHit = h4.w;
+            const uint32_t tri = __float_as_uint(h4.x);
+            const float4 T4 = wf.slotT[slot];
+            float4 L4 = wf.slotL[slot];
+            const uint32_t meta = __float_as_uint(T4.w);
+            const uint32_t depth = meta & 0xFFu;
+            const bool delta = (meta & 0x100u) != 0;
+            const float3 T = f3(T4);
+            uint32_t rngPos = __float_as_uint(L4.w);
+            bool terminated = true;
+            float3 nextDir = f3(0.0f);
+            float3 nextGn = f3(0.0f);
+            Continuation cont{true, 0, f3(0.0f)};
+            bool nextDelta = false;
+            ShadowOut sh;
+            sh.valid = false;
+            float3 hitPos = f3(0.0f);
+
+            if (MODEL == 5)  // Emissive (:882-912)
+            {
+                if (!(nee && !delta))
+                {
+                    const uint32_t mat = __float_as_uint(__ldg(&sc.shading[static_cast<size_t>(tri) * 9 + 6].w));
+                    const float3 em = mat3(sc.materials[mat].emission);
+                    const float3 c = T * em;
+                    L4.x = L4.x + c.x;
+                    L4.y = L4.y + c.y;
+                    L4.z = L4.z + c.z;
+                }
+            }
+            else if (MODEL == 0)  // Normal (:194-220)
+            {
+                const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
+                const float3 c = T * s.normal * 0.5f + 0.5f;
+                L4.x = L4.x + c.x;
+                L4.y = L4.y + c.y;
+                L4.z = L4.z + c.z;
+            }
+            else
+            {
+                const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
+                hitPos = s.position;
+                nextGn = s.gN;
+                const MaterialDev& m = sc.materials[s.material];
+                const Frame f = shading_frame(s, m);
+                curandStatePhilox4_32_10_t rng;
+                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]), static_cast<unsigned long long>(rngPos), &rng);
+                if (MODEL == 1)  // Diffuse (:311-350, :270-309)
+                {
+                    const float3 albedo = mat3(m.color);
+                    const float4 ind = curand_uniform4(&rng);
+                    rngPos += 4;
+                    if (nee)
+                    {
+                        const float4 dir4 = curand_uniform4(&rng);
+                        rngPos += 4;
+                        sh = direct_lambert_phong(sc, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
+                    }
+                    const float3 wi = f.from_local(cosine_hemisphere(make_float2(ind.x, ind.y)));
+                    const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
+                    const float gCos = fmaxf(dot(s.gN, wi), 0.0f);
+                    if (!(cosThetaI <= 0.0f || gCos <= 0.0f))
+                    {
+                        cont = continue_path(depth, T, limit, albedo, ind.z);
+                        terminated = cont.terminated;
+                        nextDir = wi;
+                        nextDelta = false;
+                    }
+                }
+                else if (MODEL == 2)  // Mirror (:352-392)
+                {
+                    const float3 reflectance = mat3(m.specular);
+                    const float rr = curand_uniform(&rng);
+                    rngPos += 1;
+                    const float3 wi = reflect(d, f.normal);
+                    cont = continue_path(depth, T, limit, reflectance, rr);
+                    terminated = cont.terminated;
+                    nextDir = wi;
+                    nextDelta = true;
+                }
+                else if (MODEL == 3)  // Phong (:544-585)
+                {
+                    const float3 albedo = mat3(m.color);
+                    const float3 specular = mat3(m.specular);
+                    const float shininess = __ldg(&m.shininess) * (1000.0f - 1.0f) + 1.0f;
+                    const float4 ind = curand_uniform4(&rng);
+                    rngPos += 4;
+                    if (nee) sh = direct_lambert_phong(sc, T, d, s, f, f3(ind), albedo, true, specular, shininess);
+                    const Scatter sc2 = indirect_phong(depth, T, limit, d, s, f, ind, albedo, specular, shininess);
+                    terminated = sc2.terminated;
+                    cont = sc2.c;
+                    nextDir = sc2.direction;
+                    nextDelta = false;
+                }
+                else if (MODEL == 4)  // GGX (:838-880)
+                {
+                    const float3 base = mat3(m.color);
+                    const float3 rma = mat3(m.rma);
+                    const float alpha = fmaxf(rma.x * rma.x, 0.001f);
+                    const float metallic = rma.y;
+                    const float ior = __ldg(&m.ior);
+                    const float4 ind = curand_uniform4(&rng);
+                    rngPos += 4;
+                    if (nee)
+                    {
+                        const float4 dir4 = curand_uniform4(&rng);
+                        rngPos += 4;
+                        sh = direct_ggx(sc, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
+                    }
+                    const Scatter sc2 = indirect_ggx(depth, T, limit, d, s, f, ind, base, alpha, metallic, ior);
+                    terminated = sc2.terminated;
+                    cont = sc2.c;
+                    nextDir = sc2.direction;
+                    nextDelta = false;
+                }
+            }
+            L4.w = __uint_as_float(rngPos);
+            wf.slotL[slot] = L4;
+            if (sh.valid)
+            {
+                const uint32_t pos = agg_push(&ctr->shadowCount);
+                wf.shO[pos] = make_float4(sh.origin.x, sh.origin.y, sh.origin.z, __uint_as_float(slot));
+                wf.shD[pos] = make_float4(sh.direction.x, sh.direction.y, sh.direction.z, sh.tMax);
+                wf.shL[pos] = make_float4(sh.radiance.x, sh.radiance.y, sh.radiance.z, 0.0f);
+            }
+            if (terminated)
+            {
+                const uint32_t pos = agg_push(&ctr->regenCount);
+                wf.regen[pos] = slot;
+            }
+            else
+            {
+                // SpawnScatteredRay (:148-156)
+                const float3 origin = o + d * tHit + nextGn * 1e-4f;
+                wf.slotT[slot] = make_float4(cont.throughput.x, cont.throughput.y, cont.throughput.z,
+                                             __uint_as_float(pack_meta(cont.depth, nextDelta)));
+                const uint32_t pos = agg_push(&ctr->rayCount[nxt]);
+                wf.rayO[nxt][pos] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(slot));
+                wf.rayD[nxt][pos] = make_float4(nextDir.x, nextDir.y, nextDir.z, kMaxT);
+            }
+            (void)hitPos;
+        }
+    }
+
+    // Finished paths write their radiance to the per-sample buffer; the first
+    // min(terminated, remaining) slots start new samples behind the extension rays
+    // (RegeneratePathsKernel, PathGeneration.cu:78-102).
+    __global__ void regen_kernel(Wavefront wf, const JobView* jobPtr)
+    {
+        Counters* ctr = wf.ctr;
+        const uint32_t n = ctr->regenCount;
+        const unsigned long long launched = ctr->launched;
+        const unsigned long long total = jobPtr->totalSamples;
+        const unsigned long long remaining = total - launched;
+        const uint32_t regenerate = static_cast<uint32_t>(remaining < n ? remaining : n);
+        const uint32_t nxt = ctr->cur ^ 1u;
+        const uint32_t base = ctr->rayCount[nxt];
+        float* out = jobPtr->sampleRadiance;
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        {
+            const uint32_t slot = wf.regen[k];
+            const float4 L = wf.slotL[slot];
+            const uint32_t sample = wf.slotSample[slot];
+            float* dst = out + static_cast<size_t>(sample) * 3;
+            dst[0] = L.x;
+            dst[1] = L.y;
+            dst[2] = L.z;
+            if (k < regenerate)
+                start_path(*jobPtr, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
+        }
+    }
+
+    __global__ void advance_kernel(Wavefront wf, const JobView* jobPtr, cudaGraphConditionalHandle handle)
+    {
+        Counters* c = wf.ctr;
+        const uint32_t cur = c->cur;
+        const uint32_t nxt = cur ^ 1u;
+        const unsigned long long remaining = jobPtr->totalSamples - c->launched;
+        const uint32_t regenerate = static_cast<uint32_t>(remaining < c->regenCount ? remaining : c->regenCount);
+        const uint32_t next = c->rayCount[nxt] + regenerate;
+        if (c->iteration < wf.logCapacity)
+        {
+            uint32_t* row = wf.queueLog + static_cast<size_t>(c->iteration) * kQueueLogColumns;
+            row[0] = c->rayCount[cur];
+            for (uint32_t m = 0; m < kModelCount; m++) row[1 + m] = c->matCount[m];
+            row[7] = c->shadowCount;
+            row[8] = c->regenCount;
+        }
+        c->raysTraced += c->rayCount[cur];
+        c->shadowRaysTraced += c->shadowCount;
+        c->launched += regenerate;
+        c->rayCount[cur] = 0;
+        c->rayCount[nxt] = next;
+        c->cur = nxt;
+        for (uint32_t m = 0; m < kModelCount; m++) c->matCount[m] = 0;
+        c->shadowCount = 0;
+        c->regenCount = 0;
+        c->traceCursor = 0;
+        c->shadowCursor = 0;
+        c->iteration += 1;
+        const bool cancelled = wf.cancel != nullptr && *wf.cancel != 0u;
+        c->done = (next == 0 || cancelled) ? 1u : 0u;
+        if (wf.progress != nullptr)
+        {
+            wf.progress[0] = c->launched;
+            wf.progress[1] = c->iteration;
+        }
+        cudaGraphSetConditional(handle, c->done ? 0u : 1u);
+    }
+
+    // Per pixel: compensated (Kahan) FP32 sum of its samples in sample order, then
+    // PostprocessKernel's tonemap (Image.cu:22-54): x/spp, Reinhard, x^(1/2.2), u8 truncation.
+    __global__ void resolve_kernel(const JobView* jobPtr, float4* accumulation, uint32_t* framebuffer)
+    {
+        const JobView job = *jobPtr;
+        const uint32_t pixels = job.width * job.height;
+        const float invSpp = 1.0f / static_cast<float>(job.spp);
+        for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += gridDim.x * blockDim.x)
+        {
+            float acc[3];
+            const uint64_t first = static_cast<uint64_t>(p) * job.spp;
+            for (int ch = 0; ch < 3; ch++)
+            {
+                float sum = 0.0f, comp = 0.0f;
+                for (uint32_t k = 0; k < job.spp; k++)
+                {
+                    const uint64_t si = first + k;
+                    if (si >= job.totalSamples) break;
+                    const float y = job.sampleRadiance[si * 3 + ch] - comp;
+                    const float t = sum + y;
+                    comp = (t - sum) - y;
+                    sum = t;
+                }
+                acc[ch] = sum;
+            }
+            accumulation[p] = make_float4(acc[0], acc[1], acc[2], 0.0f);
+            uint32_t rgb[3];
+            for (int ch = 0; ch < 3; ch++)
+            {
+                const float hdr = acc[ch] * invSpp;
+                const float ldr = hdr / (hdr + 1.0f);
+                const float g = pow_det(ldr, 1.0f / 2.2f);
+                rgb[ch] = static_cast<uint32_t>(static_cast<unsigned char>(clampf(g * 255.0f, 0.0f, 255.0f)));
+            }
+            framebuffer[p] = rgb[0] | (rgb[1] << 8) | (rgb[2] << 16) | (255u << 24);
+        }
+    }
+
+    __global__ void clear_kernel(uint32_t* framebuffer, uint32_t n, uint32_t value)  // ClearKernel (Image.cu:7-13)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) framebuffer[i] = value;
+    }
+
+    // ------------------------------------------------------------------ scene: lights and alias table on the device
+    // LightSampler::BuildSync (LightSampler.cpp:5-40): emissive triangles in input order.
+    __global__ void light_flag_kernel(const float4* shading, const MaterialDev* materials, uint32_t n, uint32_t* flags)
+    {
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        {
+            const uint32_t mat = __float_as_uint(shading[static_cast<size_t>(t) * 9 + 6].w);
+            flags[t] = materials[mat].model == kModelEmissive ? 1u : 0u;
+        }
+    }
+
+    __global__ void light_record_kernel(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+                                        const uint32_t* flags, const uint32_t* index, float4* lights, double* weights)
+    {
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        {
+            if (!flags[t]) continue;
+            const float* p = positions + static_cast<size_t>(t) * 9;
+            const float3 p0 = make_float3(p[0], p[1], p[2]);
+            const float3 e1 = make_float3(p[3], p[4], p[5]) - p0;
+            const float3 e2 = make_float3(p[6], p[7], p[8]) - p0;
+            const float area = 0.5f * length(cross(e1, e2));
+            const float4 g = shading[static_cast<size_t>(t) * 9 + 6];
+            const uint32_t mat = __float_as_uint(g.w);
+            const uint32_t li = index[t];
+            float4* L = lights + static_cast<size_t>(li) * 5;
+            L[0] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(t));
+            L[1] = make_float4(e1.x, e1.y, e1.z, area);
+            L[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
+            L[3] = make_float4(g.x, g.y, g.z, 0.0f);
+            L[4] = make_float4(materials[mat].emission[0], materials[mat].emission[1], materials[mat].emission[2], 0.0f);
+            weights[li] = static_cast<double>(area);
+        }
+    }
+
+    // Triangle records of the shading pass (Renderer.cpp:159-213): normals, tangents, geometric
+    // normal normalize(cross(e1, e2)), material, uvs; 144 bytes per triangle.
+    __global__ void shading_record_kernel(const float* positions, const float* normals, const float* tangents, const float* uvs,
+                                          const uint32_t* materialIds, uint32_t n, float4* shading)
+    {
+        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        {
+            const float* p = positions + static_cast<size_t>(t) * 9;
+            const float* nn = normals + static_cast<size_t>(t) * 9;
+            const float* tt = tangents + static_cast<size_t>(t) * 12;
+            const float* uu = uvs + static_cast<size_t>(t) * 6;
+            const float3 p0 = make_float3(p[0], p[1], p[2]);
+            const float3 e1 = make_float3(p[3], p[4], p[5]) - p0;
+            const float3 e2 = make_float3(p[6], p[7], p[8]) - p0;
+            const float3 gn = normalize(cross(e1, e2));
+            float4* S = shading + static_cast<size_t>(t) * 9;
+            S[0] = make_float4(nn[0], nn[1], nn[2], 0.0f);
+            S[1] = make_float4(nn[3], nn[4], nn[5], 0.0f);
+            S[2] = make_float4(nn[6], nn[7], nn[8], 0.0f);
+            S[3] = make_float4(tt[0], tt[1], tt[2], tt[3]);
+            S[4] = make_float4(tt[4], tt[5], tt[6], tt[7]);
+            S[5] = make_float4(tt[8], tt[9], tt[10], tt[11]);
+            S[6] = make_float4(gn.x, gn.y, gn.z, __uint_as_float(materialIds[t]));
+            S[7] = make_float4(uu[0], uu[1], uu[2], uu[3]);
+            S[8] = make_float4(uu[4], uu[5], 0.0f, 0.0f);
+        }
+    }
+
+    // Exclusive scan, one block of 1024 threads per 1024 elements; block totals out.
+    template <typename T>
+    __global__ void scan_block_kernel(const T* in, T* out, T* blockSums, uint32_t n)
+    {
+        __shared__ T warpSums[32];
+        const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+        const T x = i < n ? in[i] : T(0);
+        T v = x;
+        const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const T y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+            if (lane >= static_cast<uint32_t>(o)) v = v + y;
+        }
+        if (lane == 31) warpSums[warp] = v;
+        __syncthreads();
+        if (warp == 0)
+        {
+            T w = warpSums[lane];
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const T y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= static_cast<uint32_t>(o)) w = w + y;
+            }
+            warpSums[lane] = w;
+        }
+        __syncthreads();
+        const T warpOffset = warp > 0 ? warpSums[warp - 1] : T(0);
+        const T inclusive = v + warpOffset;
+        if (i < n) out[i] = inclusive - x;
+        if (threadIdx.x == 1023u && blockSums) blockSums[blockIdx.x] = inclusive;
+    }
+
+    template <typename T>
+    __global__ void scan_add_kernel(T* data, const T* blockOffsets, uint32_t n)
+    {
+        const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
+        if (i < n && blockIdx.x > 0) data[i] = data[i] + blockOffsets[blockIdx.x];
+    }
+
+    __global__ void scan_total_kernel(const uint32_t* flags, const uint32_t* excl, uint32_t n, uint32_t* total)
+    {
+        *total = n ? excl[n - 1] + flags[n - 1] : 0u;
+    }
+
+    // AliasTable<uint32_t>::BuildSync (AliasTable.hpp:22-84): p_i = w_i / sum (sum accumulated in
+    // FP64 by the device prefix sum, rounded to float), pHat = p * n, then the reference's
+    // sequential pairing of the last light (under) and last heavy (over) outcome. The pairing is
+    // inherently ordered, so one thread runs it; under/over stacks live in the scratch arrays.
+    __global__ void alias_build_kernel(const double* weights, const double* prefix, uint32_t n, uint4* bins,
+                                       uint32_t* stackIndex, float* stackValue)
+    {
+        if (blockIdx.x != 0 || threadIdx.x != 0 || n == 0) return;
+        const float sum = static_cast<float>(prefix[n - 1] + weights[n - 1]);
+        uint32_t* underIdx = stackIndex;
+        uint32_t* overIdx = stackIndex + n;
+        float* underVal = stackValue;
+        float* overVal = stackValue + n;
+        uint32_t nu = 0, no = 0;
+        for (uint32_t i = 0; i < n; i++)
+        {
+            const float p = static_cast<float>(weights[i]) / sum;
+            bins[i] = make_uint4(__float_as_uint(0.0f), __float_as_uint(p), 0u, i);
+            const float pHat = p * static_cast<float>(n);
+            if (pHat < 1)
+            {
+                underIdx[nu] = i;
+                underVal[nu] = pHat;
+                nu++;
+            }
+            else
+            {
+                overIdx[no] = i;
+                overVal[no] = pHat;
+                no++;
+            }
+        }
+        while (nu > 0 && no > 0)
+        {
+            nu--;
+            no--;
+            const uint32_t ui = underIdx[nu], oi = overIdx[no];
+            const float uv = underVal[nu], ov = overVal[no];
+            bins[ui].x = __float_as_uint(uv);
+            bins[ui].z = oi;
+            const float excess = uv + ov - 1;
+            if (excess < 1)
+            {
+                underIdx[nu] = oi;
+                underVal[nu] = excess;
+                nu++;
+            }
+            else
+            {
+                overIdx[no] = oi;
+                overVal[no] = excess;
+                no++;
+            }
+        }
+        while (no > 0)
+        {
+            no--;
+            bins[overIdx[no]].x = __float_as_uint(1.0f);
+            bins[overIdx[no]].z = kInvalid;
+        }
+        while (nu > 0)
+        {
+            nu--;
+            bins[underIdx[nu]].x = __float_as_uint(1.0f);
+            bins[underIdx[nu]].z = kInvalid;
+        }
+    }
+
+    // ------------------------------------------------------------------ host launchers
+    namespace
+    {
+        template <int STACK, bool ANY, class Work>
+        cudaError_t launch_trace_t(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
+        {
+            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
+            trace_kernel<STACK, ANY, Work><<<blocks, threads, smem, s>>>(w, refill, err);
+            return cudaGetLastError();
+        }
+
+        template <bool ANY, class Work>
+        cudaError_t launch_trace(const Work& w, uint32_t depth, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
+        {
+            if (depth <= 8) return launch_trace_t<8, ANY>(w, blocks, threads, refill, err, s);
+            if (depth <= 16) return launch_trace_t<16, ANY>(w, blocks, threads, refill, err, s);
+            if (depth <= 32) return launch_trace_t<32, ANY>(w, blocks, threads, refill, err, s);
+            return launch_trace_t<64, ANY>(w, blocks, threads, refill, err, s);
+        }
+    }
+
+    int trace_grid_blocks(int device, int threads, uint32_t depth)
+    {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        int perSm = 0;
+        const int stack = depth <= 8 ? 8 : depth <= 16 ? 16 : depth <= 32 ? 32 : 64;
+        const size_t smem = static_cast<size_t>(stack) * threads * sizeof(uint32_t);
+        if (depth <= 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<8, false, WavefrontClosest>, threads, smem);
+        else if (depth <= 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<16, false, WavefrontClosest>, threads, smem);
+        else if (depth <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<32, false, WavefrontClosest>, threads, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<64, false, WavefrontClosest>, threads, smem);
+        if (perSm < 1) perSm = 1;
+        return sms * perSm;
+    }
+
+    cudaError_t launch_iteration(const IterationLaunch& L, cudaStream_t s)
+    {
+        cudaError_t e;
+        WavefrontClosest wc{L.scene, L.wf};
+        e = launch_trace<false>(wc, L.scene.depth, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+        if (e != cudaSuccess) return e;
+        for (uint32_t m = 0; m < kModelCount; m++)
+        {
+            if (!L.modelPresent[m]) continue;
+            switch (m)
+            {
+                case 0: shade_kernel<0><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+                case 1: shade_kernel<1><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+                case 2: shade_kernel<2><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+                case 3: shade_kernel<3><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+                case 4: shade_kernel<4><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+                default: shade_kernel<5><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
+            }
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        if (L.nee && L.scene.lightCount > 0)
+        {
+            WavefrontShadow ws{L.scene, L.wf};
+            e = launch_trace<true>(ws, L.scene.depth, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            if (e != cudaSuccess) return e;
+        }
+        regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        advance_kernel<<<1, 1, 0, s>>>(L.wf, L.job, L.handle);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_frame_prologue(const Wavefront& wf, const JobView* job, uint32_t pool, int blocks, cudaStream_t s)
+    {
+        frame_init_kernel<<<1, 1, 0, s>>>(wf, job, pool);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        generate_kernel<<<blocks, 256, 0, s>>>(wf, job);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t s)
+    {
+        resolve_kernel<<<blocks, 128, 0, s>>>(job, accumulation, framebuffer);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_clear(uint32_t* framebuffer, uint32_t n, uint32_t value, cudaStream_t s)
+    {
+        if (n == 0) return cudaSuccess;
+        clear_kernel<<<(n + 511) / 512 < 4096 ? (n + 511) / 512 : 4096, 512, 0, s>>>(framebuffer, n, value);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_batch_trace(const SceneView& sc, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut, float* uvtOut,
+                                   uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s)
+    {
+        BatchRays b{sc, rays, n, cursor, triOut, uvtOut, occOut};
+        if (occOut) return launch_trace<true>(b, sc.depth, blocks, threads, 32, errorFlags, s);
+        return launch_trace<false>(b, sc.depth, blocks, threads, 32, errorFlags, s);
+    }
+
+    cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
+                                       const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t s)
+    {
+        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
+        shading_record_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(positions, normals, tangents, uvs, materialIds, n, shading);
+        return cudaGetLastError();
+    }
+
+    template <typename T>
+    static cudaError_t exclusive_scan(const T* in, T* out, uint32_t n, T* scratch, cudaStream_t s)
+    {
+        // scratch: >= ceil(n/1024) + ceil(n/1024^2) + ... + 3 elements
+        if (n == 0) return cudaSuccess;
+        const uint32_t blocks = (n + 1023) / 1024;
+        T* sums = scratch;
+        scan_block_kernel<T><<<blocks, 1024, 0, s>>>(in, out, blocks > 1 ? sums : nullptr, n);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess || blocks == 1) return e;
+        e = exclusive_scan<T>(sums, sums, blocks, scratch + blocks, s);
+        if (e != cudaSuccess) return e;
+        scan_add_kernel<T><<<blocks, 1024, 0, s>>>(out, sums, n);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_light_build(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+                                   uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCountDev, cudaStream_t s)
+    {
+        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
+        light_flag_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(shading, materials, n, flags);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        e = exclusive_scan<uint32_t>(flags, index, n, scanScratch, s);
+        if (e != cudaSuccess) return e;
+        scan_total_kernel<<<1, 1, 0, s>>>(flags, index, n, lightCountDev);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+                                     const uint32_t* flags, const uint32_t* index, float4* lights, double* weights, cudaStream_t s)
+    {
+        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
+        light_record_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(positions, shading, materials, n, flags, index, lights, weights);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_alias_build(const double* weights, uint32_t n, double* prefix, double* scanScratch, uint4* bins,
+                                   uint32_t* stackIndex, float* stackValue, cudaStream_t s)
+    {
+        if (n == 0) return cudaSuccess;
+        cudaError_t e = exclusive_scan<double>(weights, prefix, n, scanScratch, s);
+        if (e != cudaSuccess) return e;
+        alias_build_kernel<<<1, 32, 0, s>>>(weights, prefix, n, bins, stackIndex, stackValue);
+        return cudaGetLastError();
+    }
+
+    size_t scan_scratch_elements(uint32_t n)
+    {
+        size_t total = 3;
+        uint32_t m = n;
+        while (m > 1)
+        {
+            m = (m + 1023) / 1024;
+            total += m;
+        }
+        return total;
+    }
+}

@@ -1,0 +1,39 @@
+// Host-side launchers of the kernels in kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "pt_internal.h"
+
+namespace pt
+{
+    struct IterationLaunch
+    {
+        SceneView scene;
+        Wavefront wf;
+        const JobView* job;       // device pointer
+        cudaGraphConditionalHandle handle;
+        bool modelPresent[kModelCount];
+        bool nee;
+        int traceBlocks;
+        int traceThreads;
+        uint32_t refill;
+        int shadeBlocks;
+    };
+
+    int trace_grid_blocks(int device, int threads, uint32_t depth);
+    cudaError_t launch_iteration(const IterationLaunch& launch, cudaStream_t stream);
+    cudaError_t launch_frame_prologue(const Wavefront& wf, const JobView* job, uint32_t pool, int blocks, cudaStream_t stream);
+    cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t stream);
+    cudaError_t launch_clear(uint32_t* framebuffer, uint32_t n, uint32_t value, cudaStream_t stream);
+    cudaError_t launch_batch_trace(const SceneView& scene, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
+                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t stream);
+    cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
+                                       const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t stream);
+    cudaError_t launch_light_build(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+                                   uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCount, cudaStream_t stream);
+    cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+                                     const uint32_t* flags, const uint32_t* index, float4* lights, double* weights, cudaStream_t stream);
+    cudaError_t launch_alias_build(const double* weights, uint32_t n, double* prefix, double* scanScratch, uint4* bins,
+                                   uint32_t* stackIndex, float* stackValue, cudaStream_t stream);
+    size_t scan_scratch_elements(uint32_t n);
+}

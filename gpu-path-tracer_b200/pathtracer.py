@@ -1,0 +1,344 @@
+"""ctypes binding of libgpt_b200.so (include/gpt_b200.h) for tests, benchmarks and scripting.
+
+The product is the C ABI; this module only marshals numpy arrays and torch
+device tensors into it. There is no fallback: if the shared library is missing
+or no CUDA device is present, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpt_b200.so")
+QUEUE_LOG_COLUMNS = 9
+INVALID = 0xFFFFFFFF
+
+_lib = None
+
+
+class GptError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{message} (status {code})")
+        self.code = code
+
+
+class gpt_material(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_uint32), ("color", ctypes.c_float * 3), ("specular", ctypes.c_float * 3),
+                ("shininess", ctypes.c_float), ("rma", ctypes.c_float * 3), ("emission", ctypes.c_float * 3),
+                ("normal", ctypes.c_float * 3), ("ior", ctypes.c_float), ("transmission", ctypes.c_float),
+                ("reserved", ctypes.c_float)]
+
+
+class gpt_scene_desc(ctypes.Structure):
+    _fields_ = [("triangle_count", ctypes.c_uint32), ("positions", ctypes.c_void_p), ("normals", ctypes.c_void_p),
+                ("tangents", ctypes.c_void_p), ("uvs", ctypes.c_void_p), ("material_ids", ctypes.c_void_p),
+                ("material_count", ctypes.c_uint32), ("materials", ctypes.c_void_p)]
+
+
+class gpt_device_camera(ctypes.Structure):
+    _fields_ = [("origin", ctypes.c_float * 3), ("lower_left", ctypes.c_float * 3),
+                ("horizontal", ctypes.c_float * 3), ("vertical", ctypes.c_float * 3)]
+
+
+class gpt_motion_state(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_float * 3), ("rotation", ctypes.c_float * 4)]
+
+
+class gpt_render_settings(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("samples_per_pixel", ctypes.c_uint32),
+                ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
+                ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32)]
+
+
+class gpt_frame_stats(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("samples", ctypes.c_uint64),
+                ("rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("device_ms", ctypes.c_float),
+                ("reserved_f", ctypes.c_float)]
+
+
+# (name, restype, argtypes) of every C entry point in include/gpt_b200.h
+_SIGNATURES = [
+    ("gpt_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("gpt_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    ("gpt_destroy", None, [ctypes.c_void_p]),
+    ("gpt_init_rendering_buffers", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("gpt_init_scene_buffers", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc)]),
+    ("gpt_clear", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_uint8]),
+    ("gpt_start_simulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                            ctypes.POINTER(gpt_motion_state), ctypes.c_uint32, ctypes.c_uint32,
+                                            ctypes.c_uint32, ctypes.c_char_p, ctypes.c_int]),
+    ("gpt_resume_simulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gpt_stop_rendering", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpt_is_rendering", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpt_get_done_frames", ctypes.c_uint32, [ctypes.c_void_p]),
+    ("gpt_get_total_frames", ctypes.c_uint32, [ctypes.c_void_p]),
+    ("gpt_get_done_samples", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("gpt_get_total_samples", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("gpt_get_width", ctypes.c_uint32, [ctypes.c_void_p]),
+    ("gpt_get_height", ctypes.c_uint32, [ctypes.c_void_p]),
+    ("gpt_lock_frame", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t),
+                                      ctypes.POINTER(ctypes.c_size_t)]),
+    ("gpt_unlock_frame", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpt_peek_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    ("gpt_consume_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    ("gpt_render_frame", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_device_camera),
+                                        ctypes.POINTER(gpt_render_settings), ctypes.POINTER(gpt_frame_stats)]),
+    ("gpt_read_framebuffer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    ("gpt_read_accumulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
+    ("gpt_read_sample_radiance", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
+    ("gpt_read_queue_log", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                          ctypes.POINTER(ctypes.c_uint32)]),
+    ("gpt_intersect_closest", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                             ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpt_intersect_any", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
+    ("gpt_scene_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
+    ("gpt_bvh8_check", ctypes.c_int, [ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32),
+                                      ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
+                                      ctypes.POINTER(ctypes.c_uint64)]),
+    ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
+                                              ctypes.POINTER(gpt_device_camera)]),
+]
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libgpt_b200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-C", HERE] + ([] if verbose else ["-s"]), check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise GptError(-1, f"{LIB_PATH} is missing: run `make -C {HERE}` (or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGNATURES:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def declared_symbols() -> list[str]:
+    return [s[0] for s in _SIGNATURES]
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def camera_struct(camera12) -> gpt_device_camera:
+    c = np.asarray(camera12, dtype=np.float32).reshape(12)
+    cam = gpt_device_camera()
+    for k in range(3):
+        cam.origin[k] = c[k]
+        cam.lower_left[k] = c[3 + k]
+        cam.horizontal[k] = c[6 + k]
+        cam.vertical[k] = c[9 + k]
+    return cam
+
+
+class Renderer:
+    """Handle on one gpt_renderer (one device, one render stream)."""
+
+    def __init__(self, device: int = 0):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        rc = self.L.gpt_create(ctypes.byref(h), device)
+        if rc != 0:
+            raise GptError(rc, f"gpt_create(device={device}) failed: {self.L.gpt_status_string(rc).decode()}")
+        self.h = h
+        self._scene_keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gpt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self.L.gpt_consume_last_error(self.h, buf, 1024)
+            raise GptError(rc, f"{what}: {buf.value.decode() or self.L.gpt_status_string(rc).decode()}")
+
+    def last_error(self, consume: bool = False) -> str | None:
+        buf = ctypes.create_string_buffer(1024)
+        fn = self.L.gpt_consume_last_error if consume else self.L.gpt_peek_last_error
+        return buf.value.decode() if fn(self.h, buf, 1024) else None
+
+    def init_rendering_buffers(self, width: int, height: int):
+        self._check(self.L.gpt_init_rendering_buffers(self.h, width, height), "gpt_init_rendering_buffers")
+
+    def upload_scene(self, scene):
+        s = scene.contiguous()
+        desc = gpt_scene_desc(s.triangle_count, _ptr(s.positions).value, _ptr(s.normals).value, _ptr(s.tangents).value,
+                              _ptr(s.uvs).value, _ptr(s.material_ids).value, len(s.materials), _ptr(s.materials).value)
+        self._scene_keep = s
+        self._check(self.L.gpt_init_scene_buffers(self.h, ctypes.byref(desc)), "gpt_init_scene_buffers")
+
+    def scene_info(self) -> dict:
+        n, d, l, t = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.L.gpt_scene_info(self.h, ctypes.byref(n), ctypes.byref(d), ctypes.byref(l), ctypes.byref(t)),
+                    "gpt_scene_info")
+        return dict(nodes=n.value, depth=d.value, lights=l.value, triangles=t.value)
+
+    def alias_table(self) -> np.ndarray:
+        lights = self.scene_info()["lights"]
+        out = np.zeros((lights, 4), dtype=np.uint32)
+        if lights:
+            self._check(self.L.gpt_read_alias_table(self.h, _ptr(out), lights), "gpt_read_alias_table")
+        return out
+
+    def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
+                     pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0) -> dict:
+        cam = camera_struct(camera12)
+        st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
+                                 trace_refill)
+        stats = gpt_frame_stats()
+        self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
+                    "gpt_render_frame")
+        self.width, self.height = width, height
+        spa = int(np.sqrt(spp))
+        total = spa * spa * width * height
+        self.total_samples = min(total, max_samples) if max_samples else total
+        return dict(iterations=stats.iterations, samples=stats.samples, rays=stats.rays,
+                    shadow_rays=stats.shadow_rays, device_ms=stats.device_ms)
+
+    def framebuffer(self) -> np.ndarray:
+        out = np.zeros(self.width * self.height, dtype=np.uint32)
+        self._check(self.L.gpt_read_framebuffer(self.h, _ptr(out), out.size), "gpt_read_framebuffer")
+        return out
+
+    def accumulation(self) -> np.ndarray:
+        out = np.zeros((self.width * self.height, 4), dtype=np.float32)
+        self._check(self.L.gpt_read_accumulation(self.h, _ptr(out), self.width * self.height), "gpt_read_accumulation")
+        return out
+
+    def sample_radiance(self) -> np.ndarray:
+        out = np.zeros((self.total_samples, 3), dtype=np.float32)
+        self._check(self.L.gpt_read_sample_radiance(self.h, _ptr(out), self.total_samples), "gpt_read_sample_radiance")
+        return out
+
+    def queue_log(self, max_rows: int = 1 << 16) -> np.ndarray:
+        out = np.zeros((max_rows, QUEUE_LOG_COLUMNS), dtype=np.uint32)
+        n = ctypes.c_uint32()
+        self._check(self.L.gpt_read_queue_log(self.h, _ptr(out), max_rows, ctypes.byref(n)), "gpt_read_queue_log")
+        return out[:n.value]
+
+    def clear(self, r: int, g: int, b: int, a: int):
+        self._check(self.L.gpt_clear(self.h, r, g, b, a), "gpt_clear")
+
+    def lock_frame(self) -> np.ndarray:
+        """Copy of the host frame taken under the frame lock (GetFrameView().Lock())."""
+        data = ctypes.c_void_p()
+        size = ctypes.c_size_t()
+        elem = ctypes.c_size_t()
+        self._check(self.L.gpt_lock_frame(self.h, ctypes.byref(data), ctypes.byref(size), ctypes.byref(elem)),
+                    "gpt_lock_frame")
+        try:
+            buf = (ctypes.c_uint32 * size.value).from_address(data.value) if size.value else []
+            return np.array(buf, dtype=np.uint32)
+        finally:
+            self.L.gpt_unlock_frame(self.h)
+
+    # -- ray batches on device memory (torch tensors as plumbing) --
+    def intersect_closest(self, rays_dev, tri_dev, uvt_dev, stream=None):
+        n = rays_dev.shape[0]
+        self._check(self.L.gpt_intersect_closest(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
+                                                 ctypes.c_void_p(tri_dev.data_ptr()), ctypes.c_void_p(uvt_dev.data_ptr()),
+                                                 ctypes.c_void_p(stream)), "gpt_intersect_closest")
+
+    def intersect_any(self, rays_dev, occ_dev, stream=None):
+        n = rays_dev.shape[0]
+        self._check(self.L.gpt_intersect_any(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
+                                             ctypes.c_void_p(occ_dev.data_ptr()), ctypes.c_void_p(stream)),
+                    "gpt_intersect_any")
+
+    def trace_closest_np(self, rays: np.ndarray):
+        """Closest hits of a host ray batch [n, 8]: returns (tri [n] uint32, uvt [n, 3] float32)."""
+        import torch
+        r = torch.from_numpy(np.ascontiguousarray(rays, dtype=np.float32)).cuda()
+        tri = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        uvt = torch.empty((rays.shape[0], 3), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        self.intersect_closest(r, tri, uvt)
+        return tri.cpu().numpy().view(np.uint32), uvt.cpu().numpy()
+
+    def trace_any_np(self, rays: np.ndarray):
+        import torch
+        r = torch.from_numpy(np.ascontiguousarray(rays, dtype=np.float32)).cuda()
+        occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
+        torch.cuda.synchronize()
+        self.intersect_any(r, occ)
+        return occ.cpu().numpy()
+
+    # -- asynchronous simulation (StartSimulation / StopRendering / ResumeSimulation) --
+    def start_simulation(self, width, height, fov_y, motion_states, spp, depth, output_folder=None, nee=True):
+        arr = (gpt_motion_state * len(motion_states))()
+        for i, (pos, quat) in enumerate(motion_states):
+            for k in range(3):
+                arr[i].position[k] = pos[k]
+            for k in range(4):
+                arr[i].rotation[k] = quat[k]
+        self._motion_keep = arr
+        folder = output_folder.encode() if output_folder else None
+        self._check(self.L.gpt_start_simulation(self.h, width, height, fov_y, arr, len(motion_states), spp, depth, folder,
+                                                1 if nee else 0), "gpt_start_simulation")
+        self.width, self.height = width, height
+
+    def resume_simulation(self, start_frame: int):
+        self._check(self.L.gpt_resume_simulation(self.h, start_frame), "gpt_resume_simulation")
+
+    def stop_rendering(self):
+        self._check(self.L.gpt_stop_rendering(self.h), "gpt_stop_rendering")
+
+    def is_rendering(self) -> bool:
+        return bool(self.L.gpt_is_rendering(self.h))
+
+    def progress(self) -> dict:
+        return dict(done_frames=self.L.gpt_get_done_frames(self.h), total_frames=self.L.gpt_get_total_frames(self.h),
+                    done_samples=self.L.gpt_get_done_samples(self.h), total_samples=self.L.gpt_get_total_samples(self.h))
+
+
+def scene_desc(scene) -> gpt_scene_desc:
+    s = scene.contiguous()
+    return gpt_scene_desc(s.triangle_count, _ptr(s.positions).value, _ptr(s.normals).value, _ptr(s.tangents).value,
+                          _ptr(s.uvs).value, _ptr(s.material_ids).value, len(s.materials), _ptr(s.materials).value)
+
+
+def bvh8_check(scene) -> dict:
+    """Host-only structural validation of the BVH8 builder (no GPU needed)."""
+    desc = scene_desc(scene)
+    n, d = ctypes.c_uint32(), ctypes.c_uint32()
+    v, m = ctypes.c_uint64(), ctypes.c_uint64()
+    rc = lib().gpt_bvh8_check(ctypes.byref(desc), ctypes.byref(n), ctypes.byref(d), ctypes.byref(v), ctypes.byref(m))
+    if rc != 0:
+        raise GptError(rc, "gpt_bvh8_check")
+    return dict(nodes=n.value, depth=d.value, violations=v.value, misplaced=m.value)
+
+
+def make_device_camera(fov_y: float, aspect: float, position, quat_wxyz) -> np.ndarray:
+    st = gpt_motion_state()
+    for k in range(3):
+        st.position[k] = position[k]
+    for k in range(4):
+        st.rotation[k] = quat_wxyz[k]
+    cam = gpt_device_camera()
+    rc = lib().gpt_make_device_camera(fov_y, aspect, ctypes.byref(st), ctypes.byref(cam))
+    if rc != 0:
+        raise GptError(rc, "gpt_make_device_camera")
+    return np.array(list(cam.origin) + list(cam.lower_left) + list(cam.horizontal) + list(cam.vertical), dtype=np.float32)

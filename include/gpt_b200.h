@@ -1,0 +1,214 @@
+/*
+ * gpt_b200.h — C ABI of the B200 wavefront path tracer.
+ *
+ * Drop-in boundary for KrzystekMatej/gpu-path-tracer's CUDA renderer
+ * (Core::Graphics::Cuda::Renderer, Core/Include/Core/Graphics/Cuda/PathTracing/Renderer.hpp:42-189)
+ * and its kernel launchers (Core/Include/Core/Graphics/Cuda/PathTracing/Kernels/Launchers.hpp:20-145).
+ * Plain C types only: opaque handles, raw pointers, sizes. Every call returns an int
+ * status (GPT_OK = 0); no exception crosses the boundary. The message of the last
+ * failure is kept per renderer (gpt_peek_last_error / gpt_consume_last_error), as the
+ * reference keeps m_LastError (Renderer.cpp:453-459, 308-320).
+ */
+#ifndef GPT_B200_H
+#define GPT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define GPT_OK 0
+#define GPT_ERR_INVALID_ARGUMENT 1
+#define GPT_ERR_CUDA 2
+#define GPT_ERR_OUT_OF_MEMORY 3
+#define GPT_ERR_STATE 4          /* e.g. "Renderer is already rendering" (Renderer.cpp:347-348) */
+#define GPT_ERR_NO_SCENE 5
+#define GPT_ERR_CAPACITY 6       /* a size above a documented limit */
+#define GPT_ERR_TIMEOUT 7        /* a bounded device wait ran out */
+#define GPT_ERR_DEVICE_FAULT 8   /* a kernel reported an internal error flag */
+
+/* GlobalShadingModel (Core/Include/Core/Graphics/Cuda/PathTracing/Material.hpp:8-17). */
+enum gpt_shading_model {
+    GPT_MODEL_NORMAL = 0,
+    GPT_MODEL_DIFFUSE = 1,
+    GPT_MODEL_MIRROR = 2,
+    GPT_MODEL_PHONG = 3,
+    GPT_MODEL_GGX = 4,
+    GPT_MODEL_EMISSIVE = 5,
+    GPT_MODEL_COUNT = 6
+};
+
+/*
+ * Constant material: the values the reference's 1x1 material textures return
+ * (Material.hpp:73-87; Manager.cpp:321-380 encodes MTL constants into those texels).
+ * 80 bytes.
+ */
+typedef struct gpt_material {
+    uint32_t model;        /* gpt_shading_model */
+    float color[3];        /* albedo / base colour, linear */
+    float specular[3];     /* Phong specular / mirror reflectance, linear */
+    float shininess;       /* normalised shininess texel t in [0,1]; exponent = t*999+1 (MaterialEval.cu:405-408) */
+    float rma[3];          /* roughness, metallic, ambient occlusion */
+    float emission[3];     /* radiance of emissive triangles */
+    float normal[3];       /* tangent-space normal-map texel in [0,1]; (128,128,255)/255 is the default map */
+    float ior;
+    float transmission;
+    float reserved;
+} gpt_material;
+
+/*
+ * Scene upload, replacing InitializeSceneBuffers(entt::registry, Assets::Storage)
+ * (Renderer.hpp:115, Renderer.cpp:292-306). The arrays are the output of the
+ * reference's BuildTriangles (Renderer.cpp:159-213): world-space per-triangle
+ * vertex data, already transformed. All pointers are host memory.
+ */
+typedef struct gpt_scene_desc {
+    uint32_t triangle_count;
+    const float* positions;       /* [T][3][3] world positions */
+    const float* normals;         /* [T][3][3] world normals */
+    const float* tangents;        /* [T][3][4] world tangent xyz + handedness sign */
+    const float* uvs;             /* [T][3][2] */
+    const uint32_t* material_ids; /* [T] index into materials */
+    uint32_t material_count;
+    const gpt_material* materials;
+} gpt_scene_desc;
+
+/* DeviceCamera (Core/Include/Core/Graphics/Cuda/PathTracing/DeviceCamera.hpp:5-11). */
+typedef struct gpt_device_camera {
+    float origin[3];
+    float lower_left[3];
+    float horizontal[3];
+    float vertical[3];
+} gpt_device_camera;
+
+/* Capture::MotionState (Core/Include/Core/Capture/Sample.hpp:6-10): position, quaternion (w, x, y, z). */
+typedef struct gpt_motion_state {
+    float position[3];
+    float rotation[4];
+} gpt_motion_state;
+
+/* Per-frame settings of StartSimulation (Renderer.cpp:330-376) plus B200 tuning knobs. */
+typedef struct gpt_render_settings {
+    uint32_t width;
+    uint32_t height;
+    uint32_t samples_per_pixel;   /* rounded down to a square, as Renderer.cpp:366-367 */
+    uint32_t path_depth;          /* clamped to [1, 100] (PathTracerDefaults.hpp:15-17) */
+    uint32_t use_nee;             /* next-event estimation */
+    uint32_t pool_size;           /* path slots; 0 = 1,048,576 (PathTracerDefaults.hpp:9) */
+    uint64_t max_samples;         /* 0 = the whole frame; else render only sample indices [0, max_samples) */
+    uint32_t trace_block;         /* 0 = autotuned/default threads per block of the traversal kernels */
+    uint32_t trace_refill;        /* 0 = default; idle lanes a warp waits for before fetching new rays */
+} gpt_render_settings;
+
+typedef struct gpt_frame_stats {
+    uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */
+    uint32_t reserved;
+    uint64_t samples;             /* paths rendered */
+    uint64_t rays;                /* extension + camera rays traced (closest hit) */
+    uint64_t shadow_rays;         /* NEE shadow rays traced (any hit) */
+    float device_ms;              /* CUDA-event time of the frame on the render stream */
+    float reserved_f;
+} gpt_frame_stats;
+
+typedef struct gpt_renderer gpt_renderer;
+
+const char* gpt_status_string(int status);
+
+/* Renderer lifetime; device = CUDA ordinal. Renderer() / ~Renderer() (Renderer.hpp:105-106). */
+int gpt_create(gpt_renderer** out, int device);
+void gpt_destroy(gpt_renderer* renderer);
+
+/* Renderer::InitializeRenderingBuffers (Renderer.hpp:114, Renderer.cpp:265-290). */
+int gpt_init_rendering_buffers(gpt_renderer* renderer, uint32_t width, uint32_t height);
+/* Renderer::InitializeSceneBuffers (Renderer.hpp:115, Renderer.cpp:292-306). */
+int gpt_init_scene_buffers(gpt_renderer* renderer, const gpt_scene_desc* scene);
+/* Renderer::Clear (Renderer.hpp:117, Renderer.cpp:322-328, 677-687). */
+int gpt_clear(gpt_renderer* renderer, uint8_t r, uint8_t g, uint8_t b, uint8_t a);
+
+/*
+ * Renderer::StartSimulation (Renderer.hpp:118-126, Renderer.cpp:330-399): renders one frame per
+ * motion state on a worker thread. fov_y in radians (Graphics::Ecs::Camera::fovY). When
+ * output_folder is not NULL each finished frame is written as frame_NNNN.png there
+ * (Renderer.cpp:645-675), flipped vertically like the reference.
+ */
+int gpt_start_simulation(gpt_renderer* renderer, uint32_t width, uint32_t height, float fov_y,
+                         const gpt_motion_state* motion_states, uint32_t motion_state_count,
+                         uint32_t samples_per_pixel, uint32_t path_depth, const char* output_folder, int use_nee);
+/* Renderer::ResumeSimulation (Renderer.hpp:127, Renderer.cpp:401-427). */
+int gpt_resume_simulation(gpt_renderer* renderer, uint32_t start_frame);
+/* Renderer::StopRendering (Renderer.hpp:128, Renderer.cpp:429-440). */
+int gpt_stop_rendering(gpt_renderer* renderer);
+/* Progress getters (Renderer.hpp:131-140). */
+int gpt_is_rendering(const gpt_renderer* renderer);
+uint32_t gpt_get_done_frames(const gpt_renderer* renderer);
+uint32_t gpt_get_total_frames(const gpt_renderer* renderer);
+uint64_t gpt_get_done_samples(const gpt_renderer* renderer);
+uint64_t gpt_get_total_samples(const gpt_renderer* renderer);
+uint32_t gpt_get_width(const gpt_renderer* renderer);
+uint32_t gpt_get_height(const gpt_renderer* renderer);
+
+/* GetFrameView().Lock() (Renderer.hpp:45-103,130): the host RGBA8 frame, held until unlock. */
+int gpt_lock_frame(gpt_renderer* renderer, const uint32_t** data, size_t* size, size_t* element_size);
+int gpt_unlock_frame(gpt_renderer* renderer);
+
+/* PeekLastError / ConsumeLastError (Renderer.hpp:142-143). Writes a NUL-terminated message; returns
+ * 1 when an error was present, 0 otherwise. */
+int gpt_peek_last_error(const gpt_renderer* renderer, char* buffer, size_t length);
+int gpt_consume_last_error(gpt_renderer* renderer, char* buffer, size_t length);
+
+/*
+ * One frame, synchronously, on the calling thread: Renderer::RenderFrame (Renderer.cpp:468-647)
+ * without the worker thread or PNG output. The frame runs as one CUDA graph (device-driven
+ * wavefront loop, no host synchronisation per iteration). Results stay on the device until read.
+ */
+int gpt_render_frame(gpt_renderer* renderer, const gpt_device_camera* camera,
+                     const gpt_render_settings* settings, gpt_frame_stats* stats);
+/* Copies of the last frame's results to host memory. */
+int gpt_read_framebuffer(gpt_renderer* renderer, uint32_t* rgba, size_t pixel_count);
+int gpt_read_accumulation(gpt_renderer* renderer, float* rgba32f, size_t pixel_count);
+/* Per-sample (per-path) radiance of the last frame, [samples][3], in sample-index order. */
+int gpt_read_sample_radiance(gpt_renderer* renderer, float* rgb, uint64_t sample_count);
+/* Per-iteration queue sizes of the last frame: rows of 9 words (rays, 6 material queues,
+ * shadow rays, regenerated/terminated paths), as the reference's queues hold them. */
+int gpt_read_queue_log(gpt_renderer* renderer, uint32_t* rows, uint32_t max_rows, uint32_t* row_count);
+
+/*
+ * Ray-batch traversal on the current scene (Kernels::IntersectRaysWithScene and
+ * Kernels::IntersectShadowRaysWithScene, Launchers.hpp:60-80 / Intersect.cu:216-295, with the
+ * queue plumbing replaced by plain arrays). Device pointers; stream may be NULL (the renderer's
+ * stream). rays: [n][8] float = origin xyz, direction xyz, tMin, tMax.
+ * Closest: tri_out [n] = original triangle index or 0xFFFFFFFF; uvt_out [n][3] = u, v, t.
+ * Any: occluded_out [n] = 1 if any triangle hits with tMin <= t < tMax.
+ */
+int gpt_intersect_closest(gpt_renderer* renderer, const float* rays, uint32_t n, uint32_t* tri_out,
+                          float* uvt_out, void* stream);
+int gpt_intersect_any(gpt_renderer* renderer, const float* rays, uint32_t n, uint8_t* occluded_out,
+                      void* stream);
+
+/* Scene statistics after upload: BVH8 node count, tree depth, light count, triangle count. */
+int gpt_scene_info(const gpt_renderer* renderer, uint32_t* node_count, uint32_t* depth, uint32_t* light_count,
+                   uint32_t* triangle_count);
+/* The light alias table built on the device, [lights][4] words (q, p, alias, value)
+ * (AliasTableView.hpp:8-14). */
+int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
+
+/*
+ * Host-side validation of the BVH8 builder (no device work): builds the wide BVH for a scene and
+ * checks in exact arithmetic that every quantised child box contains its subtree, and that every
+ * triangle sits in exactly one leaf. Replaces nothing in the reference; it pins the structural
+ * guarantee behind HostBvh.cpp:37-48's padded bounds for the quantised tree.
+ */
+int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* depth,
+                   uint64_t* containment_violations, uint64_t* misplaced_triangles);
+
+/* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */
+int gpt_make_device_camera(float fov_y, float aspect, const gpt_motion_state* state, gpt_device_camera* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPT_B200_H */

@@ -1,0 +1,188 @@
+"""ORACLE — test infrastructure only (ctypes binding of oracle/liboracle.so).
+
+The CPU restatement of the reference path tracer (oracle/oracle.cpp). Only
+tests/, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg use it,
+always as the checker or the timed CPU reference, never as the product.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("left", "<u4"), ("right", "<u4"),
+                       ("first", "<u4"), ("count", "<u4")])
+BIN_DTYPE = np.dtype([("q", "<f4"), ("p", "<f4"), ("alias", "<u4"), ("value", "<u4")])
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = ctypes.CDLL(_LIB)
+        vp, u32, i32, u64, f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint64, ctypes.c_float
+        L.oracle_scene_create.restype = vp
+        L.oracle_scene_create.argtypes = [u32, vp, vp, vp, vp, vp, u32, vp]
+        L.oracle_scene_destroy.argtypes = [vp]
+        L.oracle_scene_bvh_node_count.restype = u32
+        L.oracle_scene_bvh_node_count.argtypes = [vp]
+        L.oracle_scene_bvh_depth.restype = u32
+        L.oracle_scene_bvh_depth.argtypes = [vp]
+        L.oracle_scene_bvh_export.argtypes = [vp, vp, vp]
+        L.oracle_scene_light_count.restype = u32
+        L.oracle_scene_light_count.argtypes = [vp]
+        L.oracle_scene_alias_export.argtypes = [vp, vp]
+        L.oracle_trace_closest.argtypes = [vp, vp, u32, vp, vp, i32]
+        L.oracle_trace_any.argtypes = [vp, vp, u32, vp, i32]
+        L.oracle_alias_build.argtypes = [vp, u32, vp]
+        L.oracle_alias_sample.argtypes = [vp, u32, vp, u32, vp, vp]
+        L.oracle_philox_words.argtypes = [u64, u64, u32, vp, vp]
+        L.oracle_sincos.argtypes = [vp, u32, vp, vp]
+        L.oracle_pow.argtypes = [vp, vp, u32, vp]
+        L.oracle_render.restype = i32
+        L.oracle_render.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, u64, i32, i32, vp, vp, vp, vp, u32, vp]
+        L.oracle_make_camera.argtypes = [f32, f32, vp, vp, vp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def default_threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+class OracleScene:
+    """Scene prepared the reference way: triangle records, area-weighted light
+    alias table, median-split BVH (Renderer.cpp:292-306)."""
+
+    def __init__(self, scene):
+        self.scene = scene
+        self._keep = (scene.positions, scene.normals, scene.tangents, scene.uvs, scene.material_ids, scene.materials)
+        self.handle = lib().oracle_scene_create(scene.triangle_count, _p(scene.positions), _p(scene.normals),
+                                                _p(scene.tangents), _p(scene.uvs), _p(scene.material_ids),
+                                                len(scene.materials), _p(scene.materials))
+
+    def close(self):
+        if self.handle:
+            lib().oracle_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bvh(self):
+        n = lib().oracle_scene_bvh_node_count(self.handle)
+        nodes = np.zeros(n, dtype=NODE_DTYPE)
+        order = np.zeros(self.scene.triangle_count, dtype=np.uint32)
+        lib().oracle_scene_bvh_export(self.handle, _p(nodes), _p(order))
+        return nodes, order, lib().oracle_scene_bvh_depth(self.handle)
+
+    def alias_table(self):
+        n = lib().oracle_scene_light_count(self.handle)
+        bins = np.zeros(n, dtype=BIN_DTYPE)
+        if n:
+            lib().oracle_scene_alias_export(self.handle, _p(bins))
+        return bins
+
+    def trace_closest(self, rays: np.ndarray, threads: int | None = None):
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        n = rays.shape[0]
+        tri = np.zeros(n, dtype=np.uint32)
+        uvt = np.zeros((n, 3), dtype=np.float32)
+        lib().oracle_trace_closest(self.handle, _p(rays), n, _p(tri), _p(uvt), threads or default_threads())
+        return tri, uvt
+
+    def trace_any(self, rays: np.ndarray, threads: int | None = None):
+        rays = np.ascontiguousarray(rays, dtype=np.float32)
+        occ = np.zeros(rays.shape[0], dtype=np.uint8)
+        lib().oracle_trace_any(self.handle, _p(rays), rays.shape[0], _p(occ), threads or default_threads())
+        return occ
+
+    def render(self, camera: np.ndarray, width: int, height: int, spp: int, depth: int, nee: bool = True,
+               pool_size: int = 1 << 20, max_samples: int = 0, threads: int | None = None, accumulation: int = 1,
+               log_capacity: int = 1 << 16):
+        """Replay of Renderer::RenderFrame on the CPU. accumulation: 0 = FP32 in
+        sample order, 1 = FP32 Kahan in sample order, 2 = FP64."""
+        spa = int(np.sqrt(spp))
+        spp_eff = spa * spa
+        total = spp_eff * width * height
+        if max_samples:
+            total = min(total, max_samples)
+        camera = np.ascontiguousarray(camera, dtype=np.float32)
+        radiance = np.zeros((max(total, 1), 3), dtype=np.float32)
+        accum = np.zeros((width * height, 4), dtype=np.float32)
+        fb = np.zeros(width * height, dtype=np.uint32)
+        qlog = np.zeros((log_capacity, 9), dtype=np.uint32)
+        iters = ctypes.c_uint32(0)
+        rc = lib().oracle_render(self.handle, _p(camera), width, height, spp, depth, 1 if nee else 0, pool_size,
+                                 max_samples, threads or default_threads(), accumulation, _p(radiance), _p(accum),
+                                 _p(fb), _p(qlog), log_capacity, ctypes.byref(iters))
+        if rc != 0:
+            raise RuntimeError(f"oracle_render failed: {rc}")
+        it = iters.value
+        return dict(sample_radiance=radiance[:total], accumulation=accum, framebuffer=fb,
+                    queue_log=qlog[:min(it, log_capacity)], iterations=it, total_samples=total)
+
+
+def alias_build(weights: np.ndarray) -> np.ndarray:
+    weights = np.ascontiguousarray(weights, dtype=np.float32)
+    bins = np.zeros(weights.size, dtype=BIN_DTYPE)
+    lib().oracle_alias_build(_p(weights), weights.size, _p(bins))
+    return bins
+
+
+def alias_sample(bins: np.ndarray, u: np.ndarray):
+    u = np.ascontiguousarray(u, dtype=np.float32)
+    idx = np.zeros(u.size, dtype=np.uint32)
+    pmf = np.zeros(u.size, dtype=np.float32)
+    lib().oracle_alias_sample(_p(np.ascontiguousarray(bins)), bins.size, _p(u), u.size, _p(idx), _p(pmf))
+    return idx, pmf
+
+
+def philox_words(subsequence: int, position: int, count: int):
+    words = np.zeros(count, dtype=np.uint32)
+    uni = np.zeros(count, dtype=np.float32)
+    lib().oracle_philox_words(subsequence, position, count, _p(words), _p(uni))
+    return words, uni
+
+
+def sincos(x: np.ndarray):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    s = np.zeros_like(x)
+    c = np.zeros_like(x)
+    lib().oracle_sincos(_p(x), x.size, _p(s), _p(c))
+    return s, c
+
+
+def powf(x: np.ndarray, y: np.ndarray):
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    out = np.zeros_like(x)
+    lib().oracle_pow(_p(x), _p(y), x.size, _p(out))
+    return out
+
+
+def make_camera_from_motion(fov_y: float, aspect: float, position, quat_wxyz) -> np.ndarray:
+    pos = np.ascontiguousarray(position, dtype=np.float32)
+    q = np.ascontiguousarray(quat_wxyz, dtype=np.float32)
+    out = np.zeros(12, dtype=np.float32)
+    lib().oracle_make_camera(ctypes.c_float(fov_y), ctypes.c_float(aspect), _p(pos), _p(q), _p(out))
+    return out

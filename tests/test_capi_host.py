@@ -1,0 +1,89 @@
+"""The C-ABI library without a GPU: it loads, exports every symbol include/gpt_b200.h
+declares, and its host-only entry points (BVH8 builder validation, camera) behave."""
+import ctypes
+import math
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle
+import pathtracer
+import scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "gpt_b200.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(gpt_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = pathtracer.lib()
+    declared = header_functions()
+    assert len(declared) >= 30
+    out = subprocess.run(["nm", "-D", "--defined-only", pathtracer.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (gpt_[a-z0-9_]+)", out))
+    missing = [f for f in declared if f not in exported]
+    assert not missing, missing
+    for f in declared:
+        assert getattr(lib, f) is not None
+    assert sorted(pathtracer.declared_symbols()) == declared
+
+
+def test_library_is_built_for_sm100a():
+    out = subprocess.run(["cuobjdump", "--list-elf", pathtracer.LIB_PATH], capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump not available")
+    assert "sm_100a" in out.stdout
+
+
+def test_status_strings():
+    lib = pathtracer.lib()
+    assert lib.gpt_status_string(0) == b"ok"
+    assert lib.gpt_status_string(5) == b"no scene uploaded"
+
+
+@pytest.mark.parametrize("name", ["cornell", "cornell-all", "spheres-small", "spheres-200k"])
+def test_bvh8_quantised_boxes_contain_their_subtrees(name):
+    s = scenes.config_scene(name)
+    r = pathtracer.bvh8_check(s)
+    assert r["violations"] == 0
+    assert r["misplaced"] == 0
+    assert r["depth"] <= 64
+    assert r["nodes"] >= 1
+
+
+def test_bvh8_degenerate_inputs():
+    # all triangles identical (no SAH split possible) and a single triangle
+    s = scenes.cornell_box(1)
+    same = scenes.Scene(np.repeat(s.positions[:1], 64, 0), np.repeat(s.normals[:1], 64, 0), np.repeat(s.tangents[:1], 64, 0),
+                        np.repeat(s.uvs[:1], 64, 0), np.zeros(64, np.uint32), s.materials[:1].copy())
+    r = pathtracer.bvh8_check(same)
+    assert r["violations"] == 0 and r["misplaced"] == 0
+    one = scenes.Scene(s.positions[:1].copy(), s.normals[:1].copy(), s.tangents[:1].copy(), s.uvs[:1].copy(),
+                       np.zeros(1, np.uint32), s.materials[:1].copy())
+    r = pathtracer.bvh8_check(one)
+    assert r["violations"] == 0 and r["misplaced"] == 0 and r["nodes"] == 1
+
+
+def test_make_device_camera_matches_reference_restatement():
+    pos = (0.3, 1.2, 4.0)
+    q = np.array([0.9, 0.1, -0.3, 0.2], dtype=np.float64)
+    q = q / np.linalg.norm(q)
+    got = pathtracer.make_device_camera(math.radians(40.0), 16 / 9, pos, q)
+    ref = oracle.make_camera_from_motion(math.radians(40.0), 16 / 9, pos, q)
+    assert np.allclose(got, ref, rtol=0, atol=1e-6)
+
+
+def test_scene_validation_rejects_bad_material_index():
+    s = scenes.cornell_box(1)
+    bad = scenes.Scene(s.positions.copy(), s.normals.copy(), s.tangents.copy(), s.uvs.copy(),
+                       np.full(36, 99, np.uint32), s.materials.copy())
+    with pytest.raises(pathtracer.GptError):
+        pathtracer.bvh8_check(bad)

@@ -1,0 +1,237 @@
+"""Parity of the sm_100a path (through the C ABI) with the oracle, on the same seeded inputs.
+
+Bar: bit-exact hit triangle ids, queue counts and alias-table entries; per-path (per-sample)
+radiance within 1e-4 relative (the kernels and the oracle follow the same IEEE operation order,
+so they are expected to agree bit for bit; the tolerance is the stated bar); converged image
+within a stated RMSE of the FP64-accumulated oracle.
+"""
+import ctypes
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+import pytest
+
+import oracle
+import pathtracer
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+INVALID = 0xFFFFFFFF
+RADIANCE_RTOL = 1e-4
+
+
+def kat_lib():
+    path = os.path.join(HERE, "kat", "libphilox_kat.so")
+    if not os.path.exists(path):
+        import subprocess
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "kat")], check=True)
+    L = ctypes.CDLL(path)
+    L.philox_kat.restype = ctypes.c_int
+    L.philox_kat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                             ctypes.c_void_p, ctypes.c_void_p]
+    return L
+
+
+def run_kat(subseq, offsets):
+    import torch
+    s = torch.tensor(np.asarray(subseq, dtype=np.uint64).view(np.int64), device="cuda")
+    o = torch.tensor(np.asarray(offsets, dtype=np.uint32).view(np.int32), device="cuda")
+    n, k = len(subseq), len(offsets)
+    sched = torch.zeros((n, 14), dtype=torch.float32, device="cuda")
+    reinit = torch.zeros((n, k, 4), dtype=torch.float32, device="cuda")
+    words = torch.zeros((n, 8), dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    rc = kat_lib().philox_kat(s.data_ptr(), n, o.data_ptr(), k, sched.data_ptr(), reinit.data_ptr(), words.data_ptr())
+    assert rc == 0
+    return sched.cpu().numpy(), reinit.cpu().numpy(), words.cpu().numpy().view(np.uint32)
+
+
+def test_oracle_philox_matches_device_curand():
+    subseq = [0, 1, 2, 3, 1000, 123456789, 2**32 + 5, 2**40 + 77]
+    sched, _, words = run_kat(subseq, [0])
+    for i, s in enumerate(subseq):
+        w, u = oracle.philox_words(s, 0, 17)
+        assert np.array_equal(words[i], w[:8]), s
+        assert np.array_equal(sched[i], u[:14]), s
+
+
+def test_curand_reinit_at_offset_continues_the_stream():
+    # the path slots keep (sample, stream position) instead of the 64-byte curand state
+    subseq = list(range(0, 4096, 7))
+    offsets = [0, 1, 4, 5, 8, 9, 13, 40, 41, 42, 43]
+    _, reinit, _ = run_kat(subseq, offsets)
+    for i, s in enumerate(subseq):
+        _, u = oracle.philox_words(s, 0, 48)
+        for k, off in enumerate(offsets):
+            assert np.array_equal(reinit[i, k], u[off:off + 4]), (s, off)
+
+
+@pytest.fixture(scope="module")
+def cornell(gpu_renderer, scene_factory, oracle_scene):
+    s = scene_factory("cornell")
+    gpu_renderer.upload_scene(s)
+    return gpu_renderer, s, oracle_scene("cornell")
+
+
+def test_hit_ids_cornell_1m_rays_bit_exact(cornell):
+    r, s, o = cornell
+    rays = scenes.hit_ray_set(s, 1 << 20, seed=11)
+    tri_g, uvt_g = r.trace_closest_np(rays)
+    tri_o, uvt_o = o.trace_closest(rays)
+    assert np.array_equal(tri_g, tri_o)
+    hit = tri_o != INVALID
+    assert hit.mean() > 0.5
+    assert np.array_equal(uvt_g[hit].view(np.uint32), uvt_o[hit].view(np.uint32))
+
+
+def test_any_hit_cornell_bit_exact(cornell):
+    r, s, o = cornell
+    rays = scenes.hit_ray_set(s, 1 << 18, seed=12)
+    tri, uvt = o.trace_closest(rays)
+    t = np.where(tri != INVALID, uvt[:, 2], 10.0)
+    rays[0::2, 7] = t[0::2] * 0.999
+    rays[1::2, 7] = t[1::2] * 1.001
+    occ_g = r.trace_any_np(rays)
+    occ_o = o.trace_any(rays)
+    assert np.array_equal(occ_g, occ_o)
+    assert occ_o[1::2].mean() > 0.5
+
+
+def test_alias_table_bit_exact(cornell):
+    r, s, o = cornell
+    assert np.array_equal(r.alias_table(), o.alias_table().view(np.uint32).reshape(-1, 4))
+
+
+def assert_render_parity(r, o, cam, w, h, spp, depth, nee, pool=1 << 20):
+    stats = r.render_frame(cam, w, h, spp, depth, nee, pool_size=pool)
+    ref = o.render(cam, w, h, spp, depth, nee, pool_size=pool, accumulation=1)
+    assert stats["samples"] == ref["total_samples"]
+    assert stats["iterations"] == ref["iterations"]
+    log = r.queue_log()
+    assert np.array_equal(log, ref["queue_log"])
+    rad_g, rad_o = r.sample_radiance(), ref["sample_radiance"]
+    assert np.all(np.isfinite(rad_g))
+    err = np.abs(rad_g - rad_o)
+    assert np.all(err <= RADIANCE_RTOL * np.maximum(np.abs(rad_o), 1e-6)), float(err.max())
+    exact = float(np.mean(np.all(rad_g.view(np.uint32) == rad_o.view(np.uint32), axis=1)))
+    acc = r.accumulation()
+    assert np.all(np.abs(acc - ref["accumulation"]) <= RADIANCE_RTOL * np.maximum(np.abs(ref["accumulation"]), 1e-6))
+    fb = r.framebuffer()
+    assert np.max(np.abs(fb.view(np.uint8).astype(int) - ref["framebuffer"].view(np.uint8).astype(int))) <= 1
+    return stats, exact, ref
+
+
+def test_render_cornell_c1_parity(cornell):
+    """512x512, 16 spp, depth 8, NEE, 2-entry alias table."""
+    r, s, o = cornell
+    cam = scenes.scene_camera(s, 512, 512)
+    stats, exact, ref = assert_render_parity(r, o, cam, 512, 512, 16, 8, True)
+    assert exact == 1.0
+    assert np.array_equal(r.framebuffer(), ref["framebuffer"])
+
+
+def test_render_cornell_small_pool_parity(cornell):
+    # pool smaller than the frame: exercises regeneration across many iterations
+    r, s, o = cornell
+    cam = scenes.scene_camera(s, 64, 64)
+    _, exact, _ = assert_render_parity(r, o, cam, 64, 64, 16, 8, True, pool=5000)
+    assert exact == 1.0
+
+
+@pytest.mark.parametrize("nee", [True, False])
+def test_render_all_shading_models_parity(gpu_renderer, scene_factory, oracle_scene, nee):
+    s = scene_factory("cornell-all")
+    o = oracle_scene("cornell-all")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 128, 128)
+    _, exact, _ = assert_render_parity(gpu_renderer, o, cam, 128, 128, 16, 10, nee)
+    assert exact == 1.0
+    assert np.array_equal(gpu_renderer.alias_table(), o.alias_table().view(np.uint32).reshape(-1, 4))
+
+
+def test_render_spheres_parity(gpu_renderer, scene_factory, oracle_scene):
+    s = scene_factory("spheres-small")
+    o = oracle_scene("spheres-small")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 96, 64)
+    _, exact, _ = assert_render_parity(gpu_renderer, o, cam, 96, 64, 4, 12, True, pool=3000)
+    assert exact == 1.0
+    assert np.array_equal(gpu_renderer.alias_table(), o.alias_table().view(np.uint32).reshape(-1, 4))
+
+
+def test_hit_ids_spheres_200k_bit_exact(gpu_renderer, scene_factory, oracle_scene):
+    s = scene_factory("spheres-200k")
+    o = oracle_scene("spheres-200k")
+    gpu_renderer.upload_scene(s)
+    rays = scenes.hit_ray_set(s, 1 << 20, seed=13)
+    tri_g, uvt_g = gpu_renderer.trace_closest_np(rays)
+    tri_o, uvt_o = o.trace_closest(rays)
+    assert np.array_equal(tri_g, tri_o)
+    hit = tri_o != INVALID
+    assert np.array_equal(uvt_g[hit].view(np.uint32), uvt_o[hit].view(np.uint32))
+    assert np.array_equal(gpu_renderer.alias_table(), o.alias_table().view(np.uint32).reshape(-1, 4))
+
+
+def test_converged_image_rmse_vs_fp64_oracle(gpu_renderer, scene_factory, oracle_scene):
+    s = scene_factory("cornell")
+    o = oracle_scene("cornell")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 48, 48)
+    gpu_renderer.render_frame(cam, 48, 48, 1024, 8, True)
+    ref = o.render(cam, 48, 48, 1024, 8, True, accumulation=2)
+    g = gpu_renderer.accumulation()[:, :3] / 1024.0
+    f = ref["accumulation"][:, :3].astype(np.float64) / 1024.0
+    rmse = float(np.sqrt(np.mean((g - f) ** 2)))
+    assert rmse <= 1e-6 * max(1.0, float(np.sqrt(np.mean(f ** 2))))
+
+
+def test_render_errors_and_clear(gpu_renderer, scene_factory):
+    import pathtracer as P
+    fresh = P.Renderer(0)
+    with pytest.raises(P.GptError) as e:
+        fresh.render_frame(np.zeros(12, np.float32), 8, 8, 1, 1)
+    assert e.value.code == 5
+    fresh.init_rendering_buffers(16, 8)
+    fresh.clear(10, 20, 30, 255)
+    fb = fresh.lock_frame()
+    assert fb.size == 128 and np.all(fb == (10 | 20 << 8 | 30 << 16 | 255 << 24))
+    fresh.close()
+
+
+def test_simulation_thread_frames_stop_resume(gpu_renderer, scene_factory):
+    s = scene_factory("cornell")
+    gpu_renderer.upload_scene(s)
+    states = [((0.5, 0.5, 2.0 + 0.1 * k), (1.0, 0.0, 0.0, 0.0)) for k in range(3)]
+    with tempfile.TemporaryDirectory() as d:
+        gpu_renderer.start_simulation(64, 48, np.radians(40.0), states, 4, 6, d, True)
+        with pytest.raises(pathtracer.GptError):
+            gpu_renderer.start_simulation(64, 48, np.radians(40.0), states, 4, 6, d, True)
+        t0 = time.time()
+        while gpu_renderer.is_rendering() and time.time() - t0 < 60:
+            time.sleep(0.01)
+        assert not gpu_renderer.is_rendering()
+        p = gpu_renderer.progress()
+        assert p["done_frames"] == 3 and p["total_frames"] == 3 and p["total_samples"] == 4 * 64 * 48
+        files = sorted(os.listdir(d))
+        assert files == ["frame_0000.png", "frame_0001.png", "frame_0002.png"]
+        assert open(os.path.join(d, files[0]), "rb").read(8) == b"\x89PNG\r\n\x1a\n"
+        frame = gpu_renderer.lock_frame()
+        assert frame.size == 64 * 48 and np.any(frame != 0)
+        gpu_renderer.resume_simulation(2)
+        while gpu_renderer.is_rendering() and time.time() - t0 < 60:
+            time.sleep(0.01)
+        assert gpu_renderer.progress()["done_frames"] == 3
+        with pytest.raises(pathtracer.GptError):
+            gpu_renderer.resume_simulation(3)
+    # stop mid-run: the device loop ends at the next iteration through the host-mapped flag
+    gpu_renderer.start_simulation(256, 256, np.radians(40.0), states * 4, 256, 8, None, True)
+    time.sleep(0.05)
+    gpu_renderer.stop_rendering()
+    assert not gpu_renderer.is_rendering()
+    assert gpu_renderer.progress()["done_frames"] < 12
+    assert gpu_renderer.last_error() is None
