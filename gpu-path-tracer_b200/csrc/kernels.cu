@@ -43,6 +43,24 @@ namespace pt
         return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
     }
 
+    __device__ __forceinline__ unsigned long long global_ns()
+    {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+
+    // Phase timing: thread 0 of every block stamps its start (min) and its end (max).
+    __device__ __forceinline__ void phase_begin(Counters* c, int phase)
+    {
+        if (c != nullptr && threadIdx.x == 0) atomicMin(&c->tStart[phase], global_ns());
+    }
+    __device__ __forceinline__ void phase_end(Counters* c, int phase)
+    {
+        __syncthreads();
+        if (c != nullptr && threadIdx.x == 0) atomicMax(&c->tEnd[phase], global_ns());
+    }
+
     __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
     __device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
 
@@ -59,7 +77,7 @@ namespace pt
     // ANY: stops at the first triangle with tmin <= t < tmax.
     template <bool ANY>
     __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, uint32_t* stack, uint32_t stride,
-                                                  int stackCap, bool& occluded, uint32_t* errorFlags)
+                                                  int stackCap, bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
     {
         uint32_t node;
         if (st.pending != kInvalid)
@@ -82,6 +100,7 @@ namespace pt
             node = __ldg(childRefs + (i ^ st.ray.oct));
         }
         const uint4* nw = sc.nodes[node].w;
+        visits++;
         const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3), w6 = ldg4(nw + 6);
         const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, w6, st.ray, st.hit.t);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
@@ -93,6 +112,7 @@ namespace pt
             const uint32_t slot = i ^ st.ray.oct;
             const uint32_t first = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
             const uint32_t count = __ldg(reinterpret_cast<const unsigned char*>(&nw[6]) + slot);
+            tests += count;
             for (uint32_t k = 0; k < count; k++)
             {
                 const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
@@ -139,6 +159,8 @@ namespace pt
     {
         SceneView sc;
         Wavefront wf;
+        static constexpr int kPhase = 0;
+        __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->rayCount[wf.ctr->cur]; }
         __device__ uint32_t* cursor() const { return &wf.ctr->traceCursor; }
         __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
@@ -180,6 +202,8 @@ namespace pt
     {
         SceneView sc;
         Wavefront wf;
+        static constexpr int kPhase = 2;
+        __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->shadowCount; }
         __device__ uint32_t* cursor() const { return &wf.ctr->shadowCursor; }
         __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
@@ -213,6 +237,8 @@ namespace pt
         uint32_t* triOut;
         float* uvtOut;
         uint8_t* occOut;
+        static constexpr int kPhase = 0;
+        __device__ Counters* counters() const { return nullptr; }
         __device__ uint32_t count() const { return n; }
         __device__ uint32_t* cursor() const { return cursorPtr; }
         __device__ void load(uint32_t i, float3& o, float3& d, float& tmin, float& tmax, uint32_t& tag) const
@@ -248,7 +274,10 @@ namespace pt
         extern __shared__ uint32_t smem[];
         uint32_t* stack = smem + threadIdx.x;
         const uint32_t stride = blockDim.x;
+        Counters* ctr = work.counters();
+        phase_begin(ctr, Work::kPhase);
         const uint32_t n = work.count();
+        uint32_t visits = 0, tests = 0;
         const uint32_t lane = lane_id();
         const unsigned laneMaskLt = (1u << lane) - 1u;
         TraversalState st;
@@ -295,7 +324,8 @@ namespace pt
                 bool occluded = false;
                 bool more = true;
 #pragma unroll 1
-                for (int k = 0; k < 4 && more; k++) more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags);
+                for (int k = 0; k < 4 && more; k++)
+                    more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags, visits, tests);
                 if (!more)
                 {
                     work.finish(index, tag, st.hit, occluded);
@@ -303,6 +333,21 @@ namespace pt
                 }
             }
         }
+        if (ctr != nullptr)
+        {
+            unsigned long long v = visits, t = tests;
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+                t += __shfl_down_sync(0xFFFFFFFFu, t, o);
+            }
+            if (lane == 0)
+            {
+                atomicAdd(&ctr->nodeVisits[ANY ? 1 : 0], v);
+                atomicAdd(&ctr->triTests[ANY ? 1 : 0], t);
+            }
+        }
+        phase_end(ctr, Work::kPhase);
     }
 
     // ------------------------------------------------------------------ paths
@@ -337,7 +382,7 @@ namespace pt
                                                uint32_t queue, uint32_t position)
     {
         curandStatePhilox4_32_10_t rng;
-        curand_init(kRandomSeed, static_cast<unsigned long long>(sample), 0ull, &rng);
+        curand_init(kRandomSeed, static_cast<unsigned long long>(sample) + job.rngOffset, 0ull, &rng);
         const float4 r = curand_uniform4(&rng);
         float3 o, d;
         camera_ray(job, sample, make_float2(r.x, r.y), o, d);
@@ -367,6 +412,17 @@ namespace pt
         c->launched = gen;
         c->raysTraced = 0;
         c->shadowRaysTraced = 0;
+        for (int p = 0; p < 4; p++)
+        {
+            c->tStart[p] = ~0ull;
+            c->tEnd[p] = 0;
+            c->tAccum[p] = 0;
+        }
+        for (int k = 0; k < 2; k++)
+        {
+            c->nodeVisits[k] = 0;
+            c->triTests[k] = 0;
+        }
     }
 
     __global__ void generate_kernel(Wavefront wf, const JobView* jobPtr)
@@ -762,6 +818,7 @@ namespace pt
     __global__ void __launch_bounds__(128) shade_kernel(SceneView sc, Wavefront wf, const JobView* jobPtr)
     {
         Counters* ctr = wf.ctr;
+        phase_begin(ctr, 1);
         const uint32_t n = ctr->matCount[MODEL];
         const uint32_t cur = ctr->cur;
         const uint32_t nxt = cur ^ 1u;
@@ -822,7 +879,8 @@ namespace pt
                 const MaterialDev& m = sc.materials[s.material];
                 const Frame f = shading_frame(s, m);
                 curandStatePhilox4_32_10_t rng;
-                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]), static_cast<unsigned long long>(rngPos), &rng);
+                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + jobPtr->rngOffset,
+                            static_cast<unsigned long long>(rngPos), &rng);
                 if (MODEL == 1)  // Diffuse (:311-350, :270-309)
                 {
                     const float3 albedo = mat3(m.color);
@@ -918,6 +976,7 @@ namespace pt
             }
             (void)hitPos;
         }
+        phase_end(ctr, 1);
     }
 
     // Finished paths write their radiance to the per-sample buffer; the first
@@ -926,6 +985,7 @@ namespace pt
     __global__ void regen_kernel(Wavefront wf, const JobView* jobPtr)
     {
         Counters* ctr = wf.ctr;
+        phase_begin(ctr, 3);
         const uint32_t n = ctr->regenCount;
         const unsigned long long launched = ctr->launched;
         const unsigned long long total = jobPtr->totalSamples;
@@ -946,6 +1006,7 @@ namespace pt
             if (k < regenerate)
                 start_path(*jobPtr, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
         }
+        phase_end(ctr, 3);
     }
 
     __global__ void advance_kernel(Wavefront wf, const JobView* jobPtr, cudaGraphConditionalHandle handle)
@@ -966,6 +1027,12 @@ namespace pt
         }
         c->raysTraced += c->rayCount[cur];
         c->shadowRaysTraced += c->shadowCount;
+        for (int p = 0; p < 4; p++)
+        {
+            if (c->tEnd[p] > c->tStart[p] && c->tStart[p] != ~0ull) c->tAccum[p] += c->tEnd[p] - c->tStart[p];
+            c->tStart[p] = ~0ull;
+            c->tEnd[p] = 0;
+        }
         c->launched += regenerate;
         c->rayCount[cur] = 0;
         c->rayCount[nxt] = next;
@@ -977,7 +1044,12 @@ namespace pt
         c->shadowCursor = 0;
         c->iteration += 1;
         const bool cancelled = wf.cancel != nullptr && *wf.cancel != 0u;
-        c->done = (next == 0 || cancelled) ? 1u : 0u;
+        // Every path ends within depthLimit iterations, so the frame needs at most
+        // depthLimit * (ceil(samples / pool) + 2) iterations; the cap turns a logic error
+        // into an error flag instead of an endless device loop.
+        const bool capped = c->iteration >= jobPtr->maxIterations;
+        if (capped && next != 0) c->errorFlags |= kErrIterationCap;
+        c->done = (next == 0 || cancelled || capped) ? 1u : 0u;
         if (wf.progress != nullptr)
         {
             wf.progress[0] = c->launched;

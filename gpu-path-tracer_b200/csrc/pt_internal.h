@@ -77,9 +77,10 @@ namespace pt
     {
         float camera[12];         // origin, lowerLeftCorner, horizontal, vertical
         uint32_t width, height, spp, spa;
-        uint32_t depthLimit, nee, pad0, pad1;
+        uint32_t depthLimit, nee, maxIterations, pad1;   // maxIterations: hard cap of the device loop
         uint64_t totalSamples;
         float* sampleRadiance;    // [totalSamples][3]
+        uint64_t rngOffset;       // added to the sample index to form the Philox subsequence
     };
 
     // Device-resident frame control block. One thread (advance kernel) mutates it
@@ -99,6 +100,15 @@ namespace pt
         unsigned long long launched;
         unsigned long long raysTraced;
         unsigned long long shadowRaysTraced;
+        // Device time of each kernel phase: first-block start and last-block end (%globaltimer, ns)
+        // of the current launch, summed over iterations by the advance kernel.
+        // Phases: 0 closest-hit traversal, 1 shading (all models), 2 shadow traversal, 3 regeneration.
+        unsigned long long tStart[4];
+        unsigned long long tEnd[4];
+        unsigned long long tAccum[4];
+        // Traversal work: BVH8 node visits and triangle tests; [0] closest hit, [1] shadow rays.
+        unsigned long long nodeVisits[2];
+        unsigned long long triTests[2];
     };
 
     struct Wavefront
@@ -126,5 +136,6 @@ namespace pt
     {
         kErrStackOverflow = 1u,
         kErrQueueOverflow = 2u,
+        kErrIterationCap = 4u,
     };
 }

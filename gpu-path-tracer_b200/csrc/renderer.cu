@@ -479,6 +479,9 @@ namespace pt
             jv.nee = c.nee;
             jv.totalSamples = c.totalSamples;
             jv.sampleRadiance = sampleRadiance_.get<float>();
+            jv.rngOffset = s.rng_offset;
+            const uint64_t rounds = (c.totalSamples + c.pool - 1) / c.pool;
+            jv.maxIterations = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(c.depth) * (rounds + 2) + 64));
             hostJob_ = jv;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(job_.get<void>(), &hostJob_, sizeof(JobView), cudaMemcpyHostToDevice, stream_));
             if (!graphExec_ || graphKey_ != key(c)) PT_TRY(buildGraph(c));
@@ -498,11 +501,22 @@ namespace pt
             lastIterations_ = ctr.iteration;
             if (stats)
             {
+                *stats = gpt_frame_stats{};
                 stats->iterations = ctr.iteration;
+                uint32_t models = 0;
+                for (uint32_t m = 0; m < kModelCount; m++) models += scene_->modelPresent[m] ? 1u : 0u;
+                const uint32_t perIteration = 1u + models + (c.nee && scene_->lightCount ? 1u : 0u) + 2u;
+                stats->kernel_launches = 2u + ctr.iteration * perIteration + 1u;
                 stats->samples = ctr.launched;
                 stats->rays = ctr.raysTraced;
                 stats->shadow_rays = ctr.shadowRaysTraced;
+                for (int k = 0; k < 2; k++)
+                {
+                    stats->node_visits[k] = ctr.nodeVisits[k];
+                    stats->triangle_tests[k] = ctr.triTests[k];
+                }
                 stats->device_ms = ms;
+                for (int p = 0; p < 4; p++) stats->phase_ms[p] = static_cast<float>(static_cast<double>(ctr.tAccum[p]) * 1e-6);
             }
             return Status::Ok();
         }

@@ -99,17 +99,22 @@ typedef struct gpt_render_settings {
     uint32_t use_nee;             /* next-event estimation */
     uint32_t pool_size;           /* path slots; 0 = 1,048,576 (PathTracerDefaults.hpp:9) */
     uint64_t max_samples;         /* 0 = the whole frame; else render only sample indices [0, max_samples) */
-    uint32_t trace_block;         /* 0 = autotuned/default threads per block of the traversal kernels */
+    uint32_t trace_block;         /* 0 = default threads per block of the traversal kernels (64 or 128) */
     uint32_t trace_refill;        /* 0 = default; idle lanes a warp waits for before fetching new rays */
+    uint64_t rng_offset;          /* added to every sample index to form its Philox subsequence (0 = the reference's streams) */
 } gpt_render_settings;
 
 typedef struct gpt_frame_stats {
     uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */
-    uint32_t reserved;
+    uint32_t kernel_launches;     /* kernels the frame graph launched */
     uint64_t samples;             /* paths rendered */
     uint64_t rays;                /* extension + camera rays traced (closest hit) */
     uint64_t shadow_rays;         /* NEE shadow rays traced (any hit) */
-    float device_ms;              /* CUDA-event time of the frame on the render stream */
+    uint64_t node_visits[2];      /* BVH8 nodes visited: [0] closest-hit, [1] shadow traversal */
+    uint64_t triangle_tests[2];   /* triangles tested:   [0] closest-hit, [1] shadow traversal */
+    float device_ms;              /* CUDA-event time of the frame graph on the render stream */
+    float phase_ms[4];            /* device time per phase, summed over iterations: closest-hit traversal,
+                                     shading (all models), shadow traversal, regeneration */
     float reserved_f;
 } gpt_frame_stats;
 
