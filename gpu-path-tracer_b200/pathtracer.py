@@ -106,6 +106,7 @@ _SIGNATURES = [
     ("gpt_bvh8_check", ctypes.c_int, [ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(ctypes.c_uint64)]),
+    ("gpt_build_alias_table_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
     ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
                                               ctypes.POINTER(gpt_device_camera)]),
 ]
@@ -336,6 +337,12 @@ def bvh8_check(scene) -> dict:
     if rc != 0:
         raise GptError(rc, "gpt_bvh8_check")
     return dict(nodes=n.value, depth=d.value, violations=v.value, misplaced=m.value)
+
+
+def build_alias_table_noalloc(weights_dev, bins_dev, stream=None) -> int:
+    """Allocation-free alias-table build on device tensors (float32 weights [n], int32 bins [n, 4])."""
+    return lib().gpt_build_alias_table_noalloc(ctypes.c_void_p(weights_dev.data_ptr()), weights_dev.shape[0],
+                                                ctypes.c_void_p(bins_dev.data_ptr()), ctypes.c_void_p(stream))
 
 
 def make_device_camera(fov_y: float, aspect: float, position, quat_wxyz) -> np.ndarray:

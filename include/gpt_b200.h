@@ -209,6 +209,24 @@ int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count)
 int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* depth,
                    uint64_t* containment_violations, uint64_t* misplaced_triangles);
 
+/*
+ * Allocation-free alias-table build. This entry point has no counterpart in the reference; it
+ * exists for callers that must not allocate device memory when they build a light sampler
+ * (a fixed per-frame memory budget, an engine that owns every allocation through its own pool,
+ * or code that cannot afford cudaMalloc/cudaFree stalls, since cudaFree synchronises the device).
+ * It builds the same table as the scene upload (AliasTable.hpp:22-84 semantics: FP64 sum of the
+ * weights, p = w / sum, the reference's sequential pairing) from light_count float weights into
+ * bins ([light_count][4] uint32 = q, p, alias, value; 16-byte aligned). Both pointers are device
+ * memory; stream may be NULL (the legacy default stream); the call is asynchronous on it.
+ * Working memory is a fixed array of about 2 MiB compiled into the library, held by every GPU that
+ * loads it until the process exits; light_count above GPT_NOALLOC_MAX_LIGHTS returns
+ * GPT_ERR_CAPACITY. The first call on a device looks up that array's device address (set-up),
+ * so make the first call before any stream capture. All calls share the array: calls that can
+ * overlap on the GPU race and must be ordered by the caller.
+ */
+#define GPT_NOALLOC_MAX_LIGHTS 65536u
+int gpt_build_alias_table_noalloc(const float* weights, uint32_t light_count, uint32_t* bins, void* stream);
+
 /* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */
 int gpt_make_device_camera(float fov_y, float aspect, const gpt_motion_state* state, gpt_device_camera* out);
 
