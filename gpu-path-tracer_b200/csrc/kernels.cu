@@ -1009,7 +1009,7 @@ namespace pt
         phase_end(ctr, 3);
     }
 
-    __global__ void advance_kernel(Wavefront wf, const JobView* jobPtr, cudaGraphConditionalHandle handle)
+    __global__ void advance_kernel(Wavefront wf, const JobView* jobPtr, cudaGraphConditionalHandle handle, bool graphLoop)
     {
         Counters* c = wf.ctr;
         const uint32_t cur = c->cur;
@@ -1055,7 +1055,7 @@ namespace pt
             wf.progress[0] = c->launched;
             wf.progress[1] = c->iteration;
         }
-        cudaGraphSetConditional(handle, c->done ? 0u : 1u);
+        if (graphLoop) cudaGraphSetConditional(handle, c->done ? 0u : 1u);
     }
 
     // Per pixel: compensated (Kahan) FP32 sum of its samples in sample order, then
@@ -1317,8 +1317,10 @@ namespace pt
     {
         cudaError_t e;
         WavefrontClosest wc{L.scene, L.wf};
+        if (L.traceStart && (e = cudaEventRecord(L.traceStart, s)) != cudaSuccess) return e;
         e = launch_trace<false>(wc, L.scene.depth, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
+        if (L.traceStop && (e = cudaEventRecord(L.traceStop, s)) != cudaSuccess) return e;
         for (uint32_t m = 0; m < kModelCount; m++)
         {
             if (!L.modelPresent[m]) continue;
@@ -1341,7 +1343,7 @@ namespace pt
         }
         regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        advance_kernel<<<1, 1, 0, s>>>(L.wf, L.job, L.handle);
+        advance_kernel<<<1, 1, 0, s>>>(L.wf, L.job, L.handle, L.graphLoop);
         return cudaGetLastError();
     }
 

@@ -18,6 +18,9 @@ namespace pt
         int traceThreads;
         uint32_t refill;
         int shadeBlocks;
+        bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
+        cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
+        cudaEvent_t traceStop;
     };
 
     int trace_grid_blocks(int device, int threads, uint32_t depth);

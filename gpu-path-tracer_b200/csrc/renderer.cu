@@ -159,6 +159,8 @@ namespace pt
             StopRendering();
             releaseGraph();
             if (startEvent_) cudaEventDestroy(startEvent_);
+            if (traceStart_) cudaEventDestroy(traceStart_);
+            if (traceStop_) cudaEventDestroy(traceStop_);
             if (stopEvent_) cudaEventDestroy(stopEvent_);
             if (hostMapped_) cudaFreeHost(hostMapped_);
             if (stream_) cudaStreamDestroy(stream_);
@@ -429,6 +431,7 @@ namespace pt
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth);
             L.refill = c.refill;
             L.shadeBlocks = sms * 8;
+            L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             le = launch_iteration(L, stream_);
             ce = cudaStreamEndCapture(stream_, &body);
@@ -439,6 +442,52 @@ namespace pt
             cudaGraphDestroy(res);
             PT_CUDA("cudaGraphInstantiate", cudaGraphInstantiate(&graphExec_, graph_, 0));
             graphKey_ = key(c);
+            return Status::Ok();
+        }
+
+        // The reference's host-driven structure (Renderer.cpp:517-623): every kernel is an ordinary
+        // launch and the host reads the loop condition after each iteration. Used for per-kernel
+        // profiling (ncu cannot profile nodes of graphs with conditional nodes), for CUDA-event
+        // timing of the traversal kernel, and as the host-driven baseline of the graph loop.
+        Status hostLoop(const FrameConfig& c, uint32_t maxIterations, float& traceEventMs)
+        {
+            int sms = 0;
+            PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+            const SceneView sv = scene_->view();
+            const Wavefront wf = wavefront();
+            const JobView* jobDev = job_.get<JobView>();
+            if (!traceStart_) PT_CUDA("cudaEventCreate", cudaEventCreate(&traceStart_));
+            if (!traceStop_) PT_CUDA("cudaEventCreate", cudaEventCreate(&traceStop_));
+            IterationLaunch L{};
+            L.scene = sv;
+            L.wf = wf;
+            L.job = jobDev;
+            L.handle = 0;
+            for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = scene_->modelPresent[m];
+            L.nee = c.nee != 0;
+            L.traceThreads = c.traceThreads;
+            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth);
+            L.refill = c.refill;
+            L.shadeBlocks = sms * 8;
+            L.graphLoop = false;
+            L.traceStart = traceStart_;
+            L.traceStop = traceStop_;
+            volatile uint32_t* doneHost = reinterpret_cast<volatile uint32_t*>(static_cast<char*>(hostMapped_) + 32);
+            traceEventMs = 0.0f;
+            PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
+            PT_CUDA("prologue", launch_frame_prologue(wf, jobDev, c.pool, sms * 8, stream_));
+            for (uint32_t it = 0; it <= maxIterations; it++)
+            {
+                PT_CUDA("iteration", launch_iteration(L, stream_));
+                PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(const_cast<uint32_t*>(doneHost), &counters_.get<Counters>()->done, 4, cudaMemcpyDeviceToHost, stream_));
+                PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
+                float ms = 0.0f;
+                PT_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, traceStart_, traceStop_));
+                traceEventMs += ms;
+                if (*doneHost) break;
+            }
+            PT_CUDA("resolve", launch_resolve(jobDev, accumulation_.get<float4>(), framebuffer_.get<uint32_t>(), sms * 8, stream_));
+            PT_CUDA("cudaEventRecord", cudaEventRecord(stopEvent_, stream_));
             return Status::Ok();
         }
 
@@ -484,12 +533,18 @@ namespace pt
             jv.maxIterations = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(c.depth) * (rounds + 2) + 64));
             hostJob_ = jv;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(job_.get<void>(), &hostJob_, sizeof(JobView), cudaMemcpyHostToDevice, stream_));
-            if (!graphExec_ || graphKey_ != key(c)) PT_TRY(buildGraph(c));
             lastTotalSamples_ = c.totalSamples;
             lastPixels_ = static_cast<size_t>(c.width) * c.height;
-            PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
-            PT_CUDA("cudaGraphLaunch", cudaGraphLaunch(graphExec_, stream_));
-            PT_CUDA("cudaEventRecord", cudaEventRecord(stopEvent_, stream_));
+            float traceEventMs = 0.0f;
+            if (s.loop_mode == GPT_LOOP_HOST)
+                PT_TRY(hostLoop(c, jv.maxIterations, traceEventMs));
+            else
+            {
+                if (!graphExec_ || graphKey_ != key(c)) PT_TRY(buildGraph(c));
+                PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
+                PT_CUDA("cudaGraphLaunch", cudaGraphLaunch(graphExec_, stream_));
+                PT_CUDA("cudaEventRecord", cudaEventRecord(stopEvent_, stream_));
+            }
             Counters ctr{};
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&hostCounters_, counters_.get<void>(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
             if (copyToHost) PT_TRY(copyFrameToHost());
@@ -516,6 +571,7 @@ namespace pt
                     stats->triangle_tests[k] = ctr.triTests[k];
                 }
                 stats->device_ms = ms;
+                stats->trace_event_ms = traceEventMs;
                 for (int p = 0; p < 4; p++) stats->phase_ms[p] = static_cast<float>(static_cast<double>(ctr.tAccum[p]) * 1e-6);
             }
             return Status::Ok();
@@ -686,6 +742,7 @@ namespace pt
         int device_;
         cudaStream_t stream_ = nullptr;
         cudaEvent_t startEvent_ = nullptr, stopEvent_ = nullptr;
+        cudaEvent_t traceStart_ = nullptr, traceStop_ = nullptr;
         void* hostMapped_ = nullptr;
         void* hostMappedDev_ = nullptr;
         static constexpr uint32_t kDefaultPool = 1u << 20;

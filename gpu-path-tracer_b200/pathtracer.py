@@ -52,14 +52,16 @@ class gpt_render_settings(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("samples_per_pixel", ctypes.c_uint32),
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
-                ("rng_offset", ctypes.c_uint64)]
+                ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+LOOP_GRAPH, LOOP_HOST = 0, 1
 
 
 class gpt_frame_stats(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_uint32), ("kernel_launches", ctypes.c_uint32), ("samples", ctypes.c_uint64),
                 ("rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("node_visits", ctypes.c_uint64 * 2),
                 ("triangle_tests", ctypes.c_uint64 * 2), ("device_ms", ctypes.c_float), ("phase_ms", ctypes.c_float * 4),
-                ("reserved_f", ctypes.c_float)]
+                ("trace_event_ms", ctypes.c_float)]
 
 PHASES = ("trace", "shade", "shadow", "regen")
 
@@ -210,10 +212,10 @@ class Renderer:
 
     def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                     rng_offset: int = 0) -> dict:
+                     rng_offset: int = 0, loop_mode: int = LOOP_GRAPH) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
-                                 trace_refill, rng_offset)
+                                 trace_refill, rng_offset, loop_mode, 0)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")
@@ -224,7 +226,7 @@ class Renderer:
         return dict(iterations=stats.iterations, kernel_launches=stats.kernel_launches, samples=stats.samples,
                     rays=stats.rays, shadow_rays=stats.shadow_rays, node_visits=list(stats.node_visits),
                     triangle_tests=list(stats.triangle_tests), device_ms=stats.device_ms,
-                    phase_ms={k: stats.phase_ms[i] for i, k in enumerate(PHASES)})
+                    phase_ms={k: stats.phase_ms[i] for i, k in enumerate(PHASES)}, trace_event_ms=stats.trace_event_ms)
 
     def framebuffer(self) -> np.ndarray:
         out = np.zeros(self.width * self.height, dtype=np.uint32)

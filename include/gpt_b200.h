@@ -102,7 +102,14 @@ typedef struct gpt_render_settings {
     uint32_t trace_block;         /* 0 = default threads per block of the traversal kernels (64 or 128) */
     uint32_t trace_refill;        /* 0 = default; idle lanes a warp waits for before fetching new rays */
     uint64_t rng_offset;          /* added to every sample index to form its Philox subsequence (0 = the reference's streams) */
+    uint32_t loop_mode;           /* GPT_LOOP_GRAPH (default): the whole frame is one CUDA graph whose conditional WHILE
+                                     node repeats the iteration on the device; GPT_LOOP_HOST: the host launches each
+                                     iteration and reads the loop condition after it (the reference's structure) */
+    uint32_t reserved;
 } gpt_render_settings;
+
+#define GPT_LOOP_GRAPH 0u
+#define GPT_LOOP_HOST 1u
 
 typedef struct gpt_frame_stats {
     uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */
@@ -115,7 +122,7 @@ typedef struct gpt_frame_stats {
     float device_ms;              /* CUDA-event time of the frame graph on the render stream */
     float phase_ms[4];            /* device time per phase, summed over iterations: closest-hit traversal,
                                      shading (all models), shadow traversal, regeneration */
-    float reserved_f;
+    float trace_event_ms;         /* GPT_LOOP_HOST only: CUDA-event time of the closest-hit traversal launches */
 } gpt_frame_stats;
 
 typedef struct gpt_renderer gpt_renderer;

@@ -235,3 +235,20 @@ def test_simulation_thread_frames_stop_resume(gpu_renderer, scene_factory):
     assert not gpu_renderer.is_rendering()
     assert gpu_renderer.progress()["done_frames"] < 12
     assert gpu_renderer.last_error() is None
+
+
+def test_host_loop_matches_graph_loop(gpu_renderer, scene_factory, oracle_scene):
+    """The host-driven iteration loop (the reference's structure) and the device-driven graph
+    loop run the same kernels: identical per-sample radiance and queue counts."""
+    import pathtracer as P
+    s = scene_factory("cornell-all")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 64, 64)
+    a = gpu_renderer.render_frame(cam, 64, 64, 16, 10, True, pool_size=9000, loop_mode=P.LOOP_GRAPH)
+    rad_a, log_a = gpu_renderer.sample_radiance(), gpu_renderer.queue_log()
+    b = gpu_renderer.render_frame(cam, 64, 64, 16, 10, True, pool_size=9000, loop_mode=P.LOOP_HOST)
+    rad_b, log_b = gpu_renderer.sample_radiance(), gpu_renderer.queue_log()
+    assert a["iterations"] == b["iterations"]
+    assert np.array_equal(log_a, log_b)
+    assert np.array_equal(rad_a.view(np.uint32), rad_b.view(np.uint32))
+    assert b["trace_event_ms"] > 0.0
