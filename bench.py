@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--pool", type=int, default=WORKLOAD["pool"])
+    ap.add_argument("--pool", type=int, default=0, help="path slots; 0 = autotuned")
+    ap.add_argument("--no-autotune", action="store_true", help="use the library defaults instead of gpt_autotune")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target CPU time of the bounded CPU sample")
     ap.add_argument("--loop", default="graph", choices=["graph", "host"],
@@ -212,10 +213,17 @@ def b200_arm(args):
     accum = torch.zeros((W * H, 4), dtype=torch.float32, device="cuda") if world > 1 else None
 
     loop_mode = pathtracer.LOOP_HOST if args.loop == "host" else pathtracer.LOOP_GRAPH
+    tuned = {}
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        tuned = renderer.autotune(cam, W, H, spp, depth, True)
+        tuned["seconds"] = time.perf_counter() - t0
+    knobs = dict(pool_size=args.pool or tuned.get("pool_size", WORKLOAD["pool"]),
+                 trace_occupancy=tuned.get("trace_occupancy", 0), trace_refill=tuned.get("trace_refill", 0),
+                 trace_block=tuned.get("trace_block", 0))
 
     def step():
-        st = renderer.render_frame(cam, W, H, spp, depth, True, pool_size=args.pool, rng_offset=rng_offset,
-                                   loop_mode=loop_mode)
+        st = renderer.render_frame(cam, W, H, spp, depth, True, rng_offset=rng_offset, loop_mode=loop_mode, **knobs)
         if world > 1:
             host = renderer.accumulation()
             accum.copy_(torch.from_numpy(host))
@@ -240,8 +248,7 @@ def b200_arm(args):
     clocks = sampler.stop()
     # CUDA-event timing of the closest-hit traversal launches: one more frame of the same workload
     # with host-launched iterations (events cannot bracket a node inside the graph's WHILE loop).
-    ev = renderer.render_frame(cam, W, H, spp, depth, True, pool_size=args.pool, rng_offset=rng_offset,
-                               loop_mode=pathtracer.LOOP_HOST)
+    ev = renderer.render_frame(cam, W, H, spp, depth, True, rng_offset=rng_offset, loop_mode=pathtracer.LOOP_HOST, **knobs)
 
     device_s = sum(s["device_ms"] for s in stats) / 1000.0
     if dist:
@@ -278,7 +285,7 @@ def b200_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD["workload"], "triangles": info["triangles"], "bvh8_nodes": info["nodes"],
                    "bvh8_depth": info["depth"], "lights": info["lights"], "resolution": f"{W}x{H}", "spp": spp,
-                   "depth": depth, "nee": True, "pool": args.pool,
+                   "depth": depth, "nee": True, "pool": knobs["pool_size"], "knobs": knobs, "autotune": tuned,
                    "l2": "inputs larger than L2 (1.31M-triangle scene, 189 MB shading records, 1.6 GB per-sample radiance)",
                    "parallelism": f"{world} independent frames (distinct Philox subsequences) + NCCL all-reduce of the accumulation" if world > 1 else "1 GPU"},
         "mrays_per_second": (rays + shadow) * world / device_s / 1e6,

@@ -268,8 +268,8 @@ namespace pt
     // idle the warp takes that many new rays with one atomic (ballot + popc + shuffle), so lanes
     // that finished early are refilled instead of idling until the slowest ray of the warp ends.
     // Traversal stack: STACK entries per thread in shared memory, entry = node << 8 | child mask.
-    template <int STACK, bool ANY, class Work>
-    __global__ void __launch_bounds__(128) trace_kernel(Work work, uint32_t refill, uint32_t* errorFlags)
+    template <int STACK, bool ANY, int MINB, class Work>
+    __global__ void __launch_bounds__(128, MINB) trace_kernel(Work work, uint32_t refill, uint32_t* errorFlags)
     {
         extern __shared__ uint32_t smem[];
         uint32_t* stack = smem + threadIdx.x;
@@ -1280,35 +1280,62 @@ namespace pt
     // ------------------------------------------------------------------ host launchers
     namespace
     {
-        template <int STACK, bool ANY, class Work>
+        // Traversal kernel variants: stack capacity (>= BVH8 depth) x occupancy target. MINB is the
+        // minimum resident 128-thread blocks per SM the compiler must allow (1 = registers unconstrained,
+        // 10 = <= 48 registers, 12 = <= 40 registers); the best one is measured, not assumed.
+        template <int STACK, bool ANY, int MINB, class Work>
         cudaError_t launch_trace_t(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
         {
             const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
-            trace_kernel<STACK, ANY, Work><<<blocks, threads, smem, s>>>(w, refill, err);
+            trace_kernel<STACK, ANY, MINB, Work><<<blocks, threads, smem, s>>>(w, refill, err);
             return cudaGetLastError();
         }
 
-        template <bool ANY, class Work>
-        cudaError_t launch_trace(const Work& w, uint32_t depth, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
+        template <int STACK, bool ANY, class Work>
+        cudaError_t launch_trace_m(const Work& w, int occupancy, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
         {
-            if (depth <= 8) return launch_trace_t<8, ANY>(w, blocks, threads, refill, err, s);
-            if (depth <= 16) return launch_trace_t<16, ANY>(w, blocks, threads, refill, err, s);
-            if (depth <= 32) return launch_trace_t<32, ANY>(w, blocks, threads, refill, err, s);
-            return launch_trace_t<64, ANY>(w, blocks, threads, refill, err, s);
+            if (occupancy >= 12) return launch_trace_t<STACK, ANY, 12>(w, blocks, threads, refill, err, s);
+            if (occupancy >= 10) return launch_trace_t<STACK, ANY, 10>(w, blocks, threads, refill, err, s);
+            return launch_trace_t<STACK, ANY, 1>(w, blocks, threads, refill, err, s);
+        }
+
+        template <bool ANY, class Work>
+        cudaError_t launch_trace(const Work& w, uint32_t depth, int occupancy, int blocks, int threads, uint32_t refill, uint32_t* err,
+                                 cudaStream_t s)
+        {
+            if (depth <= 8) return launch_trace_m<8, ANY>(w, occupancy, blocks, threads, refill, err, s);
+            if (depth <= 16) return launch_trace_m<16, ANY>(w, occupancy, blocks, threads, refill, err, s);
+            if (depth <= 32) return launch_trace_m<32, ANY>(w, occupancy, blocks, threads, refill, err, s);
+            return launch_trace_m<64, ANY>(w, occupancy, blocks, threads, refill, err, s);
+        }
+
+        template <int STACK, int MINB>
+        int resident_blocks(int threads)
+        {
+            int perSm = 0;
+            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<STACK, false, MINB, WavefrontClosest>, threads, smem);
+            return perSm;
+        }
+
+        template <int STACK>
+        int resident_blocks_m(int occupancy, int threads)
+        {
+            if (occupancy >= 12) return resident_blocks<STACK, 12>(threads);
+            if (occupancy >= 10) return resident_blocks<STACK, 10>(threads);
+            return resident_blocks<STACK, 1>(threads);
         }
     }
 
-    int trace_grid_blocks(int device, int threads, uint32_t depth)
+    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy)
     {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        int perSm = 0;
-        const int stack = depth <= 8 ? 8 : depth <= 16 ? 16 : depth <= 32 ? 32 : 64;
-        const size_t smem = static_cast<size_t>(stack) * threads * sizeof(uint32_t);
-        if (depth <= 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<8, false, WavefrontClosest>, threads, smem);
-        else if (depth <= 16) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<16, false, WavefrontClosest>, threads, smem);
-        else if (depth <= 32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<32, false, WavefrontClosest>, threads, smem);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<64, false, WavefrontClosest>, threads, smem);
+        int perSm;
+        if (depth <= 8) perSm = resident_blocks_m<8>(occupancy, threads);
+        else if (depth <= 16) perSm = resident_blocks_m<16>(occupancy, threads);
+        else if (depth <= 32) perSm = resident_blocks_m<32>(occupancy, threads);
+        else perSm = resident_blocks_m<64>(occupancy, threads);
         if (perSm < 1) perSm = 1;
         return sms * perSm;
     }
@@ -1318,7 +1345,7 @@ namespace pt
         cudaError_t e;
         WavefrontClosest wc{L.scene, L.wf};
         if (L.traceStart && (e = cudaEventRecord(L.traceStart, s)) != cudaSuccess) return e;
-        e = launch_trace<false>(wc, L.scene.depth, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+        e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
         if (L.traceStop && (e = cudaEventRecord(L.traceStop, s)) != cudaSuccess) return e;
         for (uint32_t m = 0; m < kModelCount; m++)
@@ -1338,7 +1365,7 @@ namespace pt
         if (L.nee && L.scene.lightCount > 0)
         {
             WavefrontShadow ws{L.scene, L.wf};
-            e = launch_trace<true>(ws, L.scene.depth, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
         regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
@@ -1373,8 +1400,8 @@ namespace pt
                                    uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s)
     {
         BatchRays b{sc, rays, n, cursor, triOut, uvtOut, occOut};
-        if (occOut) return launch_trace<true>(b, sc.depth, blocks, threads, 32, errorFlags, s);
-        return launch_trace<false>(b, sc.depth, blocks, threads, 32, errorFlags, s);
+        if (occOut) return launch_trace<true>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
+        return launch_trace<false>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
     }
 
     cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,

@@ -17,13 +17,14 @@ namespace pt
         int traceBlocks;
         int traceThreads;
         uint32_t refill;
+        int occupancy;             // traversal kernel variant: 1, 10 or 12 resident blocks per SM targeted
         int shadeBlocks;
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
         cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
         cudaEvent_t traceStop;
     };
 
-    int trace_grid_blocks(int device, int threads, uint32_t depth);
+    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy);
     cudaError_t launch_iteration(const IterationLaunch& launch, cudaStream_t stream);
     cudaError_t launch_frame_prologue(const Wavefront& wf, const JobView* job, uint32_t pool, int blocks, cudaStream_t stream);
     cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t stream);

@@ -356,6 +356,7 @@ namespace pt
             uint64_t totalSamples;
             int traceThreads;
             uint32_t refill;
+            int occupancy;
         };
 
         Status resolveConfig(const gpt_render_settings& s, FrameConfig& c) const
@@ -376,6 +377,7 @@ namespace pt
             c.traceThreads = s.trace_block ? static_cast<int>(s.trace_block) : 128;
             if (c.traceThreads != 64 && c.traceThreads != 128) c.traceThreads = 128;
             c.refill = s.trace_refill ? std::min(32u, std::max(1u, s.trace_refill)) : 16u;
+            c.occupancy = s.trace_occupancy == 0 ? 10 : (s.trace_occupancy >= 12 ? 12 : (s.trace_occupancy >= 10 ? 10 : 1));
             return Status::Ok();
         }
 
@@ -428,7 +430,8 @@ namespace pt
             for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = scene_->modelPresent[m];
             L.nee = c.nee != 0;
             L.traceThreads = c.traceThreads;
-            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth);
+            L.occupancy = c.occupancy;
+            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy);
             L.refill = c.refill;
             L.shadeBlocks = sms * 8;
             L.graphLoop = true;
@@ -466,7 +469,8 @@ namespace pt
             for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = scene_->modelPresent[m];
             L.nee = c.nee != 0;
             L.traceThreads = c.traceThreads;
-            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth);
+            L.occupancy = c.occupancy;
+            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy);
             L.refill = c.refill;
             L.shadeBlocks = sms * 8;
             L.graphLoop = false;
@@ -494,8 +498,8 @@ namespace pt
         std::string key(const FrameConfig& c) const
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool, c.nee,
-                          c.traceThreads, c.refill, width_, height_, static_cast<void*>(accumulation_.get<void>()),
+            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool, c.nee,
+                          c.traceThreads, c.refill, c.occupancy, width_, height_, static_cast<void*>(accumulation_.get<void>()),
                           static_cast<void*>(framebuffer_.get<void>()));
             return buf;
         }
@@ -577,6 +581,61 @@ namespace pt
             return Status::Ok();
         }
 
+        // Measured choice of the frame's tuning knobs for a workload: every candidate renders the
+        // same reduced frame (the whole image at min(spp, 4) samples per pixel, so all of the scene
+        // is represented) twice, and the fastest device time wins. Results do not depend on the
+        // knobs; only speed does.
+        Status Autotune(const gpt_device_camera& cam, const gpt_render_settings& base, gpt_render_settings& best, float& bestMs,
+                        uint32_t& tried)
+        {
+            if (!scene_) return Status::Err(GPT_ERR_NO_SCENE, "No scene has been uploaded");
+            gpt_render_settings trial = base;
+            trial.samples_per_pixel = std::min<uint32_t>(std::max(base.samples_per_pixel, 1u), 4u);
+            trial.max_samples = 0;
+            trial.loop_mode = GPT_LOOP_GRAPH;
+            const uint64_t pixels = static_cast<uint64_t>(std::max(base.width, 1u)) * std::max(base.height, 1u);
+            const uint32_t pools[] = {1u << 20, 2u << 20, 4u << 20, 8u << 20};
+            const uint32_t occupancies[] = {1u, 10u, 12u};
+            const uint32_t refills[] = {8u, 16u};
+            const uint32_t blocks[] = {64u, 128u};
+            best = base;
+            bestMs = 1e30f;
+            tried = 0;
+            // the frame's own sample count bounds the useful pool size
+            const uint64_t frameSamples = pixels * std::max(base.samples_per_pixel, 1u);
+            for (uint32_t pool : pools)
+            {
+                if (pool > 2 * frameSamples && pool != pools[0]) continue;
+                for (uint32_t occ : occupancies)
+                    for (uint32_t refill : refills)
+                        for (uint32_t tb : blocks)
+                        {
+                            trial.pool_size = pool;
+                            trial.trace_occupancy = occ;
+                            trial.trace_refill = refill;
+                            trial.trace_block = tb;
+                            float ms = 1e30f;
+                            for (int rep = 0; rep < 2; rep++)
+                            {
+                                gpt_frame_stats st{};
+                                PT_TRY(RenderFrame(cam, trial, &st, false));
+                                if (rep) ms = st.device_ms;
+                            }
+                            tried++;
+                            if (ms < bestMs)
+                            {
+                                bestMs = ms;
+                                best = base;
+                                best.pool_size = pool;
+                                best.trace_occupancy = occ;
+                                best.trace_refill = refill;
+                                best.trace_block = tb;
+                            }
+                        }
+            }
+            return Status::Ok();
+        }
+
         Status copyFrameToHost()
         {
             std::scoped_lock lock(frameMutex_);
@@ -605,7 +664,7 @@ namespace pt
             uint32_t* cursor = cursor_.get<uint32_t>();
             PT_CUDA("cudaMemsetAsync", cudaMemsetAsync(cursor, 0, 8, st));
             const SceneView sv = scene_->view();
-            const int blocks = trace_grid_blocks(device_, 128, sv.depth);
+            const int blocks = trace_grid_blocks(device_, 128, sv.depth, 1);
             PT_CUDA("intersect", launch_batch_trace(sv, rays, n, cursor, tri, uvt, occ, blocks, 128, cursor + 1, st));
             uint32_t err = 0;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&err, cursor + 1, 4, cudaMemcpyDeviceToHost, st));
@@ -1022,6 +1081,19 @@ extern "C"
             return GPT_ERR_INVALID_ARGUMENT;
         }
         return GPT_OK;
+    }
+
+    int gpt_autotune(gpt_renderer* r, const gpt_device_camera* camera, const gpt_render_settings* base, gpt_render_settings* best,
+                     float* best_ms, uint32_t* candidates)
+    {
+        if (!r || !camera || !base || !best) return GPT_ERR_INVALID_ARGUMENT;
+        if (r->impl->rendering_.load()) return Report(r, pt::Status::Err(GPT_ERR_STATE, "Renderer is already rendering"));
+        float ms = 0.0f;
+        uint32_t tried = 0;
+        const int rc = Report(r, r->impl->Autotune(*camera, *base, *best, ms, tried));
+        if (best_ms) *best_ms = ms;
+        if (candidates) *candidates = tried;
+        return rc;
     }
 
     // MakeDeviceCamera (Renderer.cpp:237-257) with glm's quaternion rotation v + 2w(q x v) + 2 q x (q x v),

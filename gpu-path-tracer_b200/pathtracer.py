@@ -52,7 +52,7 @@ class gpt_render_settings(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("samples_per_pixel", ctypes.c_uint32),
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
-                ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32)]
 
 LOOP_GRAPH, LOOP_HOST = 0, 1
 
@@ -93,6 +93,9 @@ _SIGNATURES = [
     ("gpt_consume_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     ("gpt_render_frame", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_device_camera),
                                         ctypes.POINTER(gpt_render_settings), ctypes.POINTER(gpt_frame_stats)]),
+    ("gpt_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_device_camera), ctypes.POINTER(gpt_render_settings),
+                                    ctypes.POINTER(gpt_render_settings), ctypes.POINTER(ctypes.c_float),
+                                    ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_read_framebuffer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_accumulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_sample_radiance", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
@@ -212,10 +215,10 @@ class Renderer:
 
     def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                     rng_offset: int = 0, loop_mode: int = LOOP_GRAPH) -> dict:
+                     rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
-                                 trace_refill, rng_offset, loop_mode, 0)
+                                 trace_refill, rng_offset, loop_mode, trace_occupancy)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")
@@ -227,6 +230,18 @@ class Renderer:
                     rays=stats.rays, shadow_rays=stats.shadow_rays, node_visits=list(stats.node_visits),
                     triangle_tests=list(stats.triangle_tests), device_ms=stats.device_ms,
                     phase_ms={k: stats.phase_ms[i] for i, k in enumerate(PHASES)}, trace_event_ms=stats.trace_event_ms)
+
+    def autotune(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True) -> dict:
+        """Measured tuning knobs for this workload: pool_size, trace_occupancy, trace_refill, trace_block."""
+        cam = camera_struct(camera12)
+        base = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, 0, 0, 0, 0, 0, LOOP_GRAPH, 0)
+        best = gpt_render_settings()
+        ms = ctypes.c_float()
+        n = ctypes.c_uint32()
+        self._check(self.L.gpt_autotune(self.h, ctypes.byref(cam), ctypes.byref(base), ctypes.byref(best), ctypes.byref(ms),
+                                        ctypes.byref(n)), "gpt_autotune")
+        return dict(pool_size=best.pool_size, trace_occupancy=best.trace_occupancy, trace_refill=best.trace_refill,
+                    trace_block=best.trace_block, trial_ms=ms.value, candidates=n.value)
 
     def framebuffer(self) -> np.ndarray:
         out = np.zeros(self.width * self.height, dtype=np.uint32)

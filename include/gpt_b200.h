@@ -105,7 +105,8 @@ typedef struct gpt_render_settings {
     uint32_t loop_mode;           /* GPT_LOOP_GRAPH (default): the whole frame is one CUDA graph whose conditional WHILE
                                      node repeats the iteration on the device; GPT_LOOP_HOST: the host launches each
                                      iteration and reads the loop condition after it (the reference's structure) */
-    uint32_t reserved;
+    uint32_t trace_occupancy;     /* traversal kernel variant: 0/1 = registers unconstrained, 10 or 12 = that many
+                                     resident 128-thread blocks per SM targeted (fewer registers, more warps) */
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
@@ -178,6 +179,17 @@ int gpt_consume_last_error(gpt_renderer* renderer, char* buffer, size_t length);
  */
 int gpt_render_frame(gpt_renderer* renderer, const gpt_device_camera* camera,
                      const gpt_render_settings* settings, gpt_frame_stats* stats);
+/*
+ * Autotuner: measures the frame's tuning knobs (pool_size = path slots and queue capacities,
+ * trace_occupancy, trace_refill, trace_block) on a reduced frame of the same workload (whole
+ * image, min(spp, 4) samples per pixel) and writes the fastest combination into *best (the other
+ * fields copied from *base). Results of a frame do not depend on these knobs, only its speed.
+ * No counterpart in the reference, whose launch shapes are compile-time constants
+ * (Kernels/LaunchUtils.cuh:7-17, PathTracerDefaults.hpp:9).
+ */
+int gpt_autotune(gpt_renderer* renderer, const gpt_device_camera* camera, const gpt_render_settings* base,
+                 gpt_render_settings* best, float* best_ms, uint32_t* candidates);
+
 /* Copies of the last frame's results to host memory. */
 int gpt_read_framebuffer(gpt_renderer* renderer, uint32_t* rgba, size_t pixel_count);
 int gpt_read_accumulation(gpt_renderer* renderer, float* rgba32f, size_t pixel_count);

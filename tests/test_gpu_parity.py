@@ -252,3 +252,19 @@ def test_host_loop_matches_graph_loop(gpu_renderer, scene_factory, oracle_scene)
     assert np.array_equal(log_a, log_b)
     assert np.array_equal(rad_a.view(np.uint32), rad_b.view(np.uint32))
     assert b["trace_event_ms"] > 0.0
+
+
+def test_autotune_returns_valid_knobs_and_results_do_not_change(gpu_renderer, scene_factory):
+    s = scene_factory("spheres-small")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 128, 96)
+    knobs = gpu_renderer.autotune(cam, 128, 96, 16, 12, True)
+    assert knobs["candidates"] >= 12 and knobs["trial_ms"] > 0
+    assert knobs["pool_size"] in (1 << 20, 2 << 20, 4 << 20, 8 << 20)
+    assert knobs["trace_occupancy"] in (1, 10, 12) and knobs["trace_refill"] in (8, 16) and knobs["trace_block"] in (64, 128)
+    gpu_renderer.render_frame(cam, 128, 96, 16, 12, True)
+    a = gpu_renderer.sample_radiance()
+    gpu_renderer.render_frame(cam, 128, 96, 16, 12, True, pool_size=knobs["pool_size"], trace_occupancy=knobs["trace_occupancy"],
+                              trace_refill=knobs["trace_refill"], trace_block=knobs["trace_block"])
+    b = gpu_renderer.sample_radiance()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
