@@ -208,8 +208,9 @@ def b200_arm(args):
     upload_s = time.perf_counter() - t0
     info = renderer.scene_info()
     cam = scenes.scene_camera(scene, W, H)
+    import multigpu
     samples_per_frame = spp * W * H
-    rng_offset = rank * samples_per_frame
+    rng_offset = multigpu.rank_rng_offset(rank, samples_per_frame)
     accum = torch.zeros((W * H, 4), dtype=torch.float32, device="cuda") if world > 1 else None
 
     loop_mode = pathtracer.LOOP_HOST if args.loop == "host" else pathtracer.LOOP_GRAPH
@@ -227,7 +228,7 @@ def b200_arm(args):
         if world > 1:
             host = renderer.accumulation()
             accum.copy_(torch.from_numpy(host))
-            dist.all_reduce(accum)
+            multigpu.combine_accumulation(accum, dist)
         return st
 
     for _ in range(args.warmup):
@@ -252,9 +253,7 @@ def b200_arm(args):
 
     device_s = sum(s["device_ms"] for s in stats) / 1000.0
     if dist:
-        t = torch.tensor([device_s, wall], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        device_s, wall = float(t[0]), float(t[1])
+        device_s, wall = multigpu.max_over_ranks([device_s, wall], dist, device="cuda")
     paths = sum(s["samples"] for s in stats) * world
     value = paths / device_s
     e2e = paths / wall
@@ -312,6 +311,22 @@ def b200_arm(args):
     }
     if clocks:
         line["clocks"] = clocks
+    if world == 1 and not args.profile_case:
+        try:
+            import ref_harness
+        except ImportError:
+            ref_harness = None
+        if ref_harness is not None and ref_harness.available():
+            # The reference's own kernels (oracle/_ref, built from its sources for sm_100a) on the same
+            # GPU, driven through its launchers with its host-synchronised loop, pool of 1,048,576 slots.
+            R = ref_harness.RefScene(scene)
+            frames = [R.render(cam, W, H, spp, depth, True) for _ in range(2)]
+            R.close()
+            ref_ms = min(f["frame_ms"] for f in frames)
+            line["reference_build_b200"] = {"value": samples_per_frame / (ref_ms / 1000.0), "unit": "paths/s",
+                                            "ms_per_frame": ref_ms, "iterations": frames[-1]["iterations"],
+                                            "speedup_of_value": value / (samples_per_frame / (ref_ms / 1000.0)),
+                                            "what": "reference kernels (Intersect/PathGeneration/MaterialEval/Iteration.cu) compiled for sm_100a, replayed RenderFrame loop"}
     if world == 1 and not args.no_cpu_baseline:
         import oracle
         threads = oracle.default_threads()

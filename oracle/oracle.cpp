@@ -597,10 +597,10 @@ namespace oracle
     }
 
     // PathGeneration.cu:56-102 for one sample: Philox stream, jitter, camera ray
-    inline void GeneratePath(const Camera& camera, const PixelGrid& grid, uint64_t sampleIndex, PathState& ps)
+    inline void GeneratePath(const Camera& camera, const PixelGrid& grid, uint64_t sampleIndex, PathState& ps, uint64_t rngOffset = 0)
     {
         ps.sample = sampleIndex;
-        ps.random = Random{sampleIndex, 0};
+        ps.random = Random{sampleIndex + rngOffset, 0};
         const float2 jitter = ps.random.NextFloat2();
         uint32_t pixel;
         float2 uv;
@@ -1190,6 +1190,7 @@ namespace oracle
         uint64_t maxSamples;   // 0 = the whole frame
         int threads;
         int accumulation;      // 0 = FP32 sequential, 1 = FP32 Kahan (sample order), 2 = FP64
+        uint64_t rngOffset;    // added to the sample index to form the Philox subsequence
     };
 
     // Renderer.cpp:468-647 replayed on the CPU, iteration by iteration, with the
@@ -1213,7 +1214,7 @@ namespace oracle
         std::vector<PathState> active(generateCount);
         ParallelFor(generateCount, s.threads, [&](size_t b, size_t e)
         {
-            for (size_t i = b; i < e; i++) GeneratePath(camera, grid, i, active[i]);
+            for (size_t i = b; i < e; i++) GeneratePath(camera, grid, i, active[i], s.rngOffset);
         });
         uint64_t launched = generateCount;
         uint32_t iter = 0;
@@ -1263,7 +1264,7 @@ namespace oracle
             {
                 uint32_t* row = queueLog + static_cast<size_t>(iter) * 9;
                 row[0] = static_cast<uint32_t>(n);
-                for (int m = 0; m < ModelCount; m++) row[1 + m] = modelCounts[m];
+                for (uint32_t m = 0; m < ModelCount; m++) row[1 + m] = modelCounts[m];
                 row[7] = shadowCount;
                 row[8] = regenCount;
             }
@@ -1288,7 +1289,7 @@ namespace oracle
             next.resize(base + regenerate);
             ParallelFor(regenerate, s.threads, [&](size_t b, size_t e)
             {
-                for (size_t i = b; i < e; i++) GeneratePath(camera, grid, launched + i, next[base + i]);
+                for (size_t i = b; i < e; i++) GeneratePath(camera, grid, launched + i, next[base + i], s.rngOffset);
             });
             launched += regenerate;
             active.swap(next);
@@ -1477,12 +1478,13 @@ extern "C"
     // camera: origin3, lowerLeft3, horizontal3, vertical3 (DeviceCamera.hpp:5-11)
     int oracle_render(void* scene, const float* camera, uint32_t width, uint32_t height, uint32_t spp, uint32_t depth, uint32_t nee,
                       uint32_t poolSize, uint64_t maxSamples, int threads, int accumulationMode, float* sampleRadiance,
-                      float* accumulation, uint32_t* framebuffer, uint32_t* queueLog, uint32_t queueLogCapacity, uint32_t* iterations)
+                      float* accumulation, uint32_t* framebuffer, uint32_t* queueLog, uint32_t queueLogCapacity, uint32_t* iterations,
+                      uint64_t rngOffset)
     {
         auto* s = static_cast<oracle::Scene*>(scene);
         oracle::Camera cam{{camera[0], camera[1], camera[2]}, {camera[3], camera[4], camera[5]},
                            {camera[6], camera[7], camera[8]}, {camera[9], camera[10], camera[11]}};
-        oracle::RenderSettings rs{width, height, spp, depth, nee, poolSize, maxSamples, threads, accumulationMode};
+        oracle::RenderSettings rs{width, height, spp, depth, nee, poolSize, maxSamples, threads, accumulationMode, rngOffset};
         return oracle::Render(*s, cam, rs, sampleRadiance, accumulation, framebuffer, queueLog, queueLogCapacity, iterations);
     }
 

@@ -52,7 +52,7 @@ def lib():
         L.oracle_sincos.argtypes = [vp, u32, vp, vp]
         L.oracle_pow.argtypes = [vp, vp, u32, vp]
         L.oracle_render.restype = i32
-        L.oracle_render.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, u64, i32, i32, vp, vp, vp, vp, u32, vp]
+        L.oracle_render.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, u64, i32, i32, vp, vp, vp, vp, u32, vp, u64]
         L.oracle_make_camera.argtypes = [f32, f32, vp, vp, vp]
         _lib = L
     return _lib
@@ -118,7 +118,7 @@ class OracleScene:
 
     def render(self, camera: np.ndarray, width: int, height: int, spp: int, depth: int, nee: bool = True,
                pool_size: int = 1 << 20, max_samples: int = 0, threads: int | None = None, accumulation: int = 1,
-               log_capacity: int = 1 << 16):
+               log_capacity: int = 1 << 16, rng_offset: int = 0):
         """Replay of Renderer::RenderFrame on the CPU. accumulation: 0 = FP32 in
         sample order, 1 = FP32 Kahan in sample order, 2 = FP64."""
         spa = int(np.sqrt(spp))
@@ -134,7 +134,7 @@ class OracleScene:
         iters = ctypes.c_uint32(0)
         rc = lib().oracle_render(self.handle, _p(camera), width, height, spp, depth, 1 if nee else 0, pool_size,
                                  max_samples, threads or default_threads(), accumulation, _p(radiance), _p(accum),
-                                 _p(fb), _p(qlog), log_capacity, ctypes.byref(iters))
+                                 _p(fb), _p(qlog), log_capacity, ctypes.byref(iters), rng_offset)
         if rc != 0:
             raise RuntimeError(f"oracle_render failed: {rc}")
         it = iters.value

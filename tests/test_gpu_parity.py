@@ -268,3 +268,17 @@ def test_autotune_returns_valid_knobs_and_results_do_not_change(gpu_renderer, sc
                               trace_refill=knobs["trace_refill"], trace_block=knobs["trace_block"])
     b = gpu_renderer.sample_radiance()
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_rng_offset_shards_match_oracle(gpu_renderer, scene_factory, oracle_scene):
+    """A rank's shard (Philox subsequences offset by rank x samples per frame) equals the oracle's."""
+    import multigpu
+    s = scene_factory("cornell-all")
+    o = oracle_scene("cornell-all")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 48, 48)
+    off = multigpu.rank_rng_offset(3, 16 * 48 * 48)
+    gpu_renderer.render_frame(cam, 48, 48, 16, 10, True, rng_offset=off)
+    ref = o.render(cam, 48, 48, 16, 10, True, rng_offset=off)
+    assert np.array_equal(gpu_renderer.sample_radiance().view(np.uint32), ref["sample_radiance"].view(np.uint32))
+    assert np.array_equal(gpu_renderer.queue_log(), ref["queue_log"])
