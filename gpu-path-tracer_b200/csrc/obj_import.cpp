@@ -1,0 +1,393 @@
+// Headless OBJ/MTL scene ingest: a Wavefront OBJ file becomes the world-space triangle arrays and
+// constant material table of gpt_scene_desc, the way the reference turns an OBJ into the input
+// of its renderer:
+//   LoadObj (Core/Source/Import/ObjLoader.cpp:67-234): triangulated faces grouped per shape and
+//     per material id (ascending, faces without a material first), vertex normals and uvs
+//     required, normals normalised, MTL keys Kd Ks Ns Pr Pm Ke Ni Tf d and the extension keys
+//     `surface` (unlit normal diffuse lambert mirror phong microfacet ggx emissive) and `flip_textures`;
+//   GenerateTangentSpace (Core/Source/Utils/Math/TangentSpace.cpp): per-vertex tangents with a
+//     handedness sign. MikkTSpace is not available here; tangents are accumulated from each
+//     triangle's uv derivatives and Gram-Schmidt orthogonalised (Lengyel's method), which agrees
+//     with MikkTSpace on planar and smoothly parameterised meshes;
+//   Manager::ImportMaterial (Core/Source/Assets/Manager.cpp:311-412): constants become the texels of
+//     1x1 textures (sRGB u8 colour and specular, linear u8 shininess (Ns-1)/999, float emission,
+//     default normal texel); like the reference, the RMA texel is the default (255, 0, 255) when no
+//     map_RMA texture is given;
+//   BuildTriangles (Core/Source/Graphics/Cuda/PathTracing/Renderer.cpp:116-213): an optional affine
+//     world transform, normals by the inverse transpose, tangents re-orthogonalised to the normal.
+// Texture maps named in the MTL file are recorded but not loaded (image decoding is not on the path).
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/gpt_b200.h"
+
+struct gpt_obj_scene
+{
+    std::vector<float> positions, normals, tangents, uvs;
+    std::vector<uint32_t> materialIds;
+    std::vector<gpt_material> materials;
+    std::vector<std::string> materialNames;
+    std::string error;
+};
+
+namespace
+{
+    struct V3 { float x, y, z; };
+
+    struct MtlEntry
+    {
+        std::string name;
+        uint32_t model = GPT_MODEL_DIFFUSE;  // Unlit maps to Diffuse (Material.hpp:122-146)
+        float kd[3] = {0, 0, 0}, ks[3] = {0, 0, 0}, ke[3] = {0, 0, 0};
+        float ns = 1.0f, ni = 1.0f, tf = 0.0f, pr = 0.0f, pm = 0.0f;
+    };
+
+    uint8_t lround_u8(float v)
+    {
+        long r = std::lround(v);
+        return static_cast<uint8_t>(std::min(255L, std::max(0L, r)));
+    }
+
+    // LinearNormalizedFloatToSrgbU8 (Manager.cpp:65-79)
+    uint8_t srgb_u8(float x)
+    {
+        if (!std::isfinite(x)) x = 0.0f;
+        x = std::clamp(x, 0.0f, 1.0f);
+        float s = x <= 0.0031308f ? 12.92f * x : 1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f;
+        return lround_u8(s * 255.0f);
+    }
+
+    // sRGB texel decode of an sRGB texture
+    float srgb_decode(uint8_t u)
+    {
+        double c = u / 255.0;
+        double l = c <= 0.04045 ? c / 12.92 : std::pow((c + 0.055) / 1.055, 2.4);
+        return static_cast<float>(l);
+    }
+
+    uint8_t linear_u8(float x)  // NormalizedFloatToU8 (Manager.cpp:48-54)
+    {
+        if (!std::isfinite(x)) x = 0.0f;
+        return lround_u8(std::clamp(x, 0.0f, 1.0f) * 255.0f);
+    }
+
+    gpt_material encode(const MtlEntry& m)
+    {
+        gpt_material g{};
+        g.model = m.model;
+        for (int k = 0; k < 3; k++)
+        {
+            g.color[k] = srgb_decode(srgb_u8(m.kd[k]));
+            g.specular[k] = srgb_decode(srgb_u8(m.ks[k]));
+            g.emission[k] = m.ke[k];
+        }
+        float ns = std::isfinite(m.ns) ? m.ns : 1.0f;
+        ns = std::clamp(ns, 1.0f, 1000.0f);
+        g.shininess = static_cast<float>(linear_u8((ns - 1.0f) / (1000.0f - 1.0f))) / 255.0f;
+        g.rma[0] = 1.0f;  // default RMA texel (255, 0, 255): Manager.cpp:369-372 uses it for constants
+        g.rma[1] = 0.0f;
+        g.rma[2] = 1.0f;
+        g.normal[0] = 128.0f / 255.0f;
+        g.normal[1] = 128.0f / 255.0f;
+        g.normal[2] = 1.0f;
+        g.ior = m.ni;
+        g.transmission = m.tf;
+        return g;
+    }
+
+    bool parse_mtl(const std::filesystem::path& file, std::vector<MtlEntry>& out)
+    {
+        std::ifstream in(file);
+        if (!in) return false;
+        std::string line;
+        MtlEntry* cur = nullptr;
+        static const std::pair<const char*, uint32_t> models[] = {
+            {"unlit", GPT_MODEL_DIFFUSE}, {"normal", GPT_MODEL_NORMAL}, {"diffuse", GPT_MODEL_DIFFUSE}, {"lambert", GPT_MODEL_DIFFUSE},
+            {"mirror", GPT_MODEL_MIRROR}, {"phong", GPT_MODEL_PHONG}, {"microfacet", GPT_MODEL_GGX}, {"ggx", GPT_MODEL_GGX},
+            {"emissive", GPT_MODEL_EMISSIVE}};
+        while (std::getline(in, line))
+        {
+            std::istringstream ss(line);
+            std::string key;
+            if (!(ss >> key) || key[0] == '#') continue;
+            if (key == "newmtl")
+            {
+                out.emplace_back();
+                ss >> out.back().name;
+                cur = &out.back();
+                continue;
+            }
+            if (!cur) continue;
+            auto read3 = [&](float* v) { ss >> v[0]; if (!(ss >> v[1] >> v[2])) v[1] = v[2] = v[0]; };
+            if (key == "Kd") read3(cur->kd);
+            else if (key == "Ks") read3(cur->ks);
+            else if (key == "Ke") read3(cur->ke);
+            else if (key == "Ns") ss >> cur->ns;
+            else if (key == "Ni") ss >> cur->ni;
+            else if (key == "Pr") ss >> cur->pr;
+            else if (key == "Pm") ss >> cur->pm;
+            else if (key == "Tf") { float t[3]; read3(t); cur->tf = t[0]; }
+            else if (key == "surface")
+            {
+                std::string v;
+                ss >> v;
+                for (const auto& [name, model] : models)
+                    if (v == name) cur->model = model;
+            }
+        }
+        return true;
+    }
+
+    int resolve_index(long i, size_t count)
+    {
+        if (i > 0) return static_cast<int>(i - 1);
+        if (i < 0) return static_cast<int>(static_cast<long>(count) + i);
+        return -1;
+    }
+
+    V3 normalize3(V3 v)
+    {
+        float l = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
+        if (l > 0.0f) return {v.x / l, v.y / l, v.z / l};
+        return v;
+    }
+}
+
+extern "C"
+{
+    int gpt_obj_load(const char* path, const float* transform, gpt_obj_scene** out)
+    {
+        if (!path || !out) return GPT_ERR_INVALID_ARGUMENT;
+        *out = nullptr;
+        std::ifstream in(path);
+        if (!in) return GPT_ERR_INVALID_ARGUMENT;
+        const std::filesystem::path dir = std::filesystem::path(path).parent_path();
+        std::vector<V3> pos, nrm;
+        std::vector<std::array<float, 2>> tex;
+        std::vector<MtlEntry> mtl;
+        std::map<std::string, int> mtlIndex;
+        struct Corner { int v, t, n; };
+        struct Face { std::array<Corner, 3> c; };
+        // shapes -> material id -> faces (tinyobj shape grouping, std::map order of material ids)
+        std::vector<std::map<int, std::vector<Face>>> shapes(1);
+        int currentMaterial = -1;
+        std::string line;
+        while (std::getline(in, line))
+        {
+            std::istringstream ss(line);
+            std::string key;
+            if (!(ss >> key) || key[0] == '#') continue;
+            if (key == "v") { V3 p; ss >> p.x >> p.y >> p.z; pos.push_back(p); }
+            else if (key == "vn") { V3 n; ss >> n.x >> n.y >> n.z; nrm.push_back(n); }
+            else if (key == "vt") { std::array<float, 2> t{0, 0}; ss >> t[0] >> t[1]; tex.push_back(t); }
+            else if (key == "mtllib")
+            {
+                std::string f;
+                while (ss >> f)
+                {
+                    std::vector<MtlEntry> entries;
+                    if (parse_mtl(dir / f, entries))
+                        for (auto& e : entries)
+                        {
+                            mtlIndex[e.name] = static_cast<int>(mtl.size());
+                            mtl.push_back(e);
+                        }
+                }
+            }
+            else if (key == "usemtl")
+            {
+                std::string n;
+                ss >> n;
+                auto it = mtlIndex.find(n);
+                currentMaterial = it == mtlIndex.end() ? -1 : it->second;
+            }
+            else if (key == "o" || key == "g")
+            {
+                if (!shapes.back().empty()) shapes.emplace_back();
+            }
+            else if (key == "f")
+            {
+                std::vector<Corner> poly;
+                std::string tok;
+                while (ss >> tok)
+                {
+                    long vi = 0, ti = 0, ni = 0;
+                    int field = 0;
+                    std::string part;
+                    std::stringstream ts(tok);
+                    while (std::getline(ts, part, '/'))
+                    {
+                        long val = part.empty() ? 0 : std::stol(part);
+                        if (field == 0) vi = val;
+                        else if (field == 1) ti = val;
+                        else ni = val;
+                        field++;
+                    }
+                    poly.push_back({resolve_index(vi, pos.size()), resolve_index(ti, tex.size()), resolve_index(ni, nrm.size())});
+                }
+                for (size_t k = 2; k < poly.size(); k++)  // fan triangulation
+                    shapes.back()[currentMaterial].push_back(Face{{poly[0], poly[k - 1], poly[k]}});
+            }
+        }
+        auto scene = std::make_unique<gpt_obj_scene>();
+        // material table: the file's materials, then a default white diffuse for faces without one
+        for (const MtlEntry& e : mtl)
+        {
+            scene->materials.push_back(encode(e));
+            scene->materialNames.push_back(e.name);
+        }
+        MtlEntry defaultMaterial;
+        defaultMaterial.name = "default";
+        defaultMaterial.kd[0] = defaultMaterial.kd[1] = defaultMaterial.kd[2] = 1.0f;
+        const uint32_t defaultIndex = static_cast<uint32_t>(scene->materials.size());
+        bool usesDefault = false;
+        float M[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};  // column-major
+        if (transform) std::memcpy(M, transform, sizeof(M));
+        // normal matrix = inverse transpose of the linear part
+        const float a = M[0], b = M[4], c = M[8], d = M[1], e = M[5], f = M[9], g = M[2], h = M[6], i = M[10];
+        const float det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+        if (!(std::fabs(det) > 0.0f)) return GPT_ERR_INVALID_ARGUMENT;
+        const float inv[9] = {(e * i - f * h) / det, (c * h - b * i) / det, (b * f - c * e) / det,
+                              (f * g - d * i) / det, (a * i - c * g) / det, (c * d - a * f) / det,
+                              (d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det};  // row-major inverse
+        auto xformP = [&](V3 p) { return V3{M[0] * p.x + M[4] * p.y + M[8] * p.z + M[12], M[1] * p.x + M[5] * p.y + M[9] * p.z + M[13],
+                                            M[2] * p.x + M[6] * p.y + M[10] * p.z + M[14]}; };
+        auto xformL = [&](V3 p) { return V3{M[0] * p.x + M[4] * p.y + M[8] * p.z, M[1] * p.x + M[5] * p.y + M[9] * p.z,
+                                            M[2] * p.x + M[6] * p.y + M[10] * p.z}; };
+        auto xformN = [&](V3 n) { return V3{inv[0] * n.x + inv[3] * n.y + inv[6] * n.z, inv[1] * n.x + inv[4] * n.y + inv[7] * n.z,
+                                            inv[2] * n.x + inv[5] * n.y + inv[8] * n.z}; };
+        for (auto& shape : shapes)
+            for (auto& [matId, faces] : shape)
+            {
+                // dedupe corners of this submesh and accumulate tangents per vertex
+                struct Key { int v, t, n; bool operator==(const Key& o) const { return v == o.v && t == o.t && n == o.n; } };
+                struct KeyHash { size_t operator()(const Key& k) const { return (size_t(k.v) * 73856093u) ^ (size_t(k.t) * 19349663u) ^ (size_t(k.n) * 83492791u); } };
+                std::unordered_map<Key, uint32_t, KeyHash> index;
+                std::vector<Key> verts;
+                std::vector<std::array<uint32_t, 3>> tris;
+                for (const Face& fc : faces)
+                {
+                    std::array<uint32_t, 3> t{};
+                    for (int k = 0; k < 3; k++)
+                    {
+                        const Corner& cr = fc.c[k];
+                        if (cr.v < 0 || cr.v >= static_cast<int>(pos.size())) return GPT_ERR_INVALID_ARGUMENT;
+                        if (cr.n < 0 || cr.n >= static_cast<int>(nrm.size())) return GPT_ERR_INVALID_ARGUMENT;  // normals are required
+                        if (cr.t < 0 || cr.t >= static_cast<int>(tex.size())) return GPT_ERR_INVALID_ARGUMENT;  // uvs are required
+                        Key key{cr.v, cr.t, cr.n};
+                        auto it = index.try_emplace(key, static_cast<uint32_t>(verts.size()));
+                        if (it.second) verts.push_back(key);
+                        t[k] = it.first->second;
+                    }
+                    tris.push_back(t);
+                }
+                std::vector<V3> tanAcc(verts.size(), V3{0, 0, 0}), bitAcc(verts.size(), V3{0, 0, 0});
+                for (const auto& t : tris)
+                {
+                    const V3 p0 = pos[verts[t[0]].v], p1 = pos[verts[t[1]].v], p2 = pos[verts[t[2]].v];
+                    const auto& w0 = tex[verts[t[0]].t];
+                    const auto& w1 = tex[verts[t[1]].t];
+                    const auto& w2 = tex[verts[t[2]].t];
+                    const V3 e1{p1.x - p0.x, p1.y - p0.y, p1.z - p0.z}, e2{p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
+                    const float du1 = w1[0] - w0[0], dv1 = w1[1] - w0[1], du2 = w2[0] - w0[0], dv2 = w2[1] - w0[1];
+                    const float den = du1 * dv2 - du2 * dv1;
+                    if (std::fabs(den) < 1e-20f) continue;
+                    const float r = 1.0f / den;
+                    const V3 sdir{(dv2 * e1.x - dv1 * e2.x) * r, (dv2 * e1.y - dv1 * e2.y) * r, (dv2 * e1.z - dv1 * e2.z) * r};
+                    const V3 tdir{(du1 * e2.x - du2 * e1.x) * r, (du1 * e2.y - du2 * e1.y) * r, (du1 * e2.z - du2 * e1.z) * r};
+                    for (int k = 0; k < 3; k++)
+                    {
+                        tanAcc[t[k]].x += sdir.x; tanAcc[t[k]].y += sdir.y; tanAcc[t[k]].z += sdir.z;
+                        bitAcc[t[k]].x += tdir.x; bitAcc[t[k]].y += tdir.y; bitAcc[t[k]].z += tdir.z;
+                    }
+                }
+                const uint32_t material = matId >= 0 ? static_cast<uint32_t>(matId) : defaultIndex;
+                if (matId < 0) usesDefault = true;
+                for (const auto& t : tris)
+                {
+                    for (int k = 0; k < 3; k++)
+                    {
+                        const Key& vk = verts[t[k]];
+                        const V3 wp = xformP(pos[vk.v]);
+                        const V3 n = normalize3(nrm[vk.n]);
+                        const V3 wn = normalize3(xformN(n));
+                        // object-space tangent: Gram-Schmidt against the normal, handedness from the bitangent
+                        V3 tg = tanAcc[t[k]];
+                        const float nd = n.x * tg.x + n.y * tg.y + n.z * tg.z;
+                        tg = V3{tg.x - n.x * nd, tg.y - n.y * nd, tg.z - n.z * nd};
+                        const V3 bt = bitAcc[t[k]];
+                        const V3 cr{n.y * tg.z - n.z * tg.y, n.z * tg.x - n.x * tg.z, n.x * tg.y - n.y * tg.x};
+                        const float sign = (cr.x * bt.x + cr.y * bt.y + cr.z * bt.z) < 0.0f ? -1.0f : 1.0f;
+                        // ComputeWorldTangent (Renderer.cpp:116-142)
+                        V3 wt = xformL(tg);
+                        float l2 = wt.x * wt.x + wt.y * wt.y + wt.z * wt.z;
+                        if (l2 > 1e-16f)
+                        {
+                            const float inv = 1.0f / std::sqrt(l2);
+                            wt = V3{wt.x * inv, wt.y * inv, wt.z * inv};
+                            const float dd = wn.x * wt.x + wn.y * wt.y + wn.z * wt.z;
+                            wt = V3{wt.x - wn.x * dd, wt.y - wn.y * dd, wt.z - wn.z * dd};
+                        }
+                        l2 = wt.x * wt.x + wt.y * wt.y + wt.z * wt.z;
+                        if (l2 > 1e-16f)
+                        {
+                            const float inv = 1.0f / std::sqrt(l2);
+                            wt = V3{wt.x * inv, wt.y * inv, wt.z * inv};
+                        }
+                        else
+                        {
+                            const V3 axis = std::fabs(wn.z) < 0.999f ? V3{0, 0, 1} : V3{1, 0, 0};
+                            wt = normalize3(V3{axis.y * wn.z - axis.z * wn.y, axis.z * wn.x - axis.x * wn.z, axis.x * wn.y - axis.y * wn.x});
+                        }
+                        scene->positions.insert(scene->positions.end(), {wp.x, wp.y, wp.z});
+                        scene->normals.insert(scene->normals.end(), {wn.x, wn.y, wn.z});
+                        scene->tangents.insert(scene->tangents.end(), {wt.x, wt.y, wt.z, sign});
+                        scene->uvs.insert(scene->uvs.end(), {tex[vk.t][0], tex[vk.t][1]});
+                    }
+                    scene->materialIds.push_back(material);
+                }
+            }
+        if (usesDefault)
+        {
+            scene->materials.push_back(encode(defaultMaterial));
+            scene->materialNames.push_back(defaultMaterial.name);
+        }
+        if (scene->materialIds.empty()) return GPT_ERR_INVALID_ARGUMENT;
+        *out = scene.release();
+        return GPT_OK;
+    }
+
+    int gpt_obj_scene_desc(const gpt_obj_scene* s, gpt_scene_desc* desc)
+    {
+        if (!s || !desc) return GPT_ERR_INVALID_ARGUMENT;
+        desc->triangle_count = static_cast<uint32_t>(s->materialIds.size());
+        desc->positions = s->positions.data();
+        desc->normals = s->normals.data();
+        desc->tangents = s->tangents.data();
+        desc->uvs = s->uvs.data();
+        desc->material_ids = s->materialIds.data();
+        desc->material_count = static_cast<uint32_t>(s->materials.size());
+        desc->materials = s->materials.data();
+        return GPT_OK;
+    }
+
+    int gpt_obj_material_name(const gpt_obj_scene* s, uint32_t index, char* buffer, size_t length)
+    {
+        if (!s || !buffer || length == 0 || index >= s->materialNames.size()) return GPT_ERR_INVALID_ARGUMENT;
+        std::snprintf(buffer, length, "%s", s->materialNames[index].c_str());
+        return GPT_OK;
+    }
+
+    void gpt_obj_free(gpt_obj_scene* s) { delete s; }
+}

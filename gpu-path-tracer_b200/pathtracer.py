@@ -112,6 +112,10 @@ _SIGNATURES = [
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(ctypes.c_uint64)]),
     ("gpt_build_alias_table_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpt_obj_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("gpt_obj_scene_desc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc)]),
+    ("gpt_obj_material_name", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t]),
+    ("gpt_obj_free", None, [ctypes.c_void_p]),
     ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
                                               ctypes.POINTER(gpt_device_camera)]),
 ]
@@ -360,6 +364,43 @@ def build_alias_table_noalloc(weights_dev, bins_dev, stream=None) -> int:
     """Allocation-free alias-table build on device tensors (float32 weights [n], int32 bins [n, 4])."""
     return lib().gpt_build_alias_table_noalloc(ctypes.c_void_p(weights_dev.data_ptr()), weights_dev.shape[0],
                                                 ctypes.c_void_p(bins_dev.data_ptr()), ctypes.c_void_p(stream))
+
+
+def load_obj(path: str, transform=None):
+    """OBJ/MTL file -> scenes.Scene (world-space triangles, constant materials encoded as texels)."""
+    import scenes
+    L = lib()
+    h = ctypes.c_void_p()
+    t = None
+    if transform is not None:
+        t = np.ascontiguousarray(np.asarray(transform, dtype=np.float32).reshape(4, 4).T)  # row-major in, column-major out
+    rc = L.gpt_obj_load(path.encode(), _ptr(t) if t is not None else None, ctypes.byref(h))
+    if rc != 0:
+        raise GptError(rc, f"gpt_obj_load({path})")
+    try:
+        d = gpt_scene_desc()
+        L.gpt_obj_scene_desc(h, ctypes.byref(d))
+        n, m = d.triangle_count, d.material_count
+
+        def arr(ptr, count, dtype):
+            return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(dtype)), shape=(count,)).copy()
+        pos = arr(d.positions, n * 9, ctypes.c_float).reshape(n, 3, 3)
+        nrm = arr(d.normals, n * 9, ctypes.c_float).reshape(n, 3, 3)
+        tan = arr(d.tangents, n * 12, ctypes.c_float).reshape(n, 3, 4)
+        uv = arr(d.uvs, n * 6, ctypes.c_float).reshape(n, 3, 2)
+        mid = arr(d.material_ids, n, ctypes.c_uint32)
+        raw = np.ctypeslib.as_array(ctypes.cast(d.materials, ctypes.POINTER(ctypes.c_uint8)), shape=(m * 80,)).copy()
+        mats = raw.view(scenes.MATERIAL_DTYPE).copy()
+        names = []
+        for i in range(m):
+            buf = ctypes.create_string_buffer(256)
+            L.gpt_obj_material_name(h, i, buf, 256)
+            names.append(buf.value.decode())
+        s = scenes.Scene(pos, nrm, tan, uv, mid, mats, name=os.path.basename(path)).contiguous()
+        s.material_names = names
+        return s
+    finally:
+        L.gpt_obj_free(h)
 
 
 def make_device_camera(fov_y: float, aspect: float, position, quat_wxyz) -> np.ndarray:

@@ -246,6 +246,20 @@ int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* 
 #define GPT_NOALLOC_MAX_LIGHTS 65536u
 int gpt_build_alias_table_noalloc(const float* weights, uint32_t light_count, uint32_t* bins, void* stream);
 
+/*
+ * Headless OBJ/MTL ingest (the reference's LoadObj + GenerateTangentSpace + Manager::ImportMaterial +
+ * BuildTriangles: Core/Source/Import/ObjLoader.cpp:67-234, Core/Source/Assets/Manager.cpp:311-412,
+ * Renderer.cpp:116-213). Produces the arrays of a gpt_scene_desc: triangles grouped per shape and
+ * material, vertex normals and uvs required, tangents from uv derivatives, constant materials
+ * encoded as the reference's texels. transform: optional column-major 4x4 world matrix (NULL =
+ * identity). The scene object owns the arrays gpt_obj_scene_desc points into.
+ */
+typedef struct gpt_obj_scene gpt_obj_scene;
+int gpt_obj_load(const char* path, const float* transform, gpt_obj_scene** out);
+int gpt_obj_scene_desc(const gpt_obj_scene* scene, gpt_scene_desc* desc);
+int gpt_obj_material_name(const gpt_obj_scene* scene, uint32_t index, char* buffer, size_t length);
+void gpt_obj_free(gpt_obj_scene* scene);
+
 /* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */
 int gpt_make_device_camera(float fov_y, float aspect, const gpt_motion_state* state, gpt_device_camera* out);
 
