@@ -470,10 +470,11 @@ namespace pt
     {
         float3 position, gN, normal;
         float4 tangent;
+        float2 uv;
         uint32_t material;
     };
 
-    // LoadResolvedHit (MaterialEval.cu:54-87), without the uv (constant materials).
+    // LoadResolvedHit (MaterialEval.cu:54-87).
     __device__ __forceinline__ Surface resolve_hit(const SceneView& sc, float3 o, float3 d, float tHit, uint32_t tri, float u, float v)
     {
         const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
@@ -491,18 +492,46 @@ namespace pt
         s.normal = b0 * f3(n0) + b1 * f3(n1) + b2 * f3(n2);
         const float4 t0 = ldg4(rec + 3), t1 = ldg4(rec + 4), t2 = ldg4(rec + 5);
         s.tangent = b0 * t0 + b1 * t1 + b2 * t2;
+        const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
+        s.uv = b0 * make_float2(u01.x, u01.y) + b1 * make_float2(u01.z, u01.w) + b2 * make_float2(u2.x, u2.y);
         return s;
+    }
+
+    // Material slot value: the slot's texture sampled at uv (TextureView::Sample, TextureView.hpp:17-20)
+    // when the material has one, else its constant texel.
+    __device__ __forceinline__ float3 slot_rgb(const SceneView& sc, uint32_t mat, int slot, float2 uv, const float* constant)
+    {
+        if (sc.textures != nullptr)
+        {
+            const unsigned long long t = __ldg(&sc.textures[mat].tex[slot]);
+            if (t != 0)
+            {
+                const float4 v = tex2D<float4>(t, uv.x, uv.y);
+                return make_float3(v.x, v.y, v.z);
+            }
+        }
+        return make_float3(__ldg(constant), __ldg(constant + 1), __ldg(constant + 2));
+    }
+
+    __device__ __forceinline__ float slot_scalar(const SceneView& sc, uint32_t mat, int slot, float2 uv, const float* constant)
+    {
+        if (sc.textures != nullptr)
+        {
+            const unsigned long long t = __ldg(&sc.textures[mat].tex[slot]);
+            if (t != 0) return tex2D<float>(t, uv.x, uv.y);
+        }
+        return __ldg(constant);
     }
 
     __device__ __forceinline__ float3 mat3(const float* v) { return make_float3(__ldg(v), __ldg(v + 1), __ldg(v + 2)); }
 
-    // GetShadingFrame (MaterialEval.cu:89-115) with a constant normal-map texel.
-    __device__ __forceinline__ Frame shading_frame(const Surface& s, const MaterialDev& m)
+    // GetShadingFrame (MaterialEval.cu:89-115).
+    __device__ __forceinline__ Frame shading_frame(const SceneView& sc, const Surface& s, const MaterialDev& m)
     {
         const float3 bt = make_float3(s.tangent.x, s.tangent.y, s.tangent.z);
         const float sign = s.tangent.w < 0.0f ? -1.0f : 1.0f;
         const Frame base = frame_from(s.normal, bt, sign);
-        const float3 ts = normalize(mat3(m.normal) * 2.0f - 1.0f);
+        const float3 ts = normalize(slot_rgb(sc, s.material, 5, s.uv, m.normal) * 2.0f - 1.0f);
         const float3 sn = ts.x * base.tangent + ts.y * base.bitangent + ts.z * base.normal;
         return frame_from(sn, bt, sign);
     }
@@ -560,20 +589,33 @@ namespace pt
             index = b.z;
             pmf = __uint_as_float(__ldg(&sc.bins[index].y));
         }
-        const float4* L = sc.lights + static_cast<size_t>(index) * 5;
+        const float4* L = sc.lights + static_cast<size_t>(index) * 7;
         const float4 l0 = ldg4(L), l1 = ldg4(L + 1), l2 = ldg4(L + 2), l3 = ldg4(L + 3), l4 = ldg4(L + 4);
         const float s0 = sqrtf(xi.x);
         const float b1 = s0 * (1.0f - xi.y);
         const float b2 = s0 * xi.y;
         LightHit h;
         h.position = f3(l0) + b1 * f3(l1) + b2 * f3(l2);
+        float3 emission = f3(l4);
+        if (sc.textures != nullptr)
+        {
+            const float4 l5 = ldg4(L + 5), l6 = ldg4(L + 6);
+            const uint32_t mat = __float_as_uint(l6.z);
+            const unsigned long long t = __ldg(&sc.textures[mat].tex[4]);
+            if (t != 0)
+            {
+                const float2 uv = make_float2(l5.x, l5.y) + b1 * make_float2(l5.z, l5.w) + b2 * make_float2(l6.x, l6.y);
+                const float4 e = tex2D<float4>(t, uv.x, uv.y);
+                emission = make_float3(e.x, e.y, e.z);
+            }
+        }
         const float3 toLight = h.position - hitPoint;
         h.distanceSquared = dot(toLight, toLight);
         h.wi = normalize(toLight);
         float3 gn = f3(l3);
         if (dot(gn, h.wi) > 0.0f) gn = -gn;
         h.gN = gn;
-        h.emission = f3(l4);
+        h.emission = emission;
         h.pdf = pmf / l1.w;
         return h;
     }
@@ -855,8 +897,13 @@ namespace pt
             {
                 if (!(nee && !delta))
                 {
-                    const uint32_t mat = __float_as_uint(__ldg(&sc.shading[static_cast<size_t>(tri) * 9 + 6].w));
-                    const float3 em = mat3(sc.materials[mat].emission);
+                    // LoadPartiallyResolvedHit (MaterialEval.cu:32-52): material and interpolated uv
+                    const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
+                    const uint32_t mat = __float_as_uint(__ldg(&rec[6].w));
+                    const float b0 = 1.0f - h4.y - h4.z;
+                    const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
+                    const float2 uv = b0 * make_float2(u01.x, u01.y) + h4.y * make_float2(u01.z, u01.w) + h4.z * make_float2(u2.x, u2.y);
+                    const float3 em = slot_rgb(sc, mat, 4, uv, sc.materials[mat].emission);
                     const float3 c = T * em;
                     L4.x = L4.x + c.x;
                     L4.y = L4.y + c.y;
@@ -877,13 +924,13 @@ namespace pt
                 hitPos = s.position;
                 nextGn = s.gN;
                 const MaterialDev& m = sc.materials[s.material];
-                const Frame f = shading_frame(s, m);
+                const Frame f = shading_frame(sc, s, m);
                 curandStatePhilox4_32_10_t rng;
                 curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + jobPtr->rngOffset,
                             static_cast<unsigned long long>(rngPos), &rng);
                 if (MODEL == 1)  // Diffuse (:311-350, :270-309)
                 {
-                    const float3 albedo = mat3(m.color);
+                    const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
                     const float4 ind = curand_uniform4(&rng);
                     rngPos += 4;
                     if (nee)
@@ -905,7 +952,7 @@ namespace pt
                 }
                 else if (MODEL == 2)  // Mirror (:352-392)
                 {
-                    const float3 reflectance = mat3(m.specular);
+                    const float3 reflectance = slot_rgb(sc, s.material, 1, s.uv, m.specular);
                     const float rr = curand_uniform(&rng);
                     rngPos += 1;
                     const float3 wi = reflect(d, f.normal);
@@ -916,9 +963,9 @@ namespace pt
                 }
                 else if (MODEL == 3)  // Phong (:544-585)
                 {
-                    const float3 albedo = mat3(m.color);
-                    const float3 specular = mat3(m.specular);
-                    const float shininess = __ldg(&m.shininess) * (1000.0f - 1.0f) + 1.0f;
+                    const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
+                    const float3 specular = slot_rgb(sc, s.material, 1, s.uv, m.specular);
+                    const float shininess = slot_scalar(sc, s.material, 2, s.uv, &m.shininess) * (1000.0f - 1.0f) + 1.0f;
                     const float4 ind = curand_uniform4(&rng);
                     rngPos += 4;
                     if (nee) sh = direct_lambert_phong(sc, T, d, s, f, f3(ind), albedo, true, specular, shininess);
@@ -930,8 +977,8 @@ namespace pt
                 }
                 else if (MODEL == 4)  // GGX (:838-880)
                 {
-                    const float3 base = mat3(m.color);
-                    const float3 rma = mat3(m.rma);
+                    const float3 base = slot_rgb(sc, s.material, 0, s.uv, m.color);
+                    const float3 rma = slot_rgb(sc, s.material, 3, s.uv, m.rma);
                     const float alpha = fmaxf(rma.x * rma.x, 0.001f);
                     const float metallic = rma.y;
                     const float ior = __ldg(&m.ior);
@@ -1126,12 +1173,16 @@ namespace pt
             const float4 g = shading[static_cast<size_t>(t) * 9 + 6];
             const uint32_t mat = __float_as_uint(g.w);
             const uint32_t li = index[t];
-            float4* L = lights + static_cast<size_t>(li) * 5;
+            float4* L = lights + static_cast<size_t>(li) * 7;
             L[0] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(t));
             L[1] = make_float4(e1.x, e1.y, e1.z, area);
             L[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
             L[3] = make_float4(g.x, g.y, g.z, 0.0f);
             L[4] = make_float4(materials[mat].emission[0], materials[mat].emission[1], materials[mat].emission[2], 0.0f);
+            // uv0, uv1 - uv0, uv2 - uv0 (LightSampler.cpp:28-30) and the material for its emission texture
+            const float4 u01 = shading[static_cast<size_t>(t) * 9 + 7], u2 = shading[static_cast<size_t>(t) * 9 + 8];
+            L[5] = make_float4(u01.x, u01.y, u01.z - u01.x, u01.w - u01.y);
+            L[6] = make_float4(u2.x - u01.x, u2.y - u01.y, __uint_as_float(mat), 0.0f);
             weights[li] = static_cast<double>(area);
         }
     }

@@ -4,7 +4,7 @@
 //   BVH8 node        128 B  (Node8 below)           scene-resident
 //   triangle (MT)     48 B  v0|orig, e1|model, e2     leaf order, scene-resident
 //   triangle shading 144 B  3 normals, 3 tangents, gN|material, uvs (Triangle.hpp:24-38 layout), input order
-//   light            80 B   v0|index, e1|area, e2, gN, emission
+//   light           112 B   v0|index, e1|area, e2, gN, emission, uv0|uvE1, uvE2|material
 //   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14)
 //   path slot         36 B  throughput|depth/flags, radiance|rng position, sample index
 //   ray queue entry   32 B  origin|slot, direction|tMax   (x2, ping-pong)
@@ -59,13 +59,22 @@ namespace pt
     };
     static_assert(sizeof(MaterialDev) == 80, "material record is 80 bytes");
 
+    // Texture objects of a material's slots (0 = use the constant of MaterialDev).
+    struct __align__(16) MaterialTextures
+    {
+        unsigned long long tex[6];  // color, specular, shininess, rma, emission, normal
+        unsigned long long pad[2];
+    };
+    static_assert(sizeof(MaterialTextures) == 64, "material texture record is 64 bytes");
+
     struct SceneView
     {
         const Node8* nodes;
         const float4* tris;       // 3 per triangle, leaf order
         const float4* shading;    // 9 per triangle, input order
         const MaterialDev* materials;
-        const float4* lights;     // 5 per light
+        const MaterialTextures* textures;  // per material, nullptr when the scene has no image textures
+        const float4* lights;     // 7 per light
         const uint4* bins;        // alias table
         uint32_t lightCount;
         uint32_t nodeCount;

@@ -83,9 +83,80 @@ namespace pt
         size_t bytes_ = 0;
     };
 
+    // An image texture with the reference's descriptors (Texture.cpp:65-189).
+    struct TextureObject
+    {
+        cudaArray_t array = nullptr;
+        cudaTextureObject_t object = 0;
+        TextureObject() = default;
+        TextureObject(const TextureObject&) = delete;
+        TextureObject& operator=(const TextureObject&) = delete;
+        ~TextureObject()
+        {
+            if (object) cudaDestroyTextureObject(object);
+            if (array) cudaFreeArray(array);
+        }
+    };
+
+    static Status CreateTexture(const gpt_texture_desc& d, TextureObject& t)
+    {
+        if (d.width == 0 || d.height == 0 || !d.data || (d.channels != 1 && d.channels != 3 && d.channels != 4) || d.format > GPT_TEXEL_F32)
+            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unsupported texture description");
+        const bool u8 = d.format != GPT_TEXEL_F32;
+        const size_t texels = static_cast<size_t>(d.width) * d.height;
+        const uint32_t outChannels = d.channels == 1 ? 1 : 4;
+        const size_t elem = (u8 ? 1 : 4) * outChannels;
+        std::vector<unsigned char> expanded;
+        const void* src = d.data;
+        if (d.channels == 3)  // Import::ConvertRgbToRgba: alpha 255 (u8) or 1.0 (float)
+        {
+            expanded.resize(texels * elem);
+            for (size_t i = 0; i < texels; i++)
+            {
+                if (u8)
+                {
+                    const unsigned char* in = static_cast<const unsigned char*>(d.data) + i * 3;
+                    unsigned char* o = expanded.data() + i * 4;
+                    o[0] = in[0];
+                    o[1] = in[1];
+                    o[2] = in[2];
+                    o[3] = 255;
+                }
+                else
+                {
+                    const float* in = static_cast<const float*>(d.data) + i * 3;
+                    float* o = reinterpret_cast<float*>(expanded.data()) + i * 4;
+                    o[0] = in[0];
+                    o[1] = in[1];
+                    o[2] = in[2];
+                    o[3] = 1.0f;
+                }
+            }
+            src = expanded.data();
+        }
+        cudaChannelFormatDesc cd = u8 ? (outChannels == 1 ? cudaCreateChannelDesc<uchar1>() : cudaCreateChannelDesc<uchar4>())
+                                      : (outChannels == 1 ? cudaCreateChannelDesc<float1>() : cudaCreateChannelDesc<float4>());
+        PT_CUDA("cudaMallocArray", cudaMallocArray(&t.array, &cd, d.width, d.height));
+        const size_t pitch = static_cast<size_t>(d.width) * elem;
+        PT_CUDA("cudaMemcpy2DToArray", cudaMemcpy2DToArray(t.array, 0, 0, src, pitch, pitch, d.height, cudaMemcpyHostToDevice));
+        cudaResourceDesc res{};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = t.array;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeClamp;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.normalizedCoords = 1;
+        td.sRGB = d.format == GPT_TEXEL_U8_SRGB ? 1 : 0;
+        td.readMode = u8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
+        PT_CUDA("cudaCreateTextureObject", cudaCreateTextureObject(&t.object, &res, &td, nullptr));
+        return Status::Ok();
+    }
+
     struct SceneGpu
     {
-        DeviceBuffer nodes, tris, shading, materials, lights, bins;
+        DeviceBuffer nodes, tris, shading, materials, lights, bins, materialTextures;
+        std::vector<std::unique_ptr<TextureObject>> textures;
         uint32_t nodeCount = 0, triangleCount = 0, depth = 0, lightCount = 0;
         bool modelPresent[kModelCount] = {};
         uint64_t version = 0;
@@ -96,6 +167,7 @@ namespace pt
             v.tris = tris.get<float4>();
             v.shading = shading.get<float4>();
             v.materials = materials.get<MaterialDev>();
+            v.textures = textures.empty() ? nullptr : materialTextures.get<MaterialTextures>();
             v.lights = lights.get<float4>();
             v.bins = bins.get<uint4>();
             v.lightCount = lightCount;
@@ -281,6 +353,35 @@ namespace pt
             releaseGraph();
             auto scene = std::make_unique<SceneGpu>();
             std::copy(present, present + kModelCount, scene->modelPresent);
+            // image textures of the material slots
+            if (d.texture_count > 0 && d.material_textures)
+            {
+                if (!d.textures) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Texture table is missing");
+                std::vector<MaterialTextures> slots(d.material_count);
+                for (uint32_t i = 0; i < d.texture_count; i++)
+                {
+                    scene->textures.push_back(std::make_unique<TextureObject>());
+                    PT_TRY(CreateTexture(d.textures[i], *scene->textures.back()));
+                }
+                for (uint32_t m = 0; m < d.material_count; m++)
+                {
+                    slots[m] = MaterialTextures{};
+                    for (int k = 0; k < GPT_TEX_SLOTS; k++)
+                    {
+                        const int32_t ti = d.material_textures[static_cast<size_t>(m) * GPT_TEX_SLOTS + k];
+                        if (ti < 0) continue;
+                        if (static_cast<uint32_t>(ti) >= d.texture_count)
+                            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Material texture index out of range");
+                        const bool scalar = k == GPT_TEX_SHININESS;
+                        if ((d.textures[ti].channels == 1) != scalar)
+                            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Shininess maps have one channel, other maps three or four");
+                        slots[m].tex[k] = scene->textures[ti]->object;
+                    }
+                }
+                PT_TRY(scene->materialTextures.allocate(slots.size() * sizeof(MaterialTextures)));
+                PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materialTextures.get<void>(), slots.data(), slots.size() * sizeof(MaterialTextures),
+                                                           cudaMemcpyHostToDevice, stream_));
+            }
             // BVH8 on the host (binned SAH, collapse, quantisation).
             Bvh8 bvh;
             try
@@ -331,7 +432,7 @@ namespace pt
             if (lightCount > 0)
             {
                 DeviceBuffer weights, prefix, stackIndex, stackValue;
-                PT_TRY(scene->lights.allocate(static_cast<size_t>(lightCount) * 5 * sizeof(float4)));
+                PT_TRY(scene->lights.allocate(static_cast<size_t>(lightCount) * 7 * sizeof(float4)));
                 PT_TRY(scene->bins.allocate(static_cast<size_t>(lightCount) * sizeof(uint4)));
                 PT_TRY(weights.allocate(static_cast<size_t>(lightCount) * 8));
                 PT_TRY(prefix.allocate(static_cast<size_t>(lightCount) * 8));
@@ -779,6 +880,8 @@ namespace pt
                 worker_.join();
             }
             if (stream_) cudaStreamSynchronize(stream_);
+            // the cancellation request applies to the stopped simulation only
+            if (hostMapped_) *static_cast<volatile uint32_t*>(hostMapped_) = 0u;
             rendering_.store(false);
             return Status::Ok();
         }
@@ -983,6 +1086,7 @@ extern "C"
     {
         if (!r || !camera || !settings) return GPT_ERR_INVALID_ARGUMENT;
         if (r->impl->rendering_.load()) return Report(r, pt::Status::Err(GPT_ERR_STATE, "Renderer is already rendering"));
+        *static_cast<volatile uint32_t*>(r->impl->hostMapped_) = 0u;  // a synchronous frame is never cancelled
         return Report(r, r->impl->RenderFrame(*camera, *settings, stats, true));
     }
 
@@ -1094,6 +1198,15 @@ extern "C"
         if (best_ms) *best_ms = ms;
         if (candidates) *candidates = tried;
         return rc;
+    }
+
+    int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count)
+    {
+        if (!sizes) return GPT_ERR_INVALID_ARGUMENT;
+        const uint32_t all[7] = {sizeof(gpt_material), sizeof(gpt_scene_desc), sizeof(gpt_device_camera), sizeof(gpt_motion_state),
+                                 sizeof(gpt_render_settings), sizeof(gpt_frame_stats), sizeof(gpt_texture_desc)};
+        for (uint32_t i = 0; i < count && i < 7; i++) sizes[i] = all[i];
+        return GPT_OK;
     }
 
     // MakeDeviceCamera (Renderer.cpp:237-257) with glm's quaternion rotation v + 2w(q x v) + 2 q x (q x v),

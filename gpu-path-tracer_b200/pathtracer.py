@@ -33,10 +33,19 @@ class gpt_material(ctypes.Structure):
                 ("reserved", ctypes.c_float)]
 
 
+class gpt_texture_desc(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("channels", ctypes.c_uint32),
+                ("format", ctypes.c_uint32), ("data", ctypes.c_void_p)]
+
+
 class gpt_scene_desc(ctypes.Structure):
     _fields_ = [("triangle_count", ctypes.c_uint32), ("positions", ctypes.c_void_p), ("normals", ctypes.c_void_p),
                 ("tangents", ctypes.c_void_p), ("uvs", ctypes.c_void_p), ("material_ids", ctypes.c_void_p),
-                ("material_count", ctypes.c_uint32), ("materials", ctypes.c_void_p)]
+                ("material_count", ctypes.c_uint32), ("materials", ctypes.c_void_p), ("texture_count", ctypes.c_uint32),
+                ("textures", ctypes.c_void_p), ("material_textures", ctypes.c_void_p)]
+
+
+TEXEL_U8_SRGB, TEXEL_U8_LINEAR, TEXEL_F32 = 0, 1, 2
 
 
 class gpt_device_camera(ctypes.Structure):
@@ -116,6 +125,7 @@ _SIGNATURES = [
     ("gpt_obj_scene_desc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc)]),
     ("gpt_obj_material_name", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t]),
     ("gpt_obj_free", None, [ctypes.c_void_p]),
+    ("gpt_abi_struct_sizes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32]),
     ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
                                               ctypes.POINTER(gpt_device_camera)]),
 ]
@@ -198,10 +208,8 @@ class Renderer:
         self._check(self.L.gpt_init_rendering_buffers(self.h, width, height), "gpt_init_rendering_buffers")
 
     def upload_scene(self, scene):
-        s = scene.contiguous()
-        desc = gpt_scene_desc(s.triangle_count, _ptr(s.positions).value, _ptr(s.normals).value, _ptr(s.tangents).value,
-                              _ptr(s.uvs).value, _ptr(s.material_ids).value, len(s.materials), _ptr(s.materials).value)
-        self._scene_keep = s
+        desc, keep = scene_desc_with_textures(scene)
+        self._scene_keep = keep
         self._check(self.L.gpt_init_scene_buffers(self.h, ctypes.byref(desc)), "gpt_init_scene_buffers")
 
     def scene_info(self) -> dict:
@@ -343,10 +351,40 @@ class Renderer:
                     done_samples=self.L.gpt_get_done_samples(self.h), total_samples=self.L.gpt_get_total_samples(self.h))
 
 
-def scene_desc(scene) -> gpt_scene_desc:
+def scene_desc_with_textures(scene):
+    """gpt_scene_desc of a scenes.Scene plus the objects that must stay alive while it is used."""
     s = scene.contiguous()
-    return gpt_scene_desc(s.triangle_count, _ptr(s.positions).value, _ptr(s.normals).value, _ptr(s.tangents).value,
-                          _ptr(s.uvs).value, _ptr(s.material_ids).value, len(s.materials), _ptr(s.materials).value)
+    keep = [s]
+    desc = gpt_scene_desc(s.triangle_count, _ptr(s.positions).value, _ptr(s.normals).value, _ptr(s.tangents).value,
+                          _ptr(s.uvs).value, _ptr(s.material_ids).value, len(s.materials), _ptr(s.materials).value,
+                          0, None, None)
+    textures = getattr(s, "textures", None) or []
+    if textures:
+        arr = (gpt_texture_desc * len(textures))()
+        for i, t in enumerate(textures):
+            data = np.ascontiguousarray(t["data"])
+            keep.append(data)
+            h, w, c = data.shape
+            arr[i] = gpt_texture_desc(w, h, c, int(t["format"]), _ptr(data).value)
+        slots = np.ascontiguousarray(s.material_textures, dtype=np.int32)
+        keep += [arr, slots]
+        desc.texture_count = len(textures)
+        desc.textures = ctypes.cast(arr, ctypes.c_void_p)
+        desc.material_textures = _ptr(slots).value
+    return desc, keep
+
+
+def scene_desc(scene) -> gpt_scene_desc:
+    return scene_desc_with_textures(scene)[0]
+
+
+def abi_struct_sizes() -> dict:
+    """sizeof() of the public structs as compiled into the library."""
+    out = (ctypes.c_uint32 * 8)()
+    lib().gpt_abi_struct_sizes(out, 8)
+    names = ["gpt_material", "gpt_scene_desc", "gpt_device_camera", "gpt_motion_state", "gpt_render_settings",
+             "gpt_frame_stats", "gpt_texture_desc"]
+    return {n: out[i] for i, n in enumerate(names)}
 
 
 def bvh8_check(scene) -> dict:

@@ -105,6 +105,8 @@ class Scene:
     materials: np.ndarray      # [M] MATERIAL_DTYPE
     name: str = "scene"
     camera: dict = field(default_factory=dict)
+    textures: list = field(default_factory=list)      # [{"data": [H, W, C] u8/f32 array, "format": 0/1/2}]
+    material_textures: np.ndarray | None = None       # [M, 6] int32 texture index per slot, -1 = constant
 
     @property
     def triangle_count(self) -> int:
@@ -264,6 +266,46 @@ def cornell_all_models(seed: int = 1) -> Scene:
     add(_quad([0.38, 0.999, 0.38], [0.62, 0.999, 0.38], [0.62, 0.999, 0.62], [0.38, 0.999, 0.62], [0, -1, 0]), 8)
     cam = dict(position=(0.5, 0.5, 2.0), look_at=(0.5, 0.5, 0.0), fov_y=40.0)
     return _assemble(parts, mats, "cornell-all-models", cam)
+
+
+TEXEL_U8_SRGB, TEXEL_U8_LINEAR, TEXEL_F32 = 0, 1, 2
+SLOT_COLOR, SLOT_SPECULAR, SLOT_SHININESS, SLOT_RMA, SLOT_EMISSION, SLOT_NORMAL = range(6)
+
+
+def cornell_textured(seed: int = 1) -> Scene:
+    """The all-models Cornell box with image textures in every material slot somewhere: a checker
+    albedo (sRGB) on the floor and back wall, a bump normal map on the floor, a shininess map on
+    the Phong ceiling, an RMA map on the GGX walls, a specular map on the mirror box and an HDR
+    emission map on the light."""
+    rng = np.random.default_rng(seed)
+    s = cornell_all_models(seed)
+    yy, xx = np.mgrid[0:64, 0:64]
+    checker = ((xx // 8 + yy // 8) % 2).astype(np.float64)
+    albedo = np.stack([60 + 150 * checker, 80 + 120 * (1 - checker), np.full_like(checker, 140)], -1).astype(np.uint8)
+    hx = np.sin(xx / 64 * 2 * np.pi * 4) * 0.35
+    hy = np.cos(yy / 64 * 2 * np.pi * 3) * 0.35
+    nrm = np.stack([hx, hy, np.ones_like(hx)], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    normal = np.round((nrm * 0.5 + 0.5) * 255).astype(np.uint8)
+    shin = rng.integers(20, 200, (16, 16, 1)).astype(np.uint8)
+    rma = np.stack([rng.integers(30, 230, (16, 16)), rng.integers(0, 256, (16, 16)), np.full((16, 16), 255)], -1).astype(np.uint8)
+    spec = rng.integers(150, 256, (16, 16, 3)).astype(np.uint8)
+    emis = (rng.random((8, 8, 3)) * np.array([17.0, 12.0, 4.0]) * 1.5).astype(np.float32)
+    s.textures = [dict(data=albedo, format=TEXEL_U8_SRGB), dict(data=normal, format=TEXEL_U8_LINEAR),
+                  dict(data=shin, format=TEXEL_U8_LINEAR), dict(data=rma, format=TEXEL_U8_LINEAR),
+                  dict(data=spec, format=TEXEL_U8_SRGB), dict(data=emis, format=TEXEL_F32)]
+    slots = np.full((len(s.materials), 6), -1, dtype=np.int32)
+    slots[0, SLOT_COLOR] = 0      # floor: albedo + normal map
+    slots[0, SLOT_NORMAL] = 1
+    slots[1, SLOT_SHININESS] = 2  # phong ceiling
+    slots[2, SLOT_COLOR] = 0      # GGX back wall: albedo + rma
+    slots[2, SLOT_RMA] = 3
+    slots[4, SLOT_RMA] = 3        # GGX right wall
+    slots[5, SLOT_SPECULAR] = 4   # mirror box
+    slots[8, SLOT_EMISSION] = 5   # light
+    s.material_textures = slots
+    s.name = "cornell-textured"
+    return s
 
 
 # ----------------------------------------------------------------------------
@@ -429,6 +471,8 @@ def config_scene(name: str) -> Scene:
         return cornell_box(1)
     if name == "cornell-all":
         return cornell_all_models(1)
+    if name == "cornell-textured":
+        return cornell_textured(1)
     table = {
         "spheres-1m": (64, 5, 256, 2),
         "spheres-10k": (2, 4, 16, 3),

@@ -60,6 +60,27 @@ typedef struct gpt_material {
 } gpt_material;
 
 /*
+ * Image texture of a material slot (Texture::Create2D, Core/Source/Graphics/Cuda/Resources/Texture.cpp:65-189):
+ * sampled with normalised coordinates, clamp addressing and bilinear filtering; u8 texels are read as
+ * normalised floats, with hardware sRGB decode for GPT_TEXEL_U8_SRGB; 3-channel images are expanded
+ * to 4 channels (alpha 255 / 1.0). Rows are stored top row first, width * channels texels each.
+ */
+enum gpt_texel_format { GPT_TEXEL_U8_SRGB = 0, GPT_TEXEL_U8_LINEAR = 1, GPT_TEXEL_F32 = 2 };
+typedef struct gpt_texture_desc {
+    uint32_t width;
+    uint32_t height;
+    uint32_t channels;            /* 1, 3 or 4 */
+    uint32_t format;              /* gpt_texel_format */
+    const void* data;
+} gpt_texture_desc;
+
+/* Texture slots of a material (Material.hpp:73-87). */
+enum gpt_texture_slot {
+    GPT_TEX_COLOR = 0, GPT_TEX_SPECULAR = 1, GPT_TEX_SHININESS = 2, GPT_TEX_RMA = 3, GPT_TEX_EMISSION = 4,
+    GPT_TEX_NORMAL = 5, GPT_TEX_SLOTS = 6
+};
+
+/*
  * Scene upload, replacing InitializeSceneBuffers(entt::registry, Assets::Storage)
  * (Renderer.hpp:115, Renderer.cpp:292-306). The arrays are the output of the
  * reference's BuildTriangles (Renderer.cpp:159-213): world-space per-triangle
@@ -74,6 +95,9 @@ typedef struct gpt_scene_desc {
     const uint32_t* material_ids; /* [T] index into materials */
     uint32_t material_count;
     const gpt_material* materials;
+    uint32_t texture_count;       /* optional image textures (0 = constant materials only) */
+    const gpt_texture_desc* textures;
+    const int32_t* material_textures; /* [material_count][GPT_TEX_SLOTS] texture index, -1 = the material's constant */
 } gpt_scene_desc;
 
 /* DeviceCamera (Core/Include/Core/Graphics/Cuda/PathTracing/DeviceCamera.hpp:5-11). */
@@ -259,6 +283,11 @@ int gpt_obj_load(const char* path, const float* transform, gpt_obj_scene** out);
 int gpt_obj_scene_desc(const gpt_obj_scene* scene, gpt_scene_desc* desc);
 int gpt_obj_material_name(const gpt_obj_scene* scene, uint32_t index, char* buffer, size_t length);
 void gpt_obj_free(gpt_obj_scene* scene);
+
+/* sizeof() of the public structs as compiled into this library, in the order gpt_material,
+ * gpt_scene_desc, gpt_device_camera, gpt_motion_state, gpt_render_settings, gpt_frame_stats,
+ * gpt_texture_desc (for binding checks from other languages). */
+int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count);
 
 /* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */
 int gpt_make_device_camera(float fov_y, float aspect, const gpt_motion_state* state, gpt_device_camera* out);

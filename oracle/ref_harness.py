@@ -20,6 +20,7 @@ REF_MATERIAL_DTYPE = np.dtype([("model", "<u4"), ("color", "<u4"), ("specular", 
                                ("rma", "<u4"), ("normal", "<u4"), ("emission", "<f4", 3), ("ior", "<f4"),
                                ("transmission", "<f4"), ("pad", "<u4")])
 assert REF_MATERIAL_DTYPE.itemsize == 48
+IMAGE_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("channels", "<u4"), ("format", "<u4"), ("data", "<u8")])
 
 
 def available() -> bool:
@@ -32,7 +33,7 @@ def lib(fma: bool = True):
         L = ctypes.CDLL(LIB_PATH if fma else LIB_PATH_NOFMA)
         vp, u32 = ctypes.c_void_p, ctypes.c_uint32
         L.ref_scene_create.restype = vp
-        L.ref_scene_create.argtypes = [u32, vp, vp, vp, vp, vp, u32, vp, ctypes.POINTER(ctypes.c_int)]
+        L.ref_scene_create.argtypes = [u32, vp, vp, vp, vp, vp, u32, vp, ctypes.POINTER(ctypes.c_int), u32, vp, vp]
         L.ref_scene_destroy.argtypes = [vp]
         L.ref_scene_info.argtypes = [vp, vp, vp, vp]
         L.ref_scene_decoded_materials.argtypes = [vp, vp]
@@ -81,8 +82,26 @@ class RefScene:
         self.scene = s
         self.refmats = reference_materials(s.materials)
         status = ctypes.c_int(1)
+        images = None
+        slots = None
+        self._keep = []
+        textures = getattr(s, "textures", None) or []
+        if textures:
+            images = np.zeros(len(textures), dtype=IMAGE_DTYPE)
+            for i, t in enumerate(textures):
+                data = np.asarray(t["data"])
+                if data.shape[2] == 3:  # Import::ConvertRgbToRgba
+                    alpha = np.full(data.shape[:2] + (1,), 255 if data.dtype == np.uint8 else 1.0, dtype=data.dtype)
+                    data = np.concatenate([data, alpha], -1)
+                data = np.ascontiguousarray(data)
+                self._keep.append(data)
+                images[i] = (data.shape[1], data.shape[0], data.shape[2], int(t["format"]), data.ctypes.data)
+            slots = np.ascontiguousarray(s.material_textures, dtype=np.int32)
+            self._keep += [images, slots]
         self.h = self.L.ref_scene_create(s.triangle_count, _p(s.positions), _p(s.normals), _p(s.tangents), _p(s.uvs),
-                                        _p(s.material_ids), len(s.materials), _p(self.refmats), ctypes.byref(status))
+                                        _p(s.material_ids), len(s.materials), _p(self.refmats), ctypes.byref(status),
+                                        len(textures), _p(images) if images is not None else None,
+                                        _p(slots) if slots is not None else None)
         if not self.h or status.value != 0:
             raise RuntimeError("ref_scene_create failed")
 

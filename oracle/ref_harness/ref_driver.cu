@@ -78,6 +78,35 @@ namespace
         return cudaCreateTextureObject(&t.object, &res, &td, nullptr) == cudaSuccess;
     }
 
+    // Image texture with Texture::Create2D's descriptors; channels 1 or 4 (3-channel data is
+    // expanded by the caller), format 0 = u8 sRGB, 1 = u8 linear, 2 = f32.
+    bool make_image_texture(Texture& t, const void* data, int w, int h, int channels, int format)
+    {
+        const bool u8 = format != 2;
+        cudaChannelFormatDesc desc = u8 ? (channels == 1 ? cudaCreateChannelDesc<uchar1>() : cudaCreateChannelDesc<uchar4>())
+                                        : (channels == 1 ? cudaCreateChannelDesc<float1>() : cudaCreateChannelDesc<float4>());
+        if (cudaMallocArray(&t.array, &desc, w, h) != cudaSuccess) return false;
+        const size_t pitch = static_cast<size_t>(w) * channels * (u8 ? 1 : 4);
+        if (cudaMemcpy2DToArray(t.array, 0, 0, data, pitch, pitch, h, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+        cudaResourceDesc res{};
+        res.resType = cudaResourceTypeArray;
+        res.res.array.array = t.array;
+        cudaTextureDesc td{};
+        td.addressMode[0] = cudaAddressModeClamp;
+        td.addressMode[1] = cudaAddressModeClamp;
+        td.filterMode = cudaFilterModeLinear;
+        td.normalizedCoords = 1;
+        td.sRGB = format == 0 ? 1 : 0;
+        td.readMode = u8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
+        return cudaCreateTextureObject(&t.object, &res, &td, nullptr) == cudaSuccess;
+    }
+
+    struct ImageDesc  // 24 bytes, see oracle/ref_harness.py
+    {
+        uint32_t width, height, channels, format;
+        const void* data;  // channels 1 or 4
+    };
+
     bool make_f32_texture(Texture& t, const float* rgba)
     {
         cudaChannelFormatDesc desc = cudaCreateChannelDesc<float4>();
@@ -290,8 +319,10 @@ extern "C"
     void ref_scene_destroy(void* s) { delete static_cast<Scene*>(s); }
 
     void* ref_scene_create(uint32_t n, const float* positions, const float* normals, const float* tangents, const float* uvs,
-                           const uint32_t* materialIds, uint32_t materialCount, const void* materialsIn, int* status)
+                           const uint32_t* materialIds, uint32_t materialCount, const void* materialsIn, int* status,
+                           uint32_t imageCount, const void* imagesIn, const int32_t* materialImages)
     {
+        const ImageDesc* images = static_cast<const ImageDesc*>(imagesIn);
         *status = 1;
         auto* scene = new Scene();
         const RefMaterial* mats = static_cast<const RefMaterial*>(materialsIn);
@@ -315,6 +346,20 @@ extern "C"
             ok = ok && make_f32_texture(emis, e);
             unpack_rgb(rm.normalU8, px);
             ok = ok && make_u8_texture(norm, px, 4, false);
+            // image textures replace the slot's 1x1 texel (Manager.cpp:337-355: file texture or pixel texture)
+            Texture* slots[6] = {&color, &spec, &shin, &rma, &emis, &norm};
+            if (materialImages)
+                for (int k = 0; k < 6; k++)
+                {
+                    const int32_t img = materialImages[static_cast<size_t>(m) * 6 + k];
+                    if (img < 0 || static_cast<uint32_t>(img) >= imageCount) continue;
+                    Texture tex;
+                    const ImageDesc& d = images[img];
+                    ok = ok && make_image_texture(tex, d.data, static_cast<int>(d.width), static_cast<int>(d.height),
+                                                  static_cast<int>(d.channels), static_cast<int>(d.format));
+                    scene->textures.push_back(*slots[k]);  // keep the replaced 1x1 texture for cleanup
+                    *slots[k] = tex;
+                }
             for (Texture* t : {&color, &spec, &shin, &rma, &emis, &norm}) scene->textures.push_back(*t);
             if (!ok)
             {

@@ -47,3 +47,54 @@ extern "C" int philox_kat(const unsigned long long* subseq, int n, const unsigne
     if (cudaGetLastError() != cudaSuccess) return 1;
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 2;
 }
+
+// Test-only: samples of a texture created with the renderer's descriptors (clamp, linear
+// filter, normalised coordinates), to pin the oracle's texture sampling against the hardware.
+// format: 0 = u8 sRGB, 1 = u8 linear, 2 = f32; channels 1 or 4.
+__global__ void texture_kat_kernel(cudaTextureObject_t tex, int channels, const float* uv, int n, float* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (channels == 1)
+        out[i] = tex2D<float>(tex, uv[2 * i], uv[2 * i + 1]);
+    else
+    {
+        float4 v = tex2D<float4>(tex, uv[2 * i], uv[2 * i + 1]);
+        out[4 * i] = v.x; out[4 * i + 1] = v.y; out[4 * i + 2] = v.z; out[4 * i + 3] = v.w;
+    }
+}
+
+extern "C" int texture_kat(const void* texels, int width, int height, int channels, int format, const float* uvHost, int n, float* outHost)
+{
+    const bool u8 = format != 2;
+    cudaChannelFormatDesc cd = u8 ? (channels == 1 ? cudaCreateChannelDesc<uchar1>() : cudaCreateChannelDesc<uchar4>())
+                                  : (channels == 1 ? cudaCreateChannelDesc<float1>() : cudaCreateChannelDesc<float4>());
+    cudaArray_t arr;
+    if (cudaMallocArray(&arr, &cd, width, height) != cudaSuccess) return 1;
+    size_t pitch = (size_t)width * channels * (u8 ? 1 : 4);
+    if (cudaMemcpy2DToArray(arr, 0, 0, texels, pitch, pitch, height, cudaMemcpyHostToDevice) != cudaSuccess) return 2;
+    cudaResourceDesc res{};
+    res.resType = cudaResourceTypeArray;
+    res.res.array.array = arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeClamp;
+    td.addressMode[1] = cudaAddressModeClamp;
+    td.filterMode = cudaFilterModeLinear;
+    td.normalizedCoords = 1;
+    td.sRGB = format == 0 ? 1 : 0;
+    td.readMode = u8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
+    cudaTextureObject_t tex;
+    if (cudaCreateTextureObject(&tex, &res, &td, nullptr) != cudaSuccess) return 3;
+    float *uvD, *outD;
+    cudaMalloc(&uvD, sizeof(float) * 2 * n);
+    cudaMalloc(&outD, sizeof(float) * channels * n);
+    cudaMemcpy(uvD, uvHost, sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    texture_kat_kernel<<<(n + 127) / 128, 128>>>(tex, channels, uvD, n, outD);
+    int rc = cudaDeviceSynchronize() == cudaSuccess ? 0 : 4;
+    cudaMemcpy(outHost, outD, sizeof(float) * channels * n, cudaMemcpyDeviceToHost);
+    cudaFree(uvD);
+    cudaFree(outD);
+    cudaDestroyTextureObject(tex);
+    cudaFreeArray(arr);
+    return rc;
+}

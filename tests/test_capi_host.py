@@ -87,3 +87,9 @@ def test_scene_validation_rejects_bad_material_index():
                        np.full(36, 99, np.uint32), s.materials.copy())
     with pytest.raises(pathtracer.GptError):
         pathtracer.bvh8_check(bad)
+
+
+def test_python_binding_struct_layouts_match_the_library():
+    sizes = pathtracer.abi_struct_sizes()
+    for name, size in sizes.items():
+        assert ctypes.sizeof(getattr(pathtracer, name)) == size, name

@@ -235,6 +235,13 @@ def test_simulation_thread_frames_stop_resume(gpu_renderer, scene_factory):
     assert not gpu_renderer.is_rendering()
     assert gpu_renderer.progress()["done_frames"] < 12
     assert gpu_renderer.last_error() is None
+    # a stopped simulation does not cut later frames short
+    cam = scenes.scene_camera(s, 32, 32)
+    st = gpu_renderer.render_frame(cam, 32, 32, 4, 8, True)
+    assert st["samples"] == 4 * 32 * 32
+    ref = oracle.OracleScene(s).render(cam, 32, 32, 4, 8, True)
+    assert st["iterations"] == ref["iterations"]
+    assert np.array_equal(gpu_renderer.sample_radiance().view(np.uint32), ref["sample_radiance"].view(np.uint32))
 
 
 def test_host_loop_matches_graph_loop(gpu_renderer, scene_factory, oracle_scene):
