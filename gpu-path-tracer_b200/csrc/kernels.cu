@@ -43,6 +43,14 @@ namespace pt
         return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
     }
 
+    // Warp-aggregated atomicAdd(ptr, 1) where lanes with equal key share ptr: one atomic per key.
+    __device__ __forceinline__ void agg_increment_keyed(uint32_t* ptr, uint32_t key)
+    {
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, key);
+        if (static_cast<int>(lane_id()) == __ffs(peers) - 1) atomicAdd(ptr, static_cast<uint32_t>(__popc(peers)));
+    }
+
     __device__ __forceinline__ unsigned long long global_ns()
     {
         unsigned long long t;
@@ -159,7 +167,9 @@ namespace pt
     {
         SceneView sc;
         Wavefront wf;
+        const SceneEntry* scenes;  // nullptr: one scene rooted at node 0
         static constexpr int kPhase = 0;
+        __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
         __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->rayCount[wf.ctr->cur]; }
         __device__ uint32_t* cursor() const { return &wf.ctr->traceCursor; }
@@ -184,7 +194,7 @@ namespace pt
             else
             {
                 const uint32_t pos = agg_push(&wf.ctr->regenCount);
-                wf.regen[pos] = slot;
+                wf.regen[pos] = slot & kSlotMask;
             }
         }
     };
@@ -202,7 +212,9 @@ namespace pt
     {
         SceneView sc;
         Wavefront wf;
+        const SceneEntry* scenes;
         static constexpr int kPhase = 2;
+        __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
         __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->shadowCount; }
         __device__ uint32_t* cursor() const { return &wf.ctr->shadowCursor; }
@@ -215,9 +227,10 @@ namespace pt
             tmax = b.w;
             tag = __float_as_uint(a.w);
         }
-        __device__ void finish(uint32_t i, uint32_t slot, const HitRecord&, bool occluded) const
+        __device__ void finish(uint32_t i, uint32_t tag, const HitRecord&, bool occluded) const
         {
             if (occluded) return;
+            const uint32_t slot = tag & kSlotMask;
             const float4 l = wf.shL[i];
             const float3 add = clamp_radiance(make_float3(l.x, l.y, l.z), 20.0f);
             float4 acc = wf.slotL[slot];
@@ -237,7 +250,9 @@ namespace pt
         uint32_t* triOut;
         float* uvtOut;
         uint8_t* occOut;
+        uint32_t rootNode;
         static constexpr int kPhase = 0;
+        __device__ uint32_t root(uint32_t) const { return rootNode; }
         __device__ Counters* counters() const { return nullptr; }
         __device__ uint32_t count() const { return n; }
         __device__ uint32_t* cursor() const { return cursorPtr; }
@@ -308,7 +323,7 @@ namespace pt
                         st.hit.u = 0.0f;
                         st.hit.v = 0.0f;
                         st.hit.model = 0;
-                        st.pending = 0;
+                        st.pending = work.root(tag);
                         st.sp = 0;
                         active = true;
                     }
@@ -351,7 +366,10 @@ namespace pt
     }
 
     // ------------------------------------------------------------------ paths
-    __device__ __forceinline__ uint32_t pack_meta(uint32_t depth, bool delta) { return depth | (delta ? 0x100u : 0u); }
+    __device__ __forceinline__ uint32_t pack_meta(uint32_t depth, bool delta, uint32_t job)
+    {
+        return depth | (delta ? 0x100u : 0u) | (job << 16);
+    }
 
     // ComputePathSample + GenerateCameraRay (PathGeneration.cu:15-54).
     __device__ __forceinline__ void camera_ray(const JobView& job, uint64_t sampleIndex, float2 jitter, float3& o, float3& d)
@@ -378,7 +396,7 @@ namespace pt
 
     // New path for a sample in a slot: Philox stream (seed 1234, subsequence = sample), jitter from
     // the first uniform4, throughput 1, depth 0, delta flag set (PathGeneration.cu:56-102).
-    __device__ __forceinline__ void start_path(const JobView& job, const Wavefront& wf, uint32_t slot, uint32_t sample,
+    __device__ __forceinline__ void start_path(const JobView& job, uint32_t jobIndex, const Wavefront& wf, uint32_t slot, uint32_t sample,
                                                uint32_t queue, uint32_t position)
     {
         curandStatePhilox4_32_10_t rng;
@@ -386,10 +404,10 @@ namespace pt
         const float4 r = curand_uniform4(&rng);
         float3 o, d;
         camera_ray(job, sample, make_float2(r.x, r.y), o, d);
-        wf.slotT[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pack_meta(0, true)));
+        wf.slotT[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pack_meta(0, true, jobIndex)));
         wf.slotL[slot] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(4u));
         wf.slotSample[slot] = sample;
-        wf.rayO[queue][position] = make_float4(o.x, o.y, o.z, __uint_as_float(slot));
+        wf.rayO[queue][position] = make_float4(o.x, o.y, o.z, __uint_as_float(slot | (job.scene << kSlotBits)));
         wf.rayD[queue][position] = make_float4(d.x, d.y, d.z, kMaxT);
     }
 
@@ -430,7 +448,7 @@ namespace pt
         const JobView job = *jobPtr;
         const uint32_t n = wf.ctr->rayCount[0];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-            start_path(job, wf, i, i, 0, i);
+            start_path(job, 0, wf, i, i, 0, i);
     }
 
     // ------------------------------------------------------------------ shading (MaterialEval.cu)
@@ -573,14 +591,22 @@ namespace pt
         float distanceSquared, pdf;
     };
 
-    // SampleLightTriangle (MaterialEval.cu:171-192) with the alias table (AliasTableView.hpp:32-60).
-    __device__ __forceinline__ LightHit sample_light(const SceneView& sc, float uSel, float2 xi, float3 hitPoint)
+    // The lights of one resident scene: a slice of the packed light list and alias table.
+    struct LightSet
     {
-        const uint32_t n = sc.lightCount;
+        uint32_t base, count;
+    };
+
+    // SampleLightTriangle (MaterialEval.cu:171-192) with the alias table (AliasTableView.hpp:32-60).
+    // Requires ls.count > 0 (NEE is off for scenes without emitters).
+    __device__ __forceinline__ LightHit sample_light(const SceneView& sc, LightSet ls, float uSel, float2 xi, float3 hitPoint)
+    {
+        const uint32_t n = ls.count;
         const float scaledU = uSel * static_cast<float>(n);
         uint32_t bin = static_cast<uint32_t>(scaledU);
         bin = bin < n - 1u ? bin : n - 1u;
         const float up = fminf(scaledU - static_cast<float>(bin), kOneMinusEpsilon);
+        bin += ls.base;
         const uint4 b = ldg4(sc.bins + bin);
         uint32_t index = bin;
         float pmf = __uint_as_float(b.y);
@@ -641,12 +667,12 @@ namespace pt
     }
 
     // Lambert NEE, EvaluateDiffuseDirect (:231-268); Phong NEE adds the lobe (:410-455).
-    __device__ __forceinline__ ShadowOut direct_lambert_phong(const SceneView& sc, float3 T, float3 dir, const Surface& s, const Frame& f,
+    __device__ __forceinline__ ShadowOut direct_lambert_phong(const SceneView& sc, LightSet ls, float3 T, float3 dir, const Surface& s, const Frame& f,
                                                               float3 rs, float3 albedo, bool phong, float3 specular, float shininess)
     {
         ShadowOut none;
         none.valid = false;
-        const LightHit lh = sample_light(sc, rs.x, make_float2(rs.y, rs.z), s.position);
+        const LightHit lh = sample_light(sc, ls, rs.x, make_float2(rs.y, rs.z), s.position);
         if (lh.distanceSquared < 1e-6f) return none;
         const float cosThetaI = fmaxf(dot(f.normal, lh.wi), 0.0f);
         const float gCos = fmaxf(dot(s.gN, lh.wi), 0.0f);
@@ -727,12 +753,12 @@ namespace pt
     }
 
     // EvaluateGgxDirect (:652-718)
-    __device__ __forceinline__ ShadowOut direct_ggx(const SceneView& sc, float3 T, float3 dir, const Surface& s, const Frame& f, float3 rs,
+    __device__ __forceinline__ ShadowOut direct_ggx(const SceneView& sc, LightSet ls, float3 T, float3 dir, const Surface& s, const Frame& f, float3 rs,
                                                     float3 base, float alpha, float metallic, float ior)
     {
         ShadowOut none;
         none.valid = false;
-        const LightHit lh = sample_light(sc, rs.x, make_float2(rs.y, rs.z), s.position);
+        const LightHit lh = sample_light(sc, ls, rs.x, make_float2(rs.y, rs.z), s.position);
         if (lh.distanceSquared < 1e-6f || lh.pdf <= 0.0f) return none;
         if (dot(s.gN, lh.wi) <= 0.0f) return none;
         const float cosThetaLight = fmaxf(dot(lh.gN, f3(0.0f) - lh.wi), 0.0f);
@@ -855,17 +881,17 @@ namespace pt
         return out;
     }
 
-    // One kernel per shading model; grid-stride over the model's queue.
+    // One kernel per shading model; grid-stride over the model's queue. A path's job (its depth
+    // limit, NEE switch and Philox offset) comes from its slot metadata, its scene (lights) from
+    // the ray tag; NEE is off in scenes without emitters.
     template <uint32_t MODEL>
-    __global__ void __launch_bounds__(128) shade_kernel(SceneView sc, Wavefront wf, const JobView* jobPtr)
+    __global__ void __launch_bounds__(128) shade_kernel(SceneView sc, Wavefront wf, const JobView* jobs, const SceneEntry* scenes)
     {
         Counters* ctr = wf.ctr;
         phase_begin(ctr, 1);
         const uint32_t n = ctr->matCount[MODEL];
         const uint32_t cur = ctr->cur;
         const uint32_t nxt = cur ^ 1u;
-        const uint32_t limit = jobPtr->depthLimit;
-        const bool nee = jobPtr->nee != 0;
         const uint32_t* queue = wf.matQ[MODEL];
         for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
         {
@@ -873,7 +899,8 @@ namespace pt
             const float4 o4 = wf.rayO[cur][r];
             const float4 d4 = wf.rayD[cur][r];
             const float4 h4 = wf.hit[r];
-            const uint32_t slot = __float_as_uint(o4.w);
+            const uint32_t tag = __float_as_uint(o4.w);
+            const uint32_t slot = tag & kSlotMask;
             const float3 o = f3(o4), d = f3(d4);
             const float tHit = h4.w;
             const uint32_t tri = __float_as_uint(h4.x);
@@ -882,6 +909,12 @@ namespace pt
             const uint32_t meta = __float_as_uint(T4.w);
             const uint32_t depth = meta & 0xFFu;
             const bool delta = (meta & 0x100u) != 0;
+            const uint32_t jobIndex = meta >> 16;
+            const JobView& job = jobs[jobIndex];
+            const uint32_t limit = __ldg(&job.depthLimit);
+            const uint4 se = __ldg(reinterpret_cast<const uint4*>(scenes) + (tag >> kSlotBits));
+            const LightSet ls{se.y, se.z};
+            const bool nee = __ldg(&job.nee) != 0 && ls.count > 0;
             const float3 T = f3(T4);
             uint32_t rngPos = __float_as_uint(L4.w);
             bool terminated = true;
@@ -926,7 +959,7 @@ namespace pt
                 const MaterialDev& m = sc.materials[s.material];
                 const Frame f = shading_frame(sc, s, m);
                 curandStatePhilox4_32_10_t rng;
-                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + jobPtr->rngOffset,
+                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + __ldg(&job.rngOffset),
                             static_cast<unsigned long long>(rngPos), &rng);
                 if (MODEL == 1)  // Diffuse (:311-350, :270-309)
                 {
@@ -937,7 +970,7 @@ namespace pt
                     {
                         const float4 dir4 = curand_uniform4(&rng);
                         rngPos += 4;
-                        sh = direct_lambert_phong(sc, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
+                        sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
                     }
                     const float3 wi = f.from_local(cosine_hemisphere(make_float2(ind.x, ind.y)));
                     const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
@@ -968,7 +1001,7 @@ namespace pt
                     const float shininess = slot_scalar(sc, s.material, 2, s.uv, &m.shininess) * (1000.0f - 1.0f) + 1.0f;
                     const float4 ind = curand_uniform4(&rng);
                     rngPos += 4;
-                    if (nee) sh = direct_lambert_phong(sc, T, d, s, f, f3(ind), albedo, true, specular, shininess);
+                    if (nee) sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(ind), albedo, true, specular, shininess);
                     const Scatter sc2 = indirect_phong(depth, T, limit, d, s, f, ind, albedo, specular, shininess);
                     terminated = sc2.terminated;
                     cont = sc2.c;
@@ -988,7 +1021,7 @@ namespace pt
                     {
                         const float4 dir4 = curand_uniform4(&rng);
                         rngPos += 4;
-                        sh = direct_ggx(sc, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
+                        sh = direct_ggx(sc, ls, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
                     }
                     const Scatter sc2 = indirect_ggx(depth, T, limit, d, s, f, ind, base, alpha, metallic, ior);
                     terminated = sc2.terminated;
@@ -1002,7 +1035,7 @@ namespace pt
             if (sh.valid)
             {
                 const uint32_t pos = agg_push(&ctr->shadowCount);
-                wf.shO[pos] = make_float4(sh.origin.x, sh.origin.y, sh.origin.z, __uint_as_float(slot));
+                wf.shO[pos] = make_float4(sh.origin.x, sh.origin.y, sh.origin.z, __uint_as_float(tag));
                 wf.shD[pos] = make_float4(sh.direction.x, sh.direction.y, sh.direction.z, sh.tMax);
                 wf.shL[pos] = make_float4(sh.radiance.x, sh.radiance.y, sh.radiance.z, 0.0f);
             }
@@ -1016,9 +1049,9 @@ namespace pt
                 // SpawnScatteredRay (:148-156)
                 const float3 origin = o + d * tHit + nextGn * 1e-4f;
                 wf.slotT[slot] = make_float4(cont.throughput.x, cont.throughput.y, cont.throughput.z,
-                                             __uint_as_float(pack_meta(cont.depth, nextDelta)));
+                                             __uint_as_float(pack_meta(cont.depth, nextDelta, jobIndex)));
                 const uint32_t pos = agg_push(&ctr->rayCount[nxt]);
-                wf.rayO[nxt][pos] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(slot));
+                wf.rayO[nxt][pos] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(tag));
                 wf.rayD[nxt][pos] = make_float4(nextDir.x, nextDir.y, nextDir.z, kMaxT);
             }
             (void)hitPos;
@@ -1051,7 +1084,7 @@ namespace pt
             dst[1] = L.y;
             dst[2] = L.z;
             if (k < regenerate)
-                start_path(*jobPtr, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
+                start_path(*jobPtr, 0, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
         }
         phase_end(ctr, 3);
     }
@@ -1105,8 +1138,30 @@ namespace pt
         if (graphLoop) cudaGraphSetConditional(handle, c->done ? 0u : 1u);
     }
 
-    // Per pixel: compensated (Kahan) FP32 sum of its samples in sample order, then
     // PostprocessKernel's tonemap (Image.cu:22-54): x/spp, Reinhard, x^(1/2.2), u8 truncation.
+    __device__ __forceinline__ uint32_t tonemap_rgba8(const float* acc, float invSpp)
+    {
+        uint32_t rgb[3];
+        for (int ch = 0; ch < 3; ch++)
+        {
+            const float hdr = acc[ch] * invSpp;
+            const float ldr = hdr / (hdr + 1.0f);
+            const float g = pow_det(ldr, 1.0f / 2.2f);
+            rgb[ch] = static_cast<uint32_t>(static_cast<unsigned char>(clampf(g * 255.0f, 0.0f, 255.0f)));
+        }
+        return rgb[0] | (rgb[1] << 8) | (rgb[2] << 16) | (255u << 24);
+    }
+
+    // One step of the compensated (Kahan) sum.
+    __device__ __forceinline__ void kahan_add(float& sum, float& comp, float x)
+    {
+        const float y = x - comp;
+        const float t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+
+    // Per pixel: compensated (Kahan) FP32 sum of its samples in sample order, then the tonemap.
     __global__ void resolve_kernel(const JobView* jobPtr, float4* accumulation, uint32_t* framebuffer)
     {
         const JobView job = *jobPtr;
@@ -1123,23 +1178,272 @@ namespace pt
                 {
                     const uint64_t si = first + k;
                     if (si >= job.totalSamples) break;
-                    const float y = job.sampleRadiance[si * 3 + ch] - comp;
-                    const float t = sum + y;
-                    comp = (t - sum) - y;
-                    sum = t;
+                    kahan_add(sum, comp, job.sampleRadiance[si * 3 + ch]);
                 }
                 acc[ch] = sum;
             }
             accumulation[p] = make_float4(acc[0], acc[1], acc[2], 0.0f);
-            uint32_t rgb[3];
-            for (int ch = 0; ch < 3; ch++)
+            framebuffer[p] = tonemap_rgba8(acc, invSpp);
+        }
+    }
+
+    // ------------------------------------------------------------------ job engine
+    // Jobs share one pool of path slots. A job hands out launch indices g in pass-major order:
+    // pass g / pixels (= the stratum), pixel g % pixels, sample pixel * spp + pass. The sample,
+    // and with it the Philox stream and the path, is the one the frame renderer traces, so the
+    // per-sample radiance is identical. Finished samples land in a ring of `ring` pass buffers;
+    // complete passes are folded in order into a per-pixel Kahan accumulator, which therefore
+    // adds every pixel's samples in the same order as resolve_kernel: the image of a job is the
+    // same alone, mixed with other jobs, and rendered by the frame renderer.
+
+    __device__ __forceinline__ uint64_t job_passes(const JobView& J)
+    {
+        return (J.totalSamples + J.pixels - 1) / J.pixels;
+    }
+
+    // Number of consecutive complete passes starting at the first unfolded one (at most `ring`).
+    __device__ __forceinline__ uint32_t foldable_passes(const JobView& J)
+    {
+        const uint64_t passes = job_passes(J);
+        uint32_t c = 0;
+        while (c < J.ring && J.folded + c < passes)
+        {
+            const uint64_t p = J.folded + c;
+            const uint64_t rem = J.totalSamples - p * J.pixels;
+            const uint32_t size = rem < J.pixels ? static_cast<uint32_t>(rem) : J.pixels;
+            if (J.passDone[p % J.ring] != size) break;
+            c++;
+        }
+        return c;
+    }
+
+    __device__ __forceinline__ uint64_t job_window_end(const JobView& J)
+    {
+        const uint64_t window = static_cast<uint64_t>(J.folded + J.ring) * J.pixels;
+        return window < J.totalSamples ? window : J.totalSamples;
+    }
+
+    __global__ void engine_init_kernel(Wavefront wf, EngineView ev, uint32_t pool)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pool; i += gridDim.x * blockDim.x) ev.freeList[i] = pool - 1u - i;
+        if (blockIdx.x != 0 || threadIdx.x != 0) return;
+        Counters* c = wf.ctr;
+        *c = Counters{};
+        for (int p = 0; p < 4; p++) c->tStart[p] = ~0ull;
+        EngineCtl* e = ev.ctl;
+        e->freeCount = pool;
+        e->launchCount = 0;
+        e->segmentCount = 0;
+        e->stalled = 0;
+    }
+
+    // One thread: hands the iteration's idle slots (finished paths + free list) to the active
+    // jobs, oldest first, within each job's ring window.
+    __global__ void plan_kernel(Wavefront wf, EngineView ev)
+    {
+        EngineCtl* e = ev.ctl;
+        const uint32_t avail = wf.ctr->regenCount + e->freeCount;
+        uint32_t launch = 0, segments = 0;
+        for (uint32_t i = 0; i < e->orderCount && launch < avail; i++)
+        {
+            const uint32_t j = ev.order[i];
+            JobView& J = ev.jobs[j];
+            if (J.state != kJobActive) continue;
+            const uint64_t end = job_window_end(J);
+            if (end <= J.launched) continue;
+            const uint64_t can = end - J.launched;
+            const uint32_t take = static_cast<uint32_t>(can < static_cast<uint64_t>(avail - launch) ? can : avail - launch);
+            ev.segments[segments] = LaunchSegment{j, launch, J.launched};
+            segments++;
+            J.launched += take;
+            launch += take;
+        }
+        e->launchCount = launch;
+        e->segmentCount = segments;
+    }
+
+    // Finished paths write their radiance into their job's ring; planned samples start in the
+    // finished slots first, then in slots popped from the free list; finished slots left over are
+    // pushed onto the free list.
+    __global__ void engine_regen_kernel(Wavefront wf, EngineView ev)
+    {
+        Counters* ctr = wf.ctr;
+        phase_begin(ctr, 3);
+        const uint32_t n = ctr->regenCount;
+        const EngineCtl* e = ev.ctl;
+        const uint32_t launch = e->launchCount;
+        const uint32_t freeCount = e->freeCount;
+        const uint32_t segmentCount = e->segmentCount;
+        const uint32_t nxt = ctr->cur ^ 1u;
+        const uint32_t base = ctr->rayCount[nxt];
+        const uint32_t total = n > launch ? n : launch;
+        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
+        {
+            uint32_t slot = 0;
+            if (k < n)
             {
-                const float hdr = acc[ch] * invSpp;
-                const float ldr = hdr / (hdr + 1.0f);
-                const float g = pow_det(ldr, 1.0f / 2.2f);
-                rgb[ch] = static_cast<uint32_t>(static_cast<unsigned char>(clampf(g * 255.0f, 0.0f, 255.0f)));
+                slot = wf.regen[k];
+                const uint32_t j = __float_as_uint(wf.slotT[slot].w) >> 16;
+                JobView& J = ev.jobs[j];
+                const uint32_t sample = wf.slotSample[slot];
+                const uint32_t pixel = sample / J.spp;
+                const uint32_t pass = sample - pixel * J.spp;
+                const uint32_t r = pass % J.ring;
+                const float4 L = wf.slotL[slot];
+                float* dst = J.sampleRadiance + (static_cast<size_t>(r) * J.pixels + pixel) * 3;
+                dst[0] = L.x;
+                dst[1] = L.y;
+                dst[2] = L.z;
+                agg_increment_keyed(&J.passDone[r], (j << 8) | r);
             }
-            framebuffer[p] = rgb[0] | (rgb[1] << 8) | (rgb[2] << 16) | (255u << 24);
+            if (k < launch)
+            {
+                if (k >= n) slot = ev.freeList[freeCount - 1u - (k - n)];
+                uint32_t lo = 0, hi = segmentCount - 1u;
+                while (lo < hi)
+                {
+                    const uint32_t mid = (lo + hi + 1u) >> 1;
+                    if (ev.segments[mid].start <= k) lo = mid;
+                    else hi = mid - 1u;
+                }
+                const LaunchSegment sg = ev.segments[lo];
+                const JobView& J = ev.jobs[sg.job];
+                const uint64_t g = sg.first + (k - sg.start);
+                const uint32_t pass = static_cast<uint32_t>(g / J.pixels);
+                const uint32_t pixel = static_cast<uint32_t>(g - static_cast<uint64_t>(pass) * J.pixels);
+                start_path(J, sg.job, wf, slot, pixel * J.spp + pass, nxt, base + k);
+            }
+            else if (k < n)
+                ev.freeList[freeCount + (k - launch)] = slot;
+        }
+        phase_end(ctr, 3);
+    }
+
+    // Folds every job's complete passes, in pass order, into its Kahan accumulator; the job's
+    // last fold also writes its tone-mapped RGBA8 image.
+    __global__ void fold_kernel(EngineView ev)
+    {
+        const uint32_t orderCount = ev.ctl->orderCount;
+        for (uint32_t i = 0; i < orderCount; i++)
+        {
+            const uint32_t j = ev.order[i];
+            const JobView& J = ev.jobs[j];
+            if (J.state != kJobActive) continue;
+            const uint32_t count = foldable_passes(J);
+            if (count == 0) continue;
+            const bool last = J.folded + count == job_passes(J);
+            const float invSpp = 1.0f / static_cast<float>(J.spp);
+            for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < J.pixels; px += gridDim.x * blockDim.x)
+            {
+                const float4 s4 = J.accum[2 * static_cast<size_t>(px)];
+                const float4 c4 = J.accum[2 * static_cast<size_t>(px) + 1];
+                float sum[3] = {s4.x, s4.y, s4.z}, comp[3] = {c4.x, c4.y, c4.z};
+                for (uint32_t q = 0; q < count; q++)
+                {
+                    const uint64_t p = static_cast<uint64_t>(J.folded) + q;
+                    if (p * J.pixels + px >= J.totalSamples) break;
+                    const float* x = J.sampleRadiance + (static_cast<size_t>(p % J.ring) * J.pixels + px) * 3;
+                    for (int ch = 0; ch < 3; ch++) kahan_add(sum[ch], comp[ch], x[ch]);
+                }
+                J.accum[2 * static_cast<size_t>(px)] = make_float4(sum[0], sum[1], sum[2], 0.0f);
+                J.accum[2 * static_cast<size_t>(px) + 1] = make_float4(comp[0], comp[1], comp[2], 0.0f);
+                if (last) J.framebuffer[px] = tonemap_rgba8(sum, invSpp);
+            }
+        }
+    }
+
+    // One thread: queue bookkeeping, fold accounting, job completion and the slice's loop
+    // condition. The slice ends when a job completes (so the host can hand out its result and
+    // admit waiting jobs), when the host rings the doorbell (a job arrived), when there is nothing
+    // left to do, or after maxSliceIterations iterations.
+    __global__ void engine_advance_kernel(Wavefront wf, EngineView ev, cudaGraphConditionalHandle handle, bool graphLoop)
+    {
+        Counters* c = wf.ctr;
+        EngineCtl* e = ev.ctl;
+        const uint32_t cur = c->cur;
+        const uint32_t nxt = cur ^ 1u;
+        const uint32_t launch = e->launchCount;
+        const uint32_t next = c->rayCount[nxt] + launch;
+        c->raysTraced += c->rayCount[cur];
+        c->shadowRaysTraced += c->shadowCount;
+        for (int p = 0; p < 4; p++)
+        {
+            if (c->tEnd[p] > c->tStart[p] && c->tStart[p] != ~0ull) c->tAccum[p] += c->tEnd[p] - c->tStart[p];
+            c->tStart[p] = ~0ull;
+            c->tEnd[p] = 0;
+        }
+        e->freeCount = e->freeCount + c->regenCount - launch;
+        c->launched += launch;
+        c->rayCount[cur] = 0;
+        c->rayCount[nxt] = next;
+        c->cur = nxt;
+        for (uint32_t m = 0; m < kModelCount; m++) c->matCount[m] = 0;
+        c->shadowCount = 0;
+        c->regenCount = 0;
+        c->traceCursor = 0;
+        c->shadowCursor = 0;
+        c->iteration += 1;
+        e->launchCount = 0;
+        e->segmentCount = 0;
+        uint32_t completed = 0;
+        bool launchable = false, unfinished = false;
+        for (uint32_t i = 0; i < e->orderCount; i++)
+        {
+            JobView& J = ev.jobs[ev.order[i]];
+            if (J.state != kJobActive) continue;
+            const uint32_t count = foldable_passes(J);
+            for (uint32_t q = 0; q < count; q++) J.passDone[(static_cast<uint64_t>(J.folded) + q) % J.ring] = 0;
+            J.folded += count;
+            if (J.folded == job_passes(J))
+            {
+                J.state = kJobDone;
+                completed++;
+                continue;
+            }
+            unfinished = true;
+            if (job_window_end(J) > J.launched) launchable = true;
+        }
+        e->completed += completed;
+        e->sliceIterations += 1;
+        const bool idle = next == 0 && !launchable;
+        if (idle && unfinished) e->stalled = 1;
+        const bool bell = ev.doorbell != nullptr && *ev.doorbell != 0u;
+        c->done = (completed > 0 || bell || idle || e->sliceIterations >= e->maxSliceIterations) ? 1u : 0u;
+        if (wf.progress != nullptr)
+        {
+            wf.progress[0] = c->launched;
+            wf.progress[1] = c->iteration;
+        }
+        if (graphLoop) cudaGraphSetConditional(handle, c->done ? 0u : 1u);
+    }
+
+    // Packing resident scenes into one set of arrays: add `offset` to one 32-bit field of every
+    // record (base points at the field of record 0, records are strideWords apart). Entries equal
+    // to kInvalid stay invalid when skipInvalid is set (alias entries without an alias).
+    __global__ void rebase_field_kernel(uint32_t* base, uint32_t n, uint32_t strideWords, uint32_t offset, bool skipInvalid)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        {
+            uint32_t* f = base + static_cast<size_t>(i) * strideWords;
+            if (skipInvalid && *f == kInvalid) continue;
+            *f += offset;
+        }
+    }
+
+    // Child references of BVH8 nodes: inner children by nodeOffset, leaf ranges by triOffset.
+    __global__ void rebase_nodes_kernel(Node8* nodes, uint32_t n, uint32_t nodeOffset, uint32_t triOffset)
+    {
+        for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        {
+            Node8& nd = nodes[i];
+            const uint32_t inner = nd.w[0].w >> 24;
+            const uint32_t leaf = nd.w[6].z & 0xFFu;
+            uint32_t* refs = reinterpret_cast<uint32_t*>(&nd.w[4]);
+            for (int k = 0; k < 8; k++)
+            {
+                if ((inner >> k) & 1u) refs[k] += nodeOffset;
+                else if ((leaf >> k) & 1u) refs[k] += triOffset;
+            }
         }
     }
 
@@ -1391,10 +1695,25 @@ namespace pt
         return sms * perSm;
     }
 
+    static cudaError_t launch_shade(uint32_t m, int blocks, const SceneView& sc, const Wavefront& wf, const JobView* jobs,
+                                    const SceneEntry* scenes, cudaStream_t s)
+    {
+        switch (m)
+        {
+            case 0: shade_kernel<0><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 1: shade_kernel<1><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 2: shade_kernel<2><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 3: shade_kernel<3><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 4: shade_kernel<4><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            default: shade_kernel<5><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+        }
+        return cudaGetLastError();
+    }
+
     cudaError_t launch_iteration(const IterationLaunch& L, cudaStream_t s)
     {
         cudaError_t e;
-        WavefrontClosest wc{L.scene, L.wf};
+        WavefrontClosest wc{L.scene, L.wf, nullptr};
         if (L.traceStart && (e = cudaEventRecord(L.traceStart, s)) != cudaSuccess) return e;
         e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
@@ -1402,26 +1721,67 @@ namespace pt
         for (uint32_t m = 0; m < kModelCount; m++)
         {
             if (!L.modelPresent[m]) continue;
-            switch (m)
-            {
-                case 0: shade_kernel<0><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-                case 1: shade_kernel<1><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-                case 2: shade_kernel<2><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-                case 3: shade_kernel<3><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-                case 4: shade_kernel<4><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-                default: shade_kernel<5><<<L.shadeBlocks, 128, 0, s>>>(L.scene, L.wf, L.job); break;
-            }
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
         }
         if (L.nee && L.scene.lightCount > 0)
         {
-            WavefrontShadow ws{L.scene, L.wf};
+            WavefrontShadow ws{L.scene, L.wf, nullptr};
             e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
         regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         advance_kernel<<<1, 1, 0, s>>>(L.wf, L.job, L.handle, L.graphLoop);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_engine_init(const Wavefront& wf, const EngineView& ev, uint32_t pool, cudaStream_t s)
+    {
+        const uint32_t blocks = (pool + 255) / 256 < 4096 ? (pool + 255) / 256 : 4096;
+        engine_init_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(wf, ev, pool);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_engine_iteration(const EngineLaunch& L, cudaStream_t s)
+    {
+        cudaError_t e;
+        WavefrontClosest wc{L.scene, L.wf, L.ev.scenes};
+        e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+        if (e != cudaSuccess) return e;
+        for (uint32_t m = 0; m < kModelCount; m++)
+        {
+            if (!L.modelPresent[m]) continue;
+            if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.ev.jobs, L.ev.scenes, s)) != cudaSuccess) return e;
+        }
+        if (L.anyLights)
+        {
+            WavefrontShadow ws{L.scene, L.wf, L.ev.scenes};
+            e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            if (e != cudaSuccess) return e;
+        }
+        plan_kernel<<<1, 1, 0, s>>>(L.wf, L.ev);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        engine_regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        fold_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.ev);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        engine_advance_kernel<<<1, 1, 0, s>>>(L.wf, L.ev, L.handle, L.graphLoop);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_rebase_field(uint32_t* base, uint32_t n, uint32_t strideWords, uint32_t offset, bool skipInvalid, cudaStream_t s)
+    {
+        if (n == 0 || (offset == 0 && !skipInvalid)) return cudaSuccess;
+        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
+        rebase_field_kernel<<<blocks, 256, 0, s>>>(base, n, strideWords, offset, skipInvalid);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_rebase_nodes(Node8* nodes, uint32_t n, uint32_t nodeOffset, uint32_t triOffset, cudaStream_t s)
+    {
+        if (n == 0) return cudaSuccess;
+        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
+        rebase_nodes_kernel<<<blocks, 256, 0, s>>>(nodes, n, nodeOffset, triOffset);
         return cudaGetLastError();
     }
 
@@ -1447,10 +1807,10 @@ namespace pt
         return cudaGetLastError();
     }
 
-    cudaError_t launch_batch_trace(const SceneView& sc, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut, float* uvtOut,
-                                   uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s)
+    cudaError_t launch_batch_trace(const SceneView& sc, uint32_t root, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
+                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s)
     {
-        BatchRays b{sc, rays, n, cursor, triOut, uvtOut, occOut};
+        BatchRays b{sc, rays, n, cursor, triOut, uvtOut, occOut, root};
         if (occOut) return launch_trace<true>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
         return launch_trace<false>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
     }

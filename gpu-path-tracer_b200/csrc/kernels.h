@@ -11,6 +11,7 @@ namespace pt
         SceneView scene;
         Wavefront wf;
         const JobView* job;       // device pointer
+        const SceneEntry* scenes; // device pointer, one entry (lights of the scene)
         cudaGraphConditionalHandle handle;
         bool modelPresent[kModelCount];
         bool nee;
@@ -24,12 +25,33 @@ namespace pt
         cudaEvent_t traceStop;
     };
 
+    // One iteration of the job engine over all resident scenes and active jobs.
+    struct EngineLaunch
+    {
+        SceneView scene;           // packed arrays of all resident scenes
+        Wavefront wf;
+        EngineView ev;
+        cudaGraphConditionalHandle handle;
+        bool modelPresent[kModelCount];
+        bool anyLights;
+        int traceBlocks;
+        int traceThreads;
+        uint32_t refill;
+        int occupancy;
+        int shadeBlocks;
+        bool graphLoop;
+    };
+
     int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy);
+    cudaError_t launch_engine_init(const Wavefront& wf, const EngineView& ev, uint32_t pool, cudaStream_t stream);
+    cudaError_t launch_engine_iteration(const EngineLaunch& launch, cudaStream_t stream);
+    cudaError_t launch_rebase_field(uint32_t* base, uint32_t n, uint32_t strideWords, uint32_t offset, bool skipInvalid, cudaStream_t stream);
+    cudaError_t launch_rebase_nodes(Node8* nodes, uint32_t n, uint32_t nodeOffset, uint32_t triOffset, cudaStream_t stream);
     cudaError_t launch_iteration(const IterationLaunch& launch, cudaStream_t stream);
     cudaError_t launch_frame_prologue(const Wavefront& wf, const JobView* job, uint32_t pool, int blocks, cudaStream_t stream);
     cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t stream);
     cudaError_t launch_clear(uint32_t* framebuffer, uint32_t n, uint32_t value, cudaStream_t stream);
-    cudaError_t launch_batch_trace(const SceneView& scene, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
+    cudaError_t launch_batch_trace(const SceneView& scene, uint32_t root, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
                                    float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t stream);
     cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
                                        const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t stream);

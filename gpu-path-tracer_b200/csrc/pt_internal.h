@@ -6,8 +6,8 @@
 //   triangle shading 144 B  3 normals, 3 tangents, gN|material, uvs (Triangle.hpp:24-38 layout), input order
 //   light           112 B   v0|index, e1|area, e2, gN, emission, uv0|uvE1, uvE2|material
 //   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14)
-//   path slot         36 B  throughput|depth/flags, radiance|rng position, sample index
-//   ray queue entry   32 B  origin|slot, direction|tMax   (x2, ping-pong)
+//   path slot         36 B  throughput|depth/flags/job, radiance|rng position, sample index
+//   ray queue entry   32 B  origin|tag, direction|tMax   (x2, ping-pong; tag = slot | scene << 24)
 //   hit record        16 B  triangle, u, v, t             (aligned with the current ray queue)
 //   material queue     4 B  ray-queue index               (x6, one per shading model)
 //   shadow queue      48 B  origin|slot, direction|tMax, radiance
@@ -27,6 +27,14 @@ namespace pt
     constexpr uint32_t kRussianRouletteStartDepth = 3;
     constexpr uint32_t kQueueLogColumns = 9;
     constexpr uint32_t kMaxStack = 64;
+    // Ray and shadow-ray entries carry a tag: the path slot in the low 24 bits and the resident
+    // scene in the high 8. Path metadata: depth (8 bits) | delta flag (bit 8) | job << 16.
+    constexpr uint32_t kSlotBits = 24;
+    constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
+    constexpr uint32_t kMaxPool = 1u << kSlotBits;
+    constexpr uint32_t kMaxScenes = 256;
+    constexpr uint32_t kMaxJobs = 65536;
+    constexpr uint32_t kMaxRing = 256;
 
     // BVH8 node, 128 bytes = 8 x uint4, loaded as one L1 line.
     //  w[0] = px, py, pz (float bits), ex | ey<<8 | ez<<16 | innerMask<<24   (biased float exponents of the scales)
@@ -82,14 +90,74 @@ namespace pt
         uint32_t depth;           // BVH8 depth (stack entries needed)
     };
 
+    // Per resident scene: where its BVH8 starts in the packed node array and its slice of the
+    // packed light list / alias table (alias entries are stored rebased to the packed list).
+    struct __align__(16) SceneEntry
+    {
+        uint32_t root;
+        uint32_t lightOffset;
+        uint32_t lightCount;
+        uint32_t triangleOffset;
+    };
+
+    // One render job. The single-frame renderer uses one of these (job 0, sample-major output);
+    // the job engine keeps a table of them (pass-major launch order, pass ring + Kahan accumulator).
     struct JobView
     {
         float camera[12];         // origin, lowerLeftCorner, horizontal, vertical
         uint32_t width, height, spp, spa;
-        uint32_t depthLimit, nee, maxIterations, pad1;   // maxIterations: hard cap of the device loop
-        uint64_t totalSamples;
-        float* sampleRadiance;    // [totalSamples][3]
+        uint32_t depthLimit, nee, maxIterations, scene;   // maxIterations: hard cap of the device loop
+        uint64_t totalSamples;    // launch indices [0, totalSamples)
+        float* sampleRadiance;    // frame renderer: [totalSamples][3]; engine: ring [ring][pixels][3]
         uint64_t rngOffset;       // added to the sample index to form the Philox subsequence
+        // job engine only
+        uint32_t pixels, ring, state, folded;             // ring: pass buffers; folded: passes summed into accum
+        uint64_t launched;        // launch indices handed out so far
+        float4* accum;            // [pixels][2]: Kahan sum (xyz), compensation (xyz)
+        uint32_t* framebuffer;    // RGBA8, written when the last pass is folded
+        uint32_t* passDone;       // [ring] finished samples of the pass held by each ring buffer
+        uint64_t pad2;
+    };
+
+    enum JobState : uint32_t
+    {
+        kJobFree = 0,
+        kJobActive = 1,
+        kJobDone = 2,
+    };
+
+    // Launches of one planned iteration for one job: new samples [start, start + count) of the
+    // iteration take launch indices first, first + 1, ... of job `job`.
+    struct LaunchSegment
+    {
+        uint32_t job;
+        uint32_t start;
+        uint64_t first;
+    };
+
+    // Device-resident state of the job engine beyond the wavefront counters. The first four
+    // words belong to the device; the host writes the last four before every slice.
+    struct EngineCtl
+    {
+        uint32_t freeCount;       // idle path slots on the free list
+        uint32_t launchCount;     // new samples planned for this iteration
+        uint32_t segmentCount;
+        uint32_t stalled;         // set if an unfinished job can make no progress (logic error)
+        uint32_t orderCount;      // active jobs, oldest first
+        uint32_t sliceIterations;
+        uint32_t maxSliceIterations;
+        uint32_t completed;       // jobs finished during the current slice
+    };
+
+    struct EngineView
+    {
+        JobView* jobs;
+        const uint32_t* order;    // [orderCount] job-table indices, oldest first
+        LaunchSegment* segments;  // [capacity of the job table]
+        uint32_t* freeList;       // [pool]
+        EngineCtl* ctl;
+        const SceneEntry* scenes;
+        const volatile uint32_t* doorbell;  // host-mapped: nonzero ends the slice after the current iteration
     };
 
     // Device-resident frame control block. One thread (advance kernel) mutates it

@@ -23,81 +23,10 @@
 #include "../../include/gpt_b200.h"
 #include "bvh8.hpp"
 #include "kernels.h"
+#include "runtime.hpp"
 
 namespace pt
 {
-    struct Status
-    {
-        int code = GPT_OK;
-        std::string message;
-        static Status Ok() { return {}; }
-        static Status Err(int c, std::string m) { return Status{c, std::move(m)}; }
-        bool ok() const { return code == GPT_OK; }
-    };
-
-    static Status CudaStatus(const char* op, cudaError_t e)
-    {
-        if (e == cudaSuccess) return Status::Ok();
-        // Error text format of the reference (Cuda/Utils/Error.cpp:22-25).
-        std::string msg = std::string(op) + " failed: " + cudaGetErrorName(e) + ": " + cudaGetErrorString(e);
-        return Status::Err(e == cudaErrorMemoryAllocation ? GPT_ERR_OUT_OF_MEMORY : GPT_ERR_CUDA, msg);
-    }
-
-#define PT_TRY(expr)                      \
-    do                                    \
-    {                                     \
-        Status _s = (expr);               \
-        if (!_s.ok()) return _s;          \
-    } while (0)
-#define PT_CUDA(op, expr) PT_TRY(CudaStatus(op, (expr)))
-
-    // RAII device allocation (the reference's DeviceBuffer1D, Runtime/Memory/DeviceBuffer1D.cpp:33-80).
-    class DeviceBuffer
-    {
-    public:
-        DeviceBuffer() = default;
-        DeviceBuffer(const DeviceBuffer&) = delete;
-        DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-        ~DeviceBuffer() { reset(); }
-        Status allocate(size_t bytes)
-        {
-            if (bytes <= bytes_ && ptr_) return Status::Ok();
-            reset();
-            if (bytes == 0) return Status::Ok();
-            PT_CUDA("cudaMalloc", cudaMalloc(&ptr_, bytes));
-            bytes_ = bytes;
-            return Status::Ok();
-        }
-        void reset()
-        {
-            if (ptr_) cudaFree(ptr_);
-            ptr_ = nullptr;
-            bytes_ = 0;
-        }
-        template <typename T>
-        T* get() const { return static_cast<T*>(ptr_); }
-        size_t bytes() const { return bytes_; }
-
-    private:
-        void* ptr_ = nullptr;
-        size_t bytes_ = 0;
-    };
-
-    // An image texture with the reference's descriptors (Texture.cpp:65-189).
-    struct TextureObject
-    {
-        cudaArray_t array = nullptr;
-        cudaTextureObject_t object = 0;
-        TextureObject() = default;
-        TextureObject(const TextureObject&) = delete;
-        TextureObject& operator=(const TextureObject&) = delete;
-        ~TextureObject()
-        {
-            if (object) cudaDestroyTextureObject(object);
-            if (array) cudaFreeArray(array);
-        }
-    };
-
     static Status CreateTexture(const gpt_texture_desc& d, TextureObject& t)
     {
         if (d.width == 0 || d.height == 0 || !d.data || (d.channels != 1 && d.channels != 3 && d.channels != 4) || d.format > GPT_TEXEL_F32)
@@ -153,33 +82,6 @@ namespace pt
         return Status::Ok();
     }
 
-    struct SceneGpu
-    {
-        DeviceBuffer nodes, tris, shading, materials, lights, bins, materialTextures;
-        std::vector<std::unique_ptr<TextureObject>> textures;
-        uint32_t nodeCount = 0, triangleCount = 0, depth = 0, lightCount = 0;
-        bool modelPresent[kModelCount] = {};
-        uint64_t version = 0;
-        SceneView view() const
-        {
-            SceneView v{};
-            v.nodes = nodes.get<Node8>();
-            v.tris = tris.get<float4>();
-            v.shading = shading.get<float4>();
-            v.materials = materials.get<MaterialDev>();
-            v.textures = textures.empty() ? nullptr : materialTextures.get<MaterialTextures>();
-            v.lights = lights.get<float4>();
-            v.bins = bins.get<uint4>();
-            v.lightCount = lightCount;
-            v.nodeCount = nodeCount;
-            v.triangleCount = triangleCount;
-            v.depth = depth;
-            return v;
-        }
-    };
-
-    // Minimal PNG writer (zlib deflate) for SaveRenderedFrame (Renderer.cpp:649-675): RGBA8, rows
-    // flipped vertically like Import::FlipVertically.
     static bool WritePng(const std::string& path, const uint32_t* rgba, uint32_t w, uint32_t h)
     {
         std::vector<unsigned char> raw(static_cast<size_t>(h) * (1 + 4 * static_cast<size_t>(w)));
@@ -220,6 +122,128 @@ namespace pt
         chunk("IDAT", z.data(), static_cast<uint32_t>(zlen));
         chunk("IEND", nullptr, 0);
         return std::fclose(f) == 0;
+    }
+
+    // Scene upload of Renderer::InitializeSceneBuffers (Renderer.cpp:292-306): validation, image textures,
+    // BVH8 (host), shading records, light list and alias table (device).
+    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out)
+    {
+        if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
+            d.material_count == 0)
+            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Scene description is incomplete");
+        const uint32_t n = d.triangle_count;
+        std::vector<uint32_t> models(n);
+        bool present[kModelCount] = {};
+        for (uint32_t m = 0; m < d.material_count; m++)
+            if (d.materials[m].model >= kModelCount)
+                return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Material has an unknown shading model");
+        for (uint32_t t = 0; t < n; t++)
+        {
+            const uint32_t mat = d.material_ids[t];
+            if (mat >= d.material_count) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Triangle material index out of range");
+            models[t] = d.materials[mat].model;
+            present[models[t]] = true;
+        }
+        auto scene = std::make_unique<SceneGpu>();
+        std::copy(present, present + kModelCount, scene->modelPresent);
+        // image textures of the material slots
+        if (d.texture_count > 0 && d.material_textures)
+        {
+            if (!d.textures) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Texture table is missing");
+            std::vector<MaterialTextures> slots(d.material_count);
+            for (uint32_t i = 0; i < d.texture_count; i++)
+            {
+                scene->textures.push_back(std::make_unique<TextureObject>());
+                PT_TRY(CreateTexture(d.textures[i], *scene->textures.back()));
+            }
+            for (uint32_t m = 0; m < d.material_count; m++)
+            {
+                slots[m] = MaterialTextures{};
+                for (int k = 0; k < GPT_TEX_SLOTS; k++)
+                {
+                    const int32_t ti = d.material_textures[static_cast<size_t>(m) * GPT_TEX_SLOTS + k];
+                    if (ti < 0) continue;
+                    if (static_cast<uint32_t>(ti) >= d.texture_count)
+                        return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Material texture index out of range");
+                    const bool scalar = k == GPT_TEX_SHININESS;
+                    if ((d.textures[ti].channels == 1) != scalar)
+                        return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Shininess maps have one channel, other maps three or four");
+                    slots[m].tex[k] = scene->textures[ti]->object;
+                }
+            }
+            PT_TRY(scene->materialTextures.allocate(slots.size() * sizeof(MaterialTextures)));
+            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materialTextures.get<void>(), slots.data(), slots.size() * sizeof(MaterialTextures),
+                                                       cudaMemcpyHostToDevice, stream));
+        }
+        // BVH8 on the host (binned SAH, collapse, quantisation).
+        Bvh8 bvh;
+        try
+        {
+            bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+        }
+        catch (const std::exception& e)
+        {
+            return Status::Err(GPT_ERR_INVALID_ARGUMENT, std::string("BVH build failed: ") + e.what());
+        }
+        if (bvh.depth > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "BVH8 deeper than the traversal stack");
+        if (bvh.nodes.size() >= (1u << 24)) return Status::Err(GPT_ERR_CAPACITY, "BVH8 has more than 2^24 nodes");
+        scene->nodeCount = static_cast<uint32_t>(bvh.nodes.size());
+        scene->triangleCount = n;
+        scene->depth = bvh.depth;
+        scene->materialCount = d.material_count;
+        PT_TRY(scene->nodes.allocate(bvh.nodes.size() * sizeof(Node8)));
+        PT_TRY(scene->tris.allocate(bvh.tris.size() * sizeof(float4)));
+        PT_TRY(scene->shading.allocate(static_cast<size_t>(n) * 9 * sizeof(float4)));
+        PT_TRY(scene->materials.allocate(static_cast<size_t>(d.material_count) * sizeof(MaterialDev)));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes.get<void>(), bvh.nodes.data(), bvh.nodes.size() * sizeof(Node8), cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materials.get<void>(), d.materials, static_cast<size_t>(d.material_count) * sizeof(MaterialDev), cudaMemcpyHostToDevice, stream));
+        // Vertex attributes go up once; shading records, lights and the alias table are built on the device.
+        DeviceBuffer pos, nrm, tan, uv, mid;
+        PT_TRY(pos.allocate(static_cast<size_t>(n) * 9 * 4));
+        PT_TRY(nrm.allocate(static_cast<size_t>(n) * 9 * 4));
+        PT_TRY(tan.allocate(static_cast<size_t>(n) * 12 * 4));
+        PT_TRY(uv.allocate(static_cast<size_t>(n) * 6 * 4));
+        PT_TRY(mid.allocate(static_cast<size_t>(n) * 4));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(pos.get<void>(), d.positions, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(nrm.get<void>(), d.normals, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(tan.get<void>(), d.tangents, static_cast<size_t>(n) * 48, cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(uv.get<void>(), d.uvs, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(mid.get<void>(), d.material_ids, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice, stream));
+        PT_CUDA("shading records", launch_shading_records(pos.get<float>(), nrm.get<float>(), tan.get<float>(), uv.get<float>(), mid.get<uint32_t>(), n,
+                                                          scene->shading.get<float4>(), stream));
+        DeviceBuffer flags, index, scanScratch, lightCountDev;
+        PT_TRY(flags.allocate(static_cast<size_t>(n) * 4));
+        PT_TRY(index.allocate(static_cast<size_t>(n) * 4));
+        PT_TRY(scanScratch.allocate(scan_scratch_elements(n) * 8));
+        PT_TRY(lightCountDev.allocate(16));
+        PT_CUDA("light build", launch_light_build(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
+                                                  flags.get<uint32_t>(), index.get<uint32_t>(), scanScratch.get<uint32_t>(), lightCountDev.get<uint32_t>(), stream));
+        uint32_t lightCount = 0;
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&lightCount, lightCountDev.get<void>(), 4, cudaMemcpyDeviceToHost, stream));
+        PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+        scene->lightCount = lightCount;
+        if (lightCount > 0)
+        {
+            DeviceBuffer weights, prefix, stackIndex, stackValue;
+            PT_TRY(scene->lights.allocate(static_cast<size_t>(lightCount) * 7 * sizeof(float4)));
+            PT_TRY(scene->bins.allocate(static_cast<size_t>(lightCount) * sizeof(uint4)));
+            PT_TRY(weights.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_TRY(prefix.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_TRY(stackIndex.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_TRY(stackValue.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_CUDA("light records", launch_light_records(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
+                                                          flags.get<uint32_t>(), index.get<uint32_t>(), scene->lights.get<float4>(), weights.get<double>(), stream));
+            PT_CUDA("alias table", launch_alias_build(weights.get<double>(), lightCount, prefix.get<double>(), scanScratch.get<double>(),
+                                                      scene->bins.get<uint4>(), stackIndex.get<uint32_t>(), stackValue.get<float>(), stream));
+            PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+        }
+        const SceneEntry entry{0u, 0u, lightCount, 0u};
+        PT_TRY(scene->entry.allocate(sizeof(SceneEntry)));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->entry.get<void>(), &entry, sizeof(entry), cudaMemcpyHostToDevice, stream));
+        PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+        out = std::move(scene);
+        return Status::Ok();
     }
 
     class Renderer
@@ -332,119 +356,11 @@ namespace pt
         // ---------------------------------------------------------------- scene
         Status InitializeSceneBuffers(const gpt_scene_desc& d)  // Renderer.cpp:292-306
         {
-            if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
-                d.material_count == 0)
-                return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Scene description is incomplete");
             if (rendering_.load()) return Status::Err(GPT_ERR_STATE, "Cannot upload a scene while rendering");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
-            const uint32_t n = d.triangle_count;
-            std::vector<uint32_t> models(n);
-            bool present[kModelCount] = {};
-            for (uint32_t m = 0; m < d.material_count; m++)
-                if (d.materials[m].model >= kModelCount)
-                    return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Material has an unknown shading model");
-            for (uint32_t t = 0; t < n; t++)
-            {
-                const uint32_t mat = d.material_ids[t];
-                if (mat >= d.material_count) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Triangle material index out of range");
-                models[t] = d.materials[mat].model;
-                present[models[t]] = true;
-            }
+            std::unique_ptr<SceneGpu> scene;
+            PT_TRY(BuildScene(d, stream_, scene));
             releaseGraph();
-            auto scene = std::make_unique<SceneGpu>();
-            std::copy(present, present + kModelCount, scene->modelPresent);
-            // image textures of the material slots
-            if (d.texture_count > 0 && d.material_textures)
-            {
-                if (!d.textures) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Texture table is missing");
-                std::vector<MaterialTextures> slots(d.material_count);
-                for (uint32_t i = 0; i < d.texture_count; i++)
-                {
-                    scene->textures.push_back(std::make_unique<TextureObject>());
-                    PT_TRY(CreateTexture(d.textures[i], *scene->textures.back()));
-                }
-                for (uint32_t m = 0; m < d.material_count; m++)
-                {
-                    slots[m] = MaterialTextures{};
-                    for (int k = 0; k < GPT_TEX_SLOTS; k++)
-                    {
-                        const int32_t ti = d.material_textures[static_cast<size_t>(m) * GPT_TEX_SLOTS + k];
-                        if (ti < 0) continue;
-                        if (static_cast<uint32_t>(ti) >= d.texture_count)
-                            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Material texture index out of range");
-                        const bool scalar = k == GPT_TEX_SHININESS;
-                        if ((d.textures[ti].channels == 1) != scalar)
-                            return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Shininess maps have one channel, other maps three or four");
-                        slots[m].tex[k] = scene->textures[ti]->object;
-                    }
-                }
-                PT_TRY(scene->materialTextures.allocate(slots.size() * sizeof(MaterialTextures)));
-                PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materialTextures.get<void>(), slots.data(), slots.size() * sizeof(MaterialTextures),
-                                                           cudaMemcpyHostToDevice, stream_));
-            }
-            // BVH8 on the host (binned SAH, collapse, quantisation).
-            Bvh8 bvh;
-            try
-            {
-                bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
-            }
-            catch (const std::exception& e)
-            {
-                return Status::Err(GPT_ERR_INVALID_ARGUMENT, std::string("BVH build failed: ") + e.what());
-            }
-            if (bvh.depth > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "BVH8 deeper than the traversal stack");
-            if (bvh.nodes.size() >= (1u << 24)) return Status::Err(GPT_ERR_CAPACITY, "BVH8 has more than 2^24 nodes");
-            scene->nodeCount = static_cast<uint32_t>(bvh.nodes.size());
-            scene->triangleCount = n;
-            scene->depth = bvh.depth;
-            PT_TRY(scene->nodes.allocate(bvh.nodes.size() * sizeof(Node8)));
-            PT_TRY(scene->tris.allocate(bvh.tris.size() * sizeof(float4)));
-            PT_TRY(scene->shading.allocate(static_cast<size_t>(n) * 9 * sizeof(float4)));
-            PT_TRY(scene->materials.allocate(static_cast<size_t>(d.material_count) * sizeof(MaterialDev)));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes.get<void>(), bvh.nodes.data(), bvh.nodes.size() * sizeof(Node8), cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materials.get<void>(), d.materials, static_cast<size_t>(d.material_count) * sizeof(MaterialDev), cudaMemcpyHostToDevice, stream_));
-            // Vertex attributes go up once; shading records, lights and the alias table are built on the device.
-            DeviceBuffer pos, nrm, tan, uv, mid;
-            PT_TRY(pos.allocate(static_cast<size_t>(n) * 9 * 4));
-            PT_TRY(nrm.allocate(static_cast<size_t>(n) * 9 * 4));
-            PT_TRY(tan.allocate(static_cast<size_t>(n) * 12 * 4));
-            PT_TRY(uv.allocate(static_cast<size_t>(n) * 6 * 4));
-            PT_TRY(mid.allocate(static_cast<size_t>(n) * 4));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(pos.get<void>(), d.positions, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(nrm.get<void>(), d.normals, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(tan.get<void>(), d.tangents, static_cast<size_t>(n) * 48, cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(uv.get<void>(), d.uvs, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(mid.get<void>(), d.material_ids, static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice, stream_));
-            PT_CUDA("shading records", launch_shading_records(pos.get<float>(), nrm.get<float>(), tan.get<float>(), uv.get<float>(), mid.get<uint32_t>(), n,
-                                                              scene->shading.get<float4>(), stream_));
-            DeviceBuffer flags, index, scanScratch, lightCountDev;
-            PT_TRY(flags.allocate(static_cast<size_t>(n) * 4));
-            PT_TRY(index.allocate(static_cast<size_t>(n) * 4));
-            PT_TRY(scanScratch.allocate(scan_scratch_elements(n) * 8));
-            PT_TRY(lightCountDev.allocate(16));
-            PT_CUDA("light build", launch_light_build(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
-                                                      flags.get<uint32_t>(), index.get<uint32_t>(), scanScratch.get<uint32_t>(), lightCountDev.get<uint32_t>(), stream_));
-            uint32_t lightCount = 0;
-            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&lightCount, lightCountDev.get<void>(), 4, cudaMemcpyDeviceToHost, stream_));
-            PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
-            scene->lightCount = lightCount;
-            if (lightCount > 0)
-            {
-                DeviceBuffer weights, prefix, stackIndex, stackValue;
-                PT_TRY(scene->lights.allocate(static_cast<size_t>(lightCount) * 7 * sizeof(float4)));
-                PT_TRY(scene->bins.allocate(static_cast<size_t>(lightCount) * sizeof(uint4)));
-                PT_TRY(weights.allocate(static_cast<size_t>(lightCount) * 8));
-                PT_TRY(prefix.allocate(static_cast<size_t>(lightCount) * 8));
-                PT_TRY(stackIndex.allocate(static_cast<size_t>(lightCount) * 8));
-                PT_TRY(stackValue.allocate(static_cast<size_t>(lightCount) * 8));
-                PT_CUDA("light records", launch_light_records(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
-                                                              flags.get<uint32_t>(), index.get<uint32_t>(), scene->lights.get<float4>(), weights.get<double>(), stream_));
-                PT_CUDA("alias table", launch_alias_build(weights.get<double>(), lightCount, prefix.get<double>(), scanScratch.get<double>(),
-                                                          scene->bins.get<uint4>(), stackIndex.get<uint32_t>(), stackValue.get<float>(), stream_));
-                PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
-            }
-            PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
             scene->version = ++sceneVersion_;
             scene_ = std::move(scene);
             return Status::Ok();
@@ -470,7 +386,7 @@ namespace pt
             c.spp = c.spa * c.spa;
             c.depth = std::min(std::max(s.path_depth, 1u), 100u);
             c.nee = s.use_nee ? 1u : 0u;
-            c.pool = s.pool_size ? s.pool_size : kDefaultPool;
+            c.pool = s.pool_size ? std::min(s.pool_size, kMaxPool) : kDefaultPool;
             c.totalSamples = static_cast<uint64_t>(c.spp) * c.width * c.height;
             if (s.max_samples && s.max_samples < c.totalSamples) c.totalSamples = s.max_samples;
             if (c.totalSamples >= 0xFFFFFFFFull)
@@ -527,6 +443,7 @@ namespace pt
             L.scene = sv;
             L.wf = wf;
             L.job = jobDev;
+            L.scenes = scene_->entry.get<SceneEntry>();
             L.handle = handle;
             for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = scene_->modelPresent[m];
             L.nee = c.nee != 0;
@@ -566,6 +483,7 @@ namespace pt
             L.scene = sv;
             L.wf = wf;
             L.job = jobDev;
+            L.scenes = scene_->entry.get<SceneEntry>();
             L.handle = 0;
             for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = scene_->modelPresent[m];
             L.nee = c.nee != 0;
@@ -766,7 +684,7 @@ namespace pt
             PT_CUDA("cudaMemsetAsync", cudaMemsetAsync(cursor, 0, 8, st));
             const SceneView sv = scene_->view();
             const int blocks = trace_grid_blocks(device_, 128, sv.depth, 1);
-            PT_CUDA("intersect", launch_batch_trace(sv, rays, n, cursor, tri, uvt, occ, blocks, 128, cursor + 1, st));
+            PT_CUDA("intersect", launch_batch_trace(sv, 0u, rays, n, cursor, tri, uvt, occ, blocks, 128, cursor + 1, st));
             uint32_t err = 0;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&err, cursor + 1, 4, cudaMemcpyDeviceToHost, st));
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(st));
@@ -1203,9 +1121,10 @@ extern "C"
     int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count)
     {
         if (!sizes) return GPT_ERR_INVALID_ARGUMENT;
-        const uint32_t all[7] = {sizeof(gpt_material), sizeof(gpt_scene_desc), sizeof(gpt_device_camera), sizeof(gpt_motion_state),
-                                 sizeof(gpt_render_settings), sizeof(gpt_frame_stats), sizeof(gpt_texture_desc)};
-        for (uint32_t i = 0; i < count && i < 7; i++) sizes[i] = all[i];
+        const uint32_t all[11] = {sizeof(gpt_material), sizeof(gpt_scene_desc), sizeof(gpt_device_camera), sizeof(gpt_motion_state),
+                                  sizeof(gpt_render_settings), sizeof(gpt_frame_stats), sizeof(gpt_texture_desc), sizeof(gpt_server_config),
+                                  sizeof(gpt_job_desc), sizeof(gpt_job_status), sizeof(gpt_server_stats)};
+        for (uint32_t i = 0; i < count && i < 11; i++) sizes[i] = all[i];
         return GPT_OK;
     }
 

@@ -75,6 +75,38 @@ class gpt_frame_stats(ctypes.Structure):
 PHASES = ("trace", "shade", "shadow", "regen")
 
 
+class gpt_server_config(ctypes.Structure):
+    _fields_ = [("pool_size", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_active_jobs", ctypes.c_uint32),
+                ("ring_passes", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_uint64), ("trace_block", ctypes.c_uint32),
+                ("trace_refill", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
+                ("max_slice_iterations", ctypes.c_uint32)]
+
+
+class gpt_job_desc(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
+                ("samples_per_pixel", ctypes.c_uint32), ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32),
+                ("rng_offset", ctypes.c_uint64), ("camera", gpt_device_camera), ("keep_accumulation", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+class gpt_job_status(ctypes.Structure):
+    _fields_ = [("state", ctypes.c_uint32), ("passes_done", ctypes.c_uint32), ("passes_total", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("samples_total", ctypes.c_uint64), ("admitted_bytes", ctypes.c_uint64),
+                ("submit_s", ctypes.c_double), ("admit_s", ctypes.c_double), ("done_s", ctypes.c_double)]
+
+
+class gpt_server_stats(ctypes.Structure):
+    _fields_ = [("slices", ctypes.c_uint64), ("iterations", ctypes.c_uint64), ("samples", ctypes.c_uint64),
+                ("rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64), ("admitted_bytes", ctypes.c_uint64),
+                ("admitted_high_water", ctypes.c_uint64), ("budget_bytes", ctypes.c_uint64),
+                ("active_jobs", ctypes.c_uint32), ("queued_jobs", ctypes.c_uint32), ("completed_jobs", ctypes.c_uint32),
+                ("scenes", ctypes.c_uint32), ("device_ms", ctypes.c_double), ("phase_ms", ctypes.c_float * 4)]
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_CANCELLED, JOB_FAILED = 0, 1, 2, 3, 4
+JOB_STATES = ("queued", "running", "done", "cancelled", "failed")
+
+
 # (name, restype, argtypes) of every C entry point in include/gpt_b200.h
 _SIGNATURES = [
     ("gpt_status_string", ctypes.c_char_p, [ctypes.c_int]),
@@ -128,6 +160,17 @@ _SIGNATURES = [
     ("gpt_abi_struct_sizes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32]),
     ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
                                               ctypes.POINTER(gpt_device_camera)]),
+    ("gpt_server_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(gpt_server_config)]),
+    ("gpt_server_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("gpt_server_add_scene", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32)]),
+    ("gpt_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_job_desc), ctypes.POINTER(ctypes.c_uint64)]),
+    ("gpt_server_poll", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(gpt_job_status)]),
+    ("gpt_server_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double]),
+    ("gpt_server_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpt_server_release", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("gpt_server_cancel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("gpt_server_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_server_stats)]),
+    ("gpt_server_peek_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
 ]
 
 
@@ -380,10 +423,11 @@ def scene_desc(scene) -> gpt_scene_desc:
 
 def abi_struct_sizes() -> dict:
     """sizeof() of the public structs as compiled into the library."""
-    out = (ctypes.c_uint32 * 8)()
-    lib().gpt_abi_struct_sizes(out, 8)
     names = ["gpt_material", "gpt_scene_desc", "gpt_device_camera", "gpt_motion_state", "gpt_render_settings",
-             "gpt_frame_stats", "gpt_texture_desc"]
+             "gpt_frame_stats", "gpt_texture_desc", "gpt_server_config", "gpt_job_desc", "gpt_job_status",
+             "gpt_server_stats"]
+    out = (ctypes.c_uint32 * len(names))()
+    lib().gpt_abi_struct_sizes(out, len(names))
     return {n: out[i] for i, n in enumerate(names)}
 
 
@@ -452,3 +496,90 @@ def make_device_camera(fov_y: float, aspect: float, position, quat_wxyz) -> np.n
     if rc != 0:
         raise GptError(rc, "gpt_make_device_camera")
     return np.array(list(cam.origin) + list(cam.lower_left) + list(cam.horizontal) + list(cam.vertical), dtype=np.float32)
+
+
+class Server:
+    """Handle on one gpt_server: resident scenes, submitted jobs rendered together on one device."""
+
+    def __init__(self, device: int = 0, pool_size: int = 0, max_jobs: int = 0, max_active_jobs: int = 0,
+                 ring_passes: int = 0, hbm_budget_bytes: int = 0, trace_block: int = 0, trace_refill: int = 0,
+                 trace_occupancy: int = 0, max_slice_iterations: int = 0):
+        self.L = lib()
+        cfg = gpt_server_config(pool_size, max_jobs, max_active_jobs, ring_passes, hbm_budget_bytes, trace_block,
+                                trace_refill, trace_occupancy, max_slice_iterations)
+        h = ctypes.c_void_p()
+        rc = self.L.gpt_server_create(ctypes.byref(h), device, ctypes.byref(cfg))
+        if rc != 0:
+            raise GptError(rc, f"gpt_server_create(device={device}) failed: {self.L.gpt_status_string(rc).decode()}")
+        self.h = h
+        self._jobs = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.gpt_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(1024)
+            self.L.gpt_server_peek_last_error(self.h, buf, 1024)
+            raise GptError(rc, f"{what}: {buf.value.decode() or self.L.gpt_status_string(rc).decode()}")
+
+    def add_scene(self, scene) -> int:
+        desc, keep = scene_desc_with_textures(scene)
+        sid = ctypes.c_uint32()
+        self._check(self.L.gpt_server_add_scene(self.h, ctypes.byref(desc), ctypes.byref(sid)), "gpt_server_add_scene")
+        del keep
+        return sid.value
+
+    def submit(self, scene_id: int, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
+               rng_offset: int = 0, keep_accumulation: bool = False) -> int:
+        d = gpt_job_desc(scene_id, width, height, spp, depth, 1 if nee else 0, rng_offset, camera_struct(camera12),
+                         1 if keep_accumulation else 0, 0)
+        jid = ctypes.c_uint64()
+        self._check(self.L.gpt_server_submit(self.h, ctypes.byref(d), ctypes.byref(jid)), "gpt_server_submit")
+        self._jobs[jid.value] = (width, height)
+        return jid.value
+
+    def poll(self, job: int) -> dict:
+        st = gpt_job_status()
+        self._check(self.L.gpt_server_poll(self.h, job, ctypes.byref(st)), "gpt_server_poll")
+        return dict(state=JOB_STATES[st.state], passes_done=st.passes_done, passes_total=st.passes_total,
+                    samples_total=st.samples_total, admitted_bytes=st.admitted_bytes, submit_s=st.submit_s,
+                    admit_s=st.admit_s, done_s=st.done_s)
+
+    def wait(self, job: int, timeout_s: float = 600.0):
+        self._check(self.L.gpt_server_wait(self.h, job, timeout_s), "gpt_server_wait")
+        return self.poll(job)
+
+    def result(self, job: int, accumulation: bool = False):
+        """(framebuffer [h*w] uint32, accumulation [h*w, 4] float32 or None)."""
+        w, h = self._jobs[job]
+        fb = np.zeros(w * h, dtype=np.uint32)
+        acc = np.zeros((w * h, 4), dtype=np.float32) if accumulation else None
+        self._check(self.L.gpt_server_read(self.h, job, _ptr(fb), _ptr(acc) if acc is not None else None), "gpt_server_read")
+        return fb, acc
+
+    def release(self, job: int):
+        self._check(self.L.gpt_server_release(self.h, job), "gpt_server_release")
+        self._jobs.pop(job, None)
+
+    def cancel(self, job: int):
+        self._check(self.L.gpt_server_cancel(self.h, job), "gpt_server_cancel")
+
+    def stats(self) -> dict:
+        st = gpt_server_stats()
+        self._check(self.L.gpt_server_get_stats(self.h, ctypes.byref(st)), "gpt_server_get_stats")
+        out = {name: getattr(st, name) for name, _ in gpt_server_stats._fields_ if name != "phase_ms"}
+        out["phase_ms"] = dict(zip(PHASES, list(st.phase_ms)))
+        return out
+
+    def last_error(self) -> str | None:
+        buf = ctypes.create_string_buffer(1024)
+        return buf.value.decode() if self.L.gpt_server_peek_last_error(self.h, buf, 1024) else None

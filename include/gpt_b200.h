@@ -284,9 +284,95 @@ int gpt_obj_scene_desc(const gpt_obj_scene* scene, gpt_scene_desc* desc);
 int gpt_obj_material_name(const gpt_obj_scene* scene, uint32_t index, char* buffer, size_t length);
 void gpt_obj_free(gpt_obj_scene* scene);
 
+/*
+ * Job server: continuous batching of render jobs over device-resident scenes. The reference renders
+ * one job at a time through Renderer (RenderFrame per camera, Renderer.cpp:401-647); the server keeps
+ * several scenes resident (gpt_server_add_scene), admits submitted jobs while others run, as long as
+ * a job-table entry and the HBM budget allow, and traces the paths of all admitted jobs together in
+ * one device loop (one CUDA graph per scheduling slice). Every job renders progressively in passes of
+ * one sample per pixel; its image equals the one gpt_render_frame produces for the same scene,
+ * camera and settings, bit for bit, alone or mixed with other jobs.
+ *
+ * Admission accounting per job: 64 bytes per path the job may have in flight (min(ring passes x
+ * pixels, pool)) plus its framebuffers (pass ring 12 B, Kahan accumulator 32 B, RGBA8 4 B per
+ * pixel and pass). Jobs are admitted in submission order; a job larger than the whole budget is
+ * refused at submission with GPT_ERR_CAPACITY. All gpt_server_* calls are thread-safe.
+ */
+typedef struct gpt_server gpt_server;
+
+typedef struct gpt_server_config {
+    uint32_t pool_size;            /* path slots shared by all jobs, <= 2^24 (0 = 4,194,304) */
+    uint32_t max_jobs;             /* job-table entries: jobs admitted at the same time (0 = 256) */
+    uint32_t max_active_jobs;      /* 0 = as many as fit; 1 = one job at a time (the plain loop) */
+    uint32_t ring_passes;          /* pass buffers per job, <= 256 (0 = chosen from pool and image size) */
+    uint64_t hbm_budget_bytes;     /* admission budget (0 = 16 GiB); also the size of the job arena */
+    uint32_t trace_block;          /* traversal tuning, as in gpt_render_settings (0 = defaults) */
+    uint32_t trace_refill;
+    uint32_t trace_occupancy;
+    uint32_t max_slice_iterations; /* wavefront iterations per graph launch at most (0 = 4096) */
+} gpt_server_config;
+
+typedef struct gpt_job_desc {
+    uint32_t scene;                /* id from gpt_server_add_scene */
+    uint32_t width, height;
+    uint32_t samples_per_pixel;    /* rounded down to a square, as StartSimulation does */
+    uint32_t path_depth;
+    uint32_t use_nee;
+    uint64_t rng_offset;           /* added to the sample index to form the Philox subsequence */
+    gpt_device_camera camera;
+    uint32_t keep_accumulation;    /* nonzero: keep the float4 accumulation for gpt_server_read */
+    uint32_t reserved;
+} gpt_job_desc;
+
+#define GPT_JOB_QUEUED 0
+#define GPT_JOB_RUNNING 1
+#define GPT_JOB_DONE 2
+#define GPT_JOB_CANCELLED 3
+#define GPT_JOB_FAILED 4
+
+typedef struct gpt_job_status {
+    uint32_t state;                /* GPT_JOB_* */
+    uint32_t passes_done;          /* samples per pixel folded into the image so far */
+    uint32_t passes_total;
+    uint32_t reserved;
+    uint64_t samples_total;
+    uint64_t admitted_bytes;
+    double submit_s, admit_s, done_s; /* seconds since gpt_server_create; -1 = not yet */
+} gpt_job_status;
+
+typedef struct gpt_server_stats {
+    uint64_t slices;               /* graph launches */
+    uint64_t iterations;           /* wavefront iterations */
+    uint64_t samples;              /* samples (paths) launched */
+    uint64_t rays, shadow_rays;
+    uint64_t admitted_bytes, admitted_high_water, budget_bytes;
+    uint32_t active_jobs, queued_jobs, completed_jobs, scenes;
+    double device_ms;              /* sum of the slices' device times */
+    float phase_ms[4];             /* as gpt_frame_stats.phase_ms, summed over all slices */
+} gpt_server_stats;
+
+int gpt_server_create(gpt_server** out, int device, const gpt_server_config* config);
+int gpt_server_destroy(gpt_server* server);
+/* Only while no job is queued or running. */
+int gpt_server_add_scene(gpt_server* server, const gpt_scene_desc* scene, uint32_t* scene_id);
+int gpt_server_submit(gpt_server* server, const gpt_job_desc* job, uint64_t* job_id);
+int gpt_server_poll(gpt_server* server, uint64_t job_id, gpt_job_status* status);
+/* GPT_OK once the job is done, cancelled or failed; GPT_ERR_TIMEOUT after timeout_s seconds. */
+int gpt_server_wait(gpt_server* server, uint64_t job_id, double timeout_s);
+/* After GPT_JOB_DONE: rgba [height][width] uint32; accumulation [height][width][4] float or NULL. */
+int gpt_server_read(gpt_server* server, uint64_t job_id, uint32_t* rgba, float* accumulation);
+/* Forgets a finished job (its host copy of the image). */
+int gpt_server_release(gpt_server* server, uint64_t job_id);
+/* A queued job is dropped; a running one launches no more samples and ends as GPT_JOB_CANCELLED
+ * (without an image) once its paths in flight finish. */
+int gpt_server_cancel(gpt_server* server, uint64_t job_id);
+int gpt_server_get_stats(gpt_server* server, gpt_server_stats* stats);
+int gpt_server_peek_last_error(gpt_server* server, char* buffer, size_t length);
+
 /* sizeof() of the public structs as compiled into this library, in the order gpt_material,
  * gpt_scene_desc, gpt_device_camera, gpt_motion_state, gpt_render_settings, gpt_frame_stats,
- * gpt_texture_desc (for binding checks from other languages). */
+ * gpt_texture_desc, gpt_server_config, gpt_job_desc, gpt_job_status, gpt_server_stats (for
+ * binding checks from other languages). */
 int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count);
 
 /* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */

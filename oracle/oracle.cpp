@@ -1209,7 +1209,9 @@ namespace oracle
         if (s.maxSamples != 0 && s.maxSamples < totalSamples)
             totalSamples = s.maxSamples;
         const uint32_t generateCount = static_cast<uint32_t>(std::min<uint64_t>(totalSamples, s.poolSize));
-        const bool nee = s.nee != 0;
+        // The reference's light sampler reads bin 0 of an empty table when NEE meets a scene without
+        // emitters (AliasTableView.hpp:32-60); here NEE is off for such scenes (nothing to connect to).
+        const bool nee = s.nee != 0 && !scene.lights.empty();
 
         std::vector<PathState> active(generateCount);
         ParallelFor(generateCount, s.threads, [&](size_t b, size_t e)

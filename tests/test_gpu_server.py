@@ -1,0 +1,184 @@
+"""Job server (gpt_server_*): jobs rendered together over resident scenes must give, bit for bit,
+the images the frame renderer (gpt_render_frame) gives for the same scene, camera and settings,
+whether a job runs alone, mixed with others, one at a time, or through a tiny path pool."""
+import numpy as np
+import pytest
+
+import pathtracer
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+BUDGET = 2 << 30
+
+
+def no_light_scene():
+    s = scenes.cornell_all_models(1)
+    mats = s.materials.copy()
+    for m in range(len(mats)):
+        if mats[m]["model"] == 5:
+            mats[m]["model"] = 1
+    return scenes.Scene(s.positions, s.normals, s.tangents, s.uvs, s.material_ids, mats, name="cornell-dark",
+                        camera=s.camera)
+
+
+@pytest.fixture(scope="module")
+def resident(scene_factory):
+    names = ["cornell-all", "cornell-textured", "spheres-small"]
+    return {n: scene_factory(n) for n in names} | {"cornell-dark": no_light_scene()}
+
+
+@pytest.fixture(scope="module")
+def frame_renderers(resident):
+    out = {}
+    for name, s in resident.items():
+        r = pathtracer.Renderer(0)
+        r.upload_scene(s)
+        out[name] = r
+    yield out
+    for r in out.values():
+        r.close()
+
+
+def frame_reference(renderers, name, scene, w, h, spp, depth, nee, rng_offset=0):
+    r = renderers[name]
+    cam = scenes.scene_camera(scene, w, h)
+    r.render_frame(cam, w, h, spp, depth, nee, rng_offset=rng_offset)
+    return r.framebuffer().reshape(-1), r.accumulation().reshape(-1, 4)
+
+
+def make_server(resident, **kw):
+    srv = pathtracer.Server(0, hbm_budget_bytes=kw.pop("hbm_budget_bytes", BUDGET), **kw)
+    ids = {name: srv.add_scene(s) for name, s in resident.items()}
+    return srv, ids
+
+
+JOBS = [
+    # scene, width, height, spp, depth, nee, rng offset
+    ("cornell-all", 40, 30, 4, 6, True, 0),
+    ("cornell-all", 33, 17, 16, 8, False, 0),
+    ("cornell-textured", 48, 48, 4, 5, True, 0),
+    ("cornell-textured", 20, 36, 9, 7, False, 77),
+    ("spheres-small", 64, 40, 4, 12, True, 0),
+    ("spheres-small", 31, 29, 1, 10, True, 5),
+    ("cornell-dark", 24, 24, 4, 6, True, 0),
+    ("cornell-all", 96, 64, 2, 8, True, 1000),
+]
+
+
+def check_job(srv, jid, renderers, resident, job):
+    name, w, h, spp, depth, nee, off = job
+    st = srv.wait(jid, 300)
+    assert st["state"] == "done", (job, st, srv.last_error())
+    fb, acc = srv.result(jid, accumulation=True)
+    ref_fb, ref_acc = frame_reference(renderers, name, resident[name], w, h, spp, depth, nee, off)
+    assert np.array_equal(acc.view(np.uint32), ref_acc.view(np.uint32)), job
+    assert np.array_equal(fb, ref_fb), job
+
+
+def submit(srv, ids, resident, job):
+    name, w, h, spp, depth, nee, off = job
+    cam = scenes.scene_camera(resident[name], w, h)
+    return srv.submit(ids[name], cam, w, h, spp, depth, nee, rng_offset=off, keep_accumulation=True)
+
+
+def test_single_jobs_match_frame_renderer(resident, frame_renderers):
+    srv, ids = make_server(resident, pool_size=1 << 16)
+    try:
+        for job in JOBS:
+            check_job(srv, submit(srv, ids, resident, job), frame_renderers, resident, job)
+    finally:
+        srv.close()
+
+
+def test_mixed_jobs_match_alone(resident, frame_renderers):
+    srv, ids = make_server(resident, pool_size=1 << 18)
+    try:
+        jids = [submit(srv, ids, resident, job) for job in JOBS]
+        for jid, job in zip(jids, JOBS):
+            check_job(srv, jid, frame_renderers, resident, job)
+        st = srv.stats()
+        assert st["completed_jobs"] == len(JOBS)
+        expected = sum(w * h * int(np.sqrt(spp)) ** 2 for _, w, h, spp, _, _, _ in JOBS)
+        assert st["samples"] == expected
+        assert st["admitted_bytes"] == 0
+        assert 0 < st["admitted_high_water"] <= BUDGET
+    finally:
+        srv.close()
+
+
+def test_tiny_pool_and_single_pass_ring(resident, frame_renderers):
+    # 512 slots and one pass buffer per job: jobs wait on each other's slots and on their own folds
+    srv, ids = make_server(resident, pool_size=512, ring_passes=1)
+    try:
+        jobs = JOBS[:4]
+        jids = [submit(srv, ids, resident, job) for job in jobs]
+        for jid, job in zip(jids, jobs):
+            check_job(srv, jid, frame_renderers, resident, job)
+    finally:
+        srv.close()
+
+
+def test_one_job_at_a_time(resident, frame_renderers):
+    srv, ids = make_server(resident, pool_size=1 << 16, max_active_jobs=1)
+    try:
+        jobs = JOBS[:3]
+        jids = [submit(srv, ids, resident, job) for job in jobs]
+        for jid, job in zip(jids, jobs):
+            check_job(srv, jid, frame_renderers, resident, job)
+        admits = [srv.poll(j)["admit_s"] for j in jids]
+        dones = [srv.poll(j)["done_s"] for j in jids]
+        # each job is admitted only after the previous one finished
+        assert admits[1] >= dones[0] and admits[2] >= dones[1]
+    finally:
+        srv.close()
+
+
+def test_budget_admission_and_refusal(resident, frame_renderers):
+    name, w, h = "cornell-all", 64, 64
+    # a budget for one such job at a time (about 0.5 MB: 64 B x 4096 in-flight paths + framebuffers)
+    budget = 600_000
+    srv, ids = make_server(resident, pool_size=1 << 12, hbm_budget_bytes=budget)
+    try:
+        with pytest.raises(pathtracer.GptError) as e:
+            srv.submit(ids[name], scenes.scene_camera(resident[name], 512, 512), 512, 512, 4, 4, True)
+        assert e.value.code == 6
+        job = (name, w, h, 4, 6, True, 0)
+        jids = [submit(srv, ids, resident, job) for _ in range(3)]
+        for jid in jids:
+            check_job(srv, jid, frame_renderers, resident, job)
+        st = srv.stats()
+        assert st["admitted_high_water"] <= budget
+        assert st["admitted_high_water"] == srv.poll(jids[0])["admitted_bytes"]
+    finally:
+        srv.close()
+
+
+def test_cancel_running_and_queued(resident, frame_renderers):
+    srv, ids = make_server(resident, pool_size=1 << 12, max_active_jobs=1)
+    try:
+        big = ("spheres-small", 256, 256, 64, 12, True, 0)
+        small = ("cornell-all", 40, 30, 4, 6, True, 0)
+        j_big = submit(srv, ids, resident, big)
+        j_queued = submit(srv, ids, resident, small)
+        srv.cancel(j_queued)
+        srv.cancel(j_big)
+        st = srv.wait(j_big, 300)
+        assert st["state"] == "cancelled"
+        assert srv.poll(j_queued)["state"] == "cancelled"
+        # the server keeps working after cancellations
+        j_ok = submit(srv, ids, resident, small)
+        check_job(srv, j_ok, frame_renderers, resident, small)
+    finally:
+        srv.close()
+
+
+def test_nee_without_emitters_matches_oracle(resident, frame_renderers):
+    import oracle
+    s = resident["cornell-dark"]
+    cam = scenes.scene_camera(s, 24, 24)
+    o = oracle.OracleScene(s).render(cam, 24, 24, 4, 6, True)
+    r = frame_renderers["cornell-dark"]
+    r.render_frame(cam, 24, 24, 4, 6, True)
+    assert np.array_equal(r.sample_radiance().view(np.uint32), o["sample_radiance"].view(np.uint32))
+    assert np.array_equal(r.framebuffer().reshape(-1), o["framebuffer"])
