@@ -13,6 +13,19 @@ Arms:
 Multi-GPU (torchrun, one process per GPU): every rank renders its own frame of the same
 workload on distinct Philox subsequences (weak scaling); the per-pixel accumulation buffers
 are summed across ranks with an NCCL all-reduce after each frame (the combined image).
+
+On one GPU the line also carries (--sections, default all):
+  plain      the plain single-job FP32 form on the same frame: binary FP32 BVH, warps refilled only
+             when all lanes are idle, host-driven iteration loop, 1,048,576 path slots, no autotuning
+  cornell    the Cornell box at 512x512, 16 spp, depth 8, NEE
+  batched    64 uneven jobs over 4 resident scenes (10k-2M triangles) through the job server in one
+             device loop, against the same jobs one at a time (server, frame renderer, plain form)
+  serving    open-loop Poisson arrivals (20, 50, 100 jobs/s) over 8 resident scenes (50k-4M
+             triangles): p50/p99 latency, paths/s and admitted-bytes high-water mark, served
+             (continuous batching) against one job at a time
+  precision  8M-triangle scene at 3840x2160, 16 spp, depth 10: BVH8 with 8-bit quantised boxes
+             against the binary FP32 BVH (node bytes per ray, traversal Mrays/s), and the FP32 Kahan
+             accumulation against FP64 accumulation of the same per-sample radiance (RMSE)
 """
 import argparse
 import json
@@ -52,7 +65,29 @@ def parse():
                     help="frame loop: one CUDA graph per frame (default) or host-launched iterations (for ncu)")
     ap.add_argument("--profile-case", action="store_true",
                     help="small frame (640x360, 16 spp) of the same scene for ncu captures; not a bench line")
+    ap.add_argument("--trace-occupancy", type=int, default=0, help="with --no-autotune: traversal variant (1, 10, 12)")
+    ap.add_argument("--trace-refill", type=int, default=0, help="with --no-autotune: idle lanes before a warp refills")
+    ap.add_argument("--trace-block", type=int, default=0, help="with --no-autotune: traversal threads per block")
+    ap.add_argument("--sections", default="all",
+                    help="comma list of extra one-GPU sections: plain,cornell,batched,serving,precision (all/none)")
+    ap.add_argument("--serve-jobs", type=int, default=48, help="jobs per arrival rate in the serving section")
+    ap.add_argument("--serve-rates", default="20,50,100", help="Poisson arrival rates (jobs/s) of the serving section")
     return ap.parse_args()
+
+
+SECTIONS = ("plain", "cornell", "batched", "serving", "precision")
+
+
+def wanted_sections(args):
+    if args.sections == "all":
+        return set(SECTIONS)
+    if args.sections in ("", "none"):
+        return set()
+    out = {x.strip() for x in args.sections.split(",") if x.strip()}
+    unknown = out - set(SECTIONS)
+    if unknown:
+        raise SystemExit(f"unknown sections: {sorted(unknown)}")
+    return out
 
 
 def measured_peaks():
@@ -183,6 +218,238 @@ def reference_arm(args):
     return 0
 
 
+def traversal_summary(st, node_bytes):
+    """Per-ray traversal work and rates of one frame's statistics."""
+    rays, shadow = st["rays"], st["shadow_rays"]
+    out = {"rays": rays, "shadow_rays": shadow, "node_bytes": node_bytes}
+    for k, name, n, phase in ((0, "closest", rays, "trace"), (1, "shadow", shadow, "shadow")):
+        if n == 0:
+            continue
+        visits, tests = st["node_visits"][k] / n, st["triangle_tests"][k] / n
+        out[name] = {"node_visits_per_ray": visits, "triangle_tests_per_ray": tests,
+                     "node_bytes_per_ray": visits * node_bytes, "bvh_bytes_per_ray": visits * node_bytes + tests * TRIANGLE_BYTES,
+                     "traversal_mrays_per_second": n / (st["phase_ms"][phase] / 1000.0) / 1e6 if st["phase_ms"][phase] > 0 else None}
+    return out
+
+
+def plain_form(renderer, cam, W, H, spp, depth, frames=2):
+    """The plain single-job FP32 wavefront form of a frame: binary FP32 BVH (64-B nodes, local-memory
+    stack), warps refilled only when all 32 lanes are idle, host-driven iteration loop with a flag
+    read per iteration, 1,048,576 path slots (the reference's pool), no autotuning. Same images bit
+    for bit as the optimised form."""
+    import pathtracer
+    settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
+                    loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32)
+    renderer.render_frame(cam, W, H, spp, depth, True, **settings)
+    stats = [renderer.render_frame(cam, W, H, spp, depth, True, **settings) for _ in range(frames)]
+    ms = sum(s["device_ms"] for s in stats) / frames
+    return {"value": stats[0]["samples"] / (ms / 1000.0), "unit": "paths/s", "ms_per_frame": ms,
+            "iterations": stats[0]["iterations"], "settings": {k: v for k, v in settings.items()},
+            "traversal": traversal_summary(stats[-1], pathtracer.NODE_BYTES[pathtracer.BVH2_FP32]),
+            "what": "binary FP32 BVH, warps refilled only when all lanes are idle, host-driven loop, 1,048,576 slots, no autotune"}
+
+
+def cornell_section(knobs):
+    """Cornell box, 512x512, 16 spp, depth 8, NEE (36 triangles, 2-entry alias table)."""
+    import pathtracer
+    import scenes
+    s = scenes.config_scene("cornell")
+    r = pathtracer.Renderer(0)
+    try:
+        r.upload_scene(s)
+        W, H, spp, depth = 512, 512, 16, 8
+        cam = scenes.scene_camera(s, W, H)
+        tuned = r.autotune(cam, W, H, spp, depth, True)
+        kn = {k: tuned[k] for k in ("pool_size", "trace_occupancy", "trace_refill", "trace_block")}
+        for _ in range(3):
+            r.render_frame(cam, W, H, spp, depth, True, **kn)
+        stats = [r.render_frame(cam, W, H, spp, depth, True, **kn) for _ in range(10)]
+        ms = sum(x["device_ms"] for x in stats) / len(stats)
+        rays = sum(x["rays"] + x["shadow_rays"] for x in stats) / len(stats)
+        plain = plain_form(r, cam, W, H, spp, depth)
+    finally:
+        r.close()
+    return {"value": W * H * spp / (ms / 1000.0), "unit": "paths/s", "ms_per_frame": ms,
+            "mrays_per_second": rays / (ms / 1000.0) / 1e6, "knobs": kn, "plain_form_paths_per_second": plain["value"],
+            "config": "cornell box (36 triangles), 512x512, 16 spp, depth 8, NEE"}
+
+
+def _server_knobs(knobs):
+    return dict(trace_block=knobs["trace_block"], trace_refill=knobs["trace_refill"],
+                trace_occupancy=knobs["trace_occupancy"])
+
+
+def _run_jobs_on_server(srv, ids, jobs, open_loop):
+    """Submits the jobs (at their arrival times when open_loop, else all at once), waits for all and
+    reads every image back. Returns (wall seconds, per-job latency seconds)."""
+    t0 = time.perf_counter()
+    jids = []
+    for j in jobs:
+        if open_loop:
+            delay = j.arrival_s - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+        jids.append(srv.submit(ids[j.scene], j.camera, j.width, j.height, j.spp, j.depth, True))
+    lat = []
+    for jid in jids:
+        st = srv.wait(jid, 3600.0)
+        if st["state"] != "done":
+            raise RuntimeError(f"job {jid} ended as {st['state']}: {srv.last_error()}")
+        srv.result(jid)
+        lat.append(st["done_s"] - st["submit_s"])
+        srv.release(jid)
+    return time.perf_counter() - t0, lat
+
+
+def batched_section(knobs):
+    """64 uneven jobs over 4 resident scenes: one device loop for all (job server) against one job at
+    a time (server with max_active_jobs=1, the optimised frame renderer, and the plain form)."""
+    import pathtracer
+    import scenes
+    import workloads
+    jobs = workloads.batched_jobs()
+    resident = {n: scenes.config_scene(n) for n in workloads.BATCH_SCENES}
+    total = sum(j.paths for j in jobs)
+    out = {"jobs": len(jobs), "paths": total, "scenes": {n: s.triangle_count for n, s in resident.items()},
+           "config": "64 jobs, resolution log-uniform 256x256..1920x1080, spp in {1,4,16,64}, depth 8..12, seeded orbit cameras"}
+    warm = [workloads.Job(n, 64, 64, 1, 8, scenes.scene_camera(s, 64, 64)) for n, s in resident.items()]
+    for mode, active in (("batched", 0), ("server_one_at_a_time", 1)):
+        srv = pathtracer.Server(0, pool_size=knobs["pool_size"], max_active_jobs=active, hbm_budget_bytes=32 << 30,
+                                **_server_knobs(knobs))
+        try:
+            ids = {n: srv.add_scene(s) for n, s in resident.items()}
+            _run_jobs_on_server(srv, ids, warm, False)
+            before = srv.stats()
+            wall, _ = _run_jobs_on_server(srv, ids, jobs, False)
+            st = srv.stats()
+        finally:
+            srv.close()
+        dev_ms = st["device_ms"] - before["device_ms"]
+        out[mode] = {"paths_per_second": total / wall, "device_paths_per_second": total / (dev_ms / 1000.0),
+                     "wall_s": wall, "device_s": dev_ms / 1000.0, "slices": st["slices"] - before["slices"],
+                     "admitted_high_water_bytes": st["admitted_high_water"]}
+    # one frame at a time through gpt_render_frame: optimised (BVH8, graph loop) and plain form
+    renderers = {}
+    try:
+        for n, s in resident.items():
+            renderers[n] = pathtracer.Renderer(0)
+            renderers[n].upload_scene(s)
+        plain_settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
+                              loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32)
+        for mode, settings in (("frames_one_at_a_time", dict(knobs)), ("plain_form_one_at_a_time", plain_settings)):
+            for j in warm:
+                renderers[j.scene].render_frame(j.camera, j.width, j.height, j.spp, j.depth, True, **settings)
+            t0 = time.perf_counter()
+            dev = 0.0
+            for j in jobs:
+                st = renderers[j.scene].render_frame(j.camera, j.width, j.height, j.spp, j.depth, True, **settings)
+                dev += st["device_ms"]
+            wall = time.perf_counter() - t0
+            out[mode] = {"paths_per_second": total / wall, "device_paths_per_second": total / (dev / 1000.0),
+                         "wall_s": wall, "device_s": dev / 1000.0}
+    finally:
+        for r in renderers.values():
+            r.close()
+    out["speedup_vs_plain_form"] = out["batched"]["paths_per_second"] / out["plain_form_one_at_a_time"]["paths_per_second"]
+    out["speedup_vs_frames_one_at_a_time"] = out["batched"]["paths_per_second"] / out["frames_one_at_a_time"]["paths_per_second"]
+    out["timing"] = "wall clock from the first submit (or frame) to the last image read back to host memory"
+    return out
+
+
+def serving_section(knobs, rates, n_jobs):
+    """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time."""
+    import pathtracer
+    import scenes
+    import workloads
+    resident = {n: scenes.config_scene(n) for n in workloads.SERVE_SCENES}
+    out = {"scenes": {n: s.triangle_count for n, s in resident.items()}, "jobs_per_rate": n_jobs,
+           "budget_bytes": 16 << 30,
+           "config": "Poisson arrivals; resolution log-uniform 128x128..2048x2048, spp in {4,16,64,256}, depth 8..12, "
+                     "seeded orbit cameras; admission: 64 B per in-flight path + framebuffers within the budget",
+           "latency": "server done_s - submit_s per job (submission at the scheduled arrival time)"}
+    warm = [workloads.Job(n, 64, 64, 4, 8, scenes.scene_camera(s, 64, 64)) for n, s in resident.items()]
+    for mode, active in (("served", 0), ("plain", 1)):
+        srv = pathtracer.Server(0, pool_size=knobs["pool_size"], max_active_jobs=active, hbm_budget_bytes=16 << 30,
+                                **_server_knobs(knobs))
+        res = {}
+        try:
+            ids = {n: srv.add_scene(s) for n, s in resident.items()}
+            _run_jobs_on_server(srv, ids, warm, False)
+            for rate in rates:
+                jobs = workloads.served_jobs(rate, n_jobs)
+                before = srv.stats()
+                wall, lat = _run_jobs_on_server(srv, ids, jobs, True)
+                st = srv.stats()
+                paths = sum(j.paths for j in jobs)
+                res[f"{rate:g}_jobs_per_s"] = {
+                    "p50_latency_s": workloads.percentile(lat, 50), "p99_latency_s": workloads.percentile(lat, 99),
+                    "mean_latency_s": sum(lat) / len(lat), "paths_per_second": paths / wall, "wall_s": wall,
+                    "device_paths_per_second": paths / ((st["device_ms"] - before["device_ms"]) / 1000.0),
+                    "offered_paths_per_second": paths / jobs[-1].arrival_s}
+            res["admitted_high_water_bytes"] = srv.stats()["admitted_high_water"]
+        finally:
+            srv.close()
+        out[mode] = res
+    return out
+
+
+def precision_section(knobs):
+    """8M-triangle scene, 3840x2160, 16 spp, depth 10: quantised BVH8 against binary FP32 BVH, and
+    FP32 Kahan accumulation against FP64 accumulation of the same per-sample radiance."""
+    import pathtracer
+    import scenes
+    s = scenes.config_scene("spheres-8m")
+    W, H, spp, depth = 3840, 2160, 16, 10
+    r = pathtracer.Renderer(0)
+    out = {"config": "spheres-8m (400 displaced icospheres + ground, 4,096 emissive triangles), 3840x2160, 16 spp, depth 10, NEE"}
+    try:
+        t0 = time.perf_counter()
+        r.upload_scene(s)
+        out["scene_upload_s"] = time.perf_counter() - t0
+        info = r.scene_info()
+        out["triangles"], out["lights"] = info["triangles"], info["lights"]
+        cam = scenes.scene_camera(s, W, H)
+        formats = {}
+        for name, fmt in (("bvh8_q8", pathtracer.BVH8_Q8), ("bvh2_fp32", pathtracer.BVH2_FP32)):
+            r.render_frame(cam, W, H, spp, depth, True, bvh_format=fmt, **knobs)
+            st = r.render_frame(cam, W, H, spp, depth, True, bvh_format=fmt, **knobs)
+            formats[name] = {"paths_per_second": st["samples"] / (st["device_ms"] / 1000.0), "ms_per_frame": st["device_ms"],
+                             "nodes": info["nodes"] if fmt == pathtracer.BVH8_Q8 else info["binary_nodes"],
+                             "depth": info["depth"] if fmt == pathtracer.BVH8_Q8 else info["binary_depth"],
+                             "traversal": traversal_summary(st, pathtracer.NODE_BYTES[fmt])}
+            if fmt == pathtracer.BVH8_Q8:
+                fb8 = r.framebuffer()
+            else:
+                formats["identical_images"] = bool(np.array_equal(fb8, r.framebuffer()))
+        out["bvh"] = formats
+        # the BVH8 frame again for its buffers: per-pixel Kahan sums and the per-sample radiance
+        r.render_frame(cam, W, H, spp, depth, True, **knobs)
+        kahan = r.accumulation()[:, :3].astype(np.float64)
+        rad = r.sample_radiance().reshape(W * H, spp, 3)
+        fp64 = np.zeros((W * H, 3), dtype=np.float64)
+        naive = np.zeros((W * H, 3), dtype=np.float32)
+        for k in range(spp):  # sample order, as the resolve kernel sums
+            fp64 += rad[:, k, :].astype(np.float64)
+            naive += rad[:, k, :]
+        del rad
+        ref = fp64 / spp
+        rms_ref = float(np.sqrt(np.mean(ref ** 2)))
+        acc = {}
+        for name, img in (("fp32_kahan", kahan / spp), ("fp32_naive", naive.astype(np.float64) / spp)):
+            err = img - ref
+            per_pixel = np.sqrt(np.mean(err ** 2, axis=1))
+            acc[name] = {"image_rmse": float(np.sqrt(np.mean(err ** 2))),
+                         "image_rmse_relative": float(np.sqrt(np.mean(err ** 2))) / rms_ref if rms_ref > 0 else None,
+                         "per_pixel_rmse_max": float(per_pixel.max()),
+                         "per_pixel_rmse_p99": float(np.percentile(per_pixel, 99)),
+                         "pixels_exact": float(np.mean(np.all(err == 0.0, axis=1)))}
+        out["accumulation_vs_fp64"] = acc
+        out["fp64_image_rms"] = rms_ref
+    finally:
+        r.close()
+    return out
+
+
 def b200_arm(args):
     import torch
     import pathtracer
@@ -220,8 +487,9 @@ def b200_arm(args):
         tuned = renderer.autotune(cam, W, H, spp, depth, True)
         tuned["seconds"] = time.perf_counter() - t0
     knobs = dict(pool_size=args.pool or tuned.get("pool_size", WORKLOAD["pool"]),
-                 trace_occupancy=tuned.get("trace_occupancy", 0), trace_refill=tuned.get("trace_refill", 0),
-                 trace_block=tuned.get("trace_block", 0))
+                 trace_occupancy=tuned.get("trace_occupancy", args.trace_occupancy),
+                 trace_refill=tuned.get("trace_refill", args.trace_refill),
+                 trace_block=tuned.get("trace_block", args.trace_block))
 
     def step():
         st = renderer.render_frame(cam, W, H, spp, depth, True, rng_offset=rng_offset, loop_mode=loop_mode, **knobs)
@@ -327,6 +595,42 @@ def b200_arm(args):
                                             "ms_per_frame": ref_ms, "iterations": frames[-1]["iterations"],
                                             "speedup_of_value": value / (samples_per_frame / (ref_ms / 1000.0)),
                                             "what": "reference kernels (Intersect/PathGeneration/MaterialEval/Iteration.cu) compiled for sm_100a, replayed RenderFrame loop"}
+    sections = wanted_sections(args) if (world == 1 and not args.profile_case) else set()
+    per_scene = {WORKLOAD["workload"]: {"value": value, "unit": "paths/s", "mrays_per_second": line["mrays_per_second"],
+                                        "config": "1920x1080, 64 spp, depth 12, NEE"}}
+    timings = {}
+
+    def run_section(name, fn):
+        t0 = time.perf_counter()
+        try:
+            return fn()
+        except Exception as e:  # a failed section is reported, the rest of the line stands
+            return {"error": f"{type(e).__name__}: {e}"}
+        finally:
+            timings[name] = time.perf_counter() - t0
+
+    if "plain" in sections:
+        pf = run_section("plain", lambda: plain_form(renderer, cam, W, H, spp, depth))
+        if "value" in pf:
+            pf["speedup_of_value"] = value / pf["value"]
+        line["plain_form"] = pf
+    renderer.close()
+    if "cornell" in sections:
+        per_scene["cornell"] = run_section("cornell", lambda: cornell_section(knobs))
+    if "batched" in sections:
+        line["batched"] = run_section("batched", lambda: batched_section(knobs))
+    if "serving" in sections:
+        rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
+        line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs))
+    if "precision" in sections:
+        pr = run_section("precision", lambda: precision_section(knobs))
+        line["precision"] = pr
+        if "bvh" in pr:
+            per_scene["spheres-8m"] = {"value": pr["bvh"]["bvh8_q8"]["paths_per_second"], "unit": "paths/s",
+                                       "config": "3840x2160, 16 spp, depth 10, NEE"}
+    if sections:
+        line["per_scene"] = per_scene
+        line["section_seconds"] = timings
     if world == 1 and not args.no_cpu_baseline:
         import oracle
         threads = oracle.default_threads()

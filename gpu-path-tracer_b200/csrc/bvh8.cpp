@@ -407,9 +407,90 @@ namespace pt
                 return me;
             }
         };
+
+        // The binary tree itself as 64-byte FP32 nodes in depth-first order (the plain format): each
+        // node holds the boxes of its two children, padded like the BVH8's (WideBuilder::padBox) and
+        // rounded outward to float, so the boxes contain their subtrees. A single-leaf root becomes a
+        // node with one valid child.
+        struct BinaryFlattener
+        {
+            const BinaryBuilder& bin;
+            std::vector<Node2> out;
+            uint32_t maxDepth = 0;
+
+            static void outwardBox(const Box& b, float lo[3], float hi[3])
+            {
+                double dlo[3], dhi[3];
+                WideBuilder::padBox(b, dlo, dhi);
+                for (int k = 0; k < 3; k++)
+                {
+                    float l = static_cast<float>(dlo[k]);
+                    if (static_cast<double>(l) > dlo[k]) l = std::nextafter(l, -FLT_MAX);
+                    float h = static_cast<float>(dhi[k]);
+                    if (static_cast<double>(h) < dhi[k]) h = std::nextafter(h, FLT_MAX);
+                    lo[k] = l;
+                    hi[k] = h;
+                }
+            }
+
+            uint32_t emit(uint32_t bnode, uint32_t depth)
+            {
+                maxDepth = std::max(maxDepth, depth + 1);
+                const uint32_t me = static_cast<uint32_t>(out.size());
+                out.push_back(Node2{});
+                const BNode& nd = bin.nodes[bnode];
+                uint32_t kids[2] = {bnode, kInvalid};
+                if (!nd.leaf())
+                {
+                    kids[0] = nd.left;
+                    kids[1] = nd.right;
+                }
+                float lo[2][3], hi[2][3];
+                uint32_t ref[2] = {0, 0}, count[2] = {0, 0}, leafMask = 0, validMask = 0;
+                for (int i = 0; i < 2; i++)
+                {
+                    if (kids[i] == kInvalid)
+                    {
+                        for (int k = 0; k < 3; k++)
+                        {
+                            lo[i][k] = FLT_MAX;
+                            hi[i][k] = -FLT_MAX;
+                        }
+                        continue;
+                    }
+                    const BNode& c = bin.nodes[kids[i]];
+                    outwardBox(c.box, lo[i], hi[i]);
+                    validMask |= 1u << i;
+                    if (c.leaf())
+                    {
+                        if (c.count > 255) throw std::runtime_error("BVH leaf larger than 255 triangles");
+                        ref[i] = c.first;
+                        count[i] = c.count;
+                        leafMask |= 1u << i;
+                    }
+                    else
+                    {
+                        ref[i] = emit(kids[i], depth + 1);
+                    }
+                }
+                auto bits = [](float f)
+                {
+                    uint32_t u;
+                    std::memcpy(&u, &f, 4);
+                    return u;
+                };
+                Node2 node{};
+                node.w[0] = make_uint4(bits(lo[0][0]), bits(lo[0][1]), bits(lo[0][2]), bits(hi[0][0]));
+                node.w[1] = make_uint4(bits(hi[0][1]), bits(hi[0][2]), bits(lo[1][0]), bits(lo[1][1]));
+                node.w[2] = make_uint4(bits(lo[1][2]), bits(hi[1][0]), bits(hi[1][1]), bits(hi[1][2]));
+                node.w[3] = make_uint4(ref[0], ref[1], count[0] | (count[1] << 8) | (leafMask << 16) | (validMask << 24), 0u);
+                out[me] = node;
+                return me;
+            }
+        };
     }
 
-    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads)
+    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads, bool withBinary)
     {
         if (n == 0) throw std::runtime_error("scene has no triangles");
         BinaryBuilder b;
@@ -436,6 +517,14 @@ namespace pt
         Bvh8 result;
         result.nodes = std::move(w.out);
         result.depth = w.maxDepth;
+        if (withBinary)
+        {
+            BinaryFlattener f{b, {}, 0};
+            f.out.reserve(b.nodeCount.load() / 2 + 1);
+            f.emit(root, 0);
+            result.nodes2 = std::move(f.out);
+            result.depth2 = f.maxDepth;
+        }
         result.order = b.idx;
         result.tris.resize(static_cast<size_t>(n) * 3);
         for (uint32_t j = 0; j < n; j++)
@@ -527,6 +616,56 @@ namespace pt
                 }
             }
         }
+
+        // Same for the binary FP32 tree: each child box (exact float values) must contain its subtree.
+        void check_binary(CheckState& cs, uint32_t node, double lo[3], double hi[3])
+        {
+            const Node2& n = cs.b.nodes2[node];
+            float f[12];
+            std::memcpy(f, &n.w[0], 48);  // lo0 xyz, hi0 xyz, lo1 xyz, hi1 xyz
+            const uint32_t meta = n.w[3].z;
+            const uint32_t ref[2] = {n.w[3].x, n.w[3].y};
+            for (int k = 0; k < 3; k++)
+            {
+                lo[k] = DBL_MAX;
+                hi[k] = -DBL_MAX;
+            }
+            for (int c = 0; c < 2; c++)
+            {
+                if (!((meta >> (24 + c)) & 1u)) continue;
+                double clo[3], chi[3];
+                if ((meta >> (16 + c)) & 1u)
+                {
+                    for (int k = 0; k < 3; k++)
+                    {
+                        clo[k] = DBL_MAX;
+                        chi[k] = -DBL_MAX;
+                    }
+                    const uint32_t count = (meta >> (8 * c)) & 0xFFu;
+                    for (uint32_t j = 0; j < count; j++)
+                    {
+                        const uint32_t t = cs.b.order[ref[c] + j];
+                        cs.seen[t]++;
+                        cs.leafTriangles++;
+                        for (int v = 0; v < 3; v++)
+                            for (int k = 0; k < 3; k++)
+                            {
+                                const double x = cs.positions[(static_cast<size_t>(t) * 3 + v) * 3 + k];
+                                clo[k] = std::min(clo[k], x);
+                                chi[k] = std::max(chi[k], x);
+                            }
+                    }
+                }
+                else
+                    check_binary(cs, ref[c], clo, chi);
+                for (int k = 0; k < 3; k++)
+                {
+                    if (!(static_cast<double>(f[c * 6 + k]) <= clo[k] && static_cast<double>(f[c * 6 + 3 + k]) >= chi[k])) cs.violations++;
+                    lo[k] = std::min(lo[k], clo[k]);
+                    hi[k] = std::max(hi[k], chi[k]);
+                }
+            }
+        }
     }
 
     Bvh8Check CheckBvh8(const Bvh8& b, const float* positions, uint32_t n)
@@ -540,6 +679,14 @@ namespace pt
         r.trianglesNotExactlyOnce = 0;
         for (uint32_t t = 0; t < n; t++)
             if (cs.seen[t] != 1) r.trianglesNotExactlyOnce++;
+        if (!b.nodes2.empty())
+        {
+            CheckState bs{b, positions, std::vector<uint32_t>(n, 0)};
+            check_binary(bs, 0, lo, hi);
+            r.containmentViolations += bs.violations;
+            for (uint32_t t = 0; t < n; t++)
+                if (bs.seen[t] != 1) r.trianglesNotExactlyOnce++;
+        }
         return r;
     }
 }

@@ -13,10 +13,13 @@ namespace pt
         std::vector<float4> tris;      // 3 per triangle, leaf order: (v0, orig), (e1, model), (e2, 0)
         std::vector<uint32_t> order;   // leaf position -> input triangle index
         uint32_t depth = 0;            // levels of the wide tree
+        std::vector<Node2> nodes2;     // the binary tree the BVH8 is collapsed from, FP32 boxes (same leaf order)
+        uint32_t depth2 = 0;           // levels of the binary tree
     };
 
-    // positions: [n][3][3] world positions; models: shading model per triangle.
-    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads);
+    // positions: [n][3][3] world positions; models: shading model per triangle. withBinary: also
+    // flatten the binary tree into FP32 Node2 records (nodes2, depth2).
+    Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads, bool withBinary = false);
 
     struct Bvh8Check
     {

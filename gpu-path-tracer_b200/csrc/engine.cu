@@ -233,6 +233,7 @@ namespace pt
             threads_ = cfg_.trace_block == 64 ? 64 : 128;
             refill_ = cfg_.trace_refill ? std::min(32u, std::max(1u, cfg_.trace_refill)) : 16u;
             occupancy_ = cfg_.trace_occupancy == 0 ? 10 : (cfg_.trace_occupancy >= 12 ? 12 : (cfg_.trace_occupancy >= 10 ? 10 : 1));
+            shortestFirst_ = cfg_.schedule != GPT_SCHEDULE_OLDEST_FIRST;
             t0_ = std::chrono::steady_clock::now();
         }
 
@@ -256,6 +257,7 @@ namespace pt
 
         Status Init()
         {
+            if (cfg_.schedule > GPT_SCHEDULE_OLDEST_FIRST) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&startEvent_));
@@ -614,8 +616,19 @@ namespace pt
                 active_.push_back(J.id);
                 pending_.pop_front();
             }
+            // Slot priority of the next slice: the device plan hands idle slots to the jobs in this order.
+            std::vector<std::pair<uint64_t, uint32_t>> ranked;
+            ranked.reserve(active_.size());
+            for (uint64_t id : active_)
+            {
+                const uint32_t t = records_[id].tableIndex;
+                const JobView& v = mirror_[t];
+                const uint64_t left = v.totalSamples > v.launched ? v.totalSamples - v.launched : 0;
+                ranked.emplace_back(shortestFirst_ ? left : 0, t);  // stable: submission order among equals
+            }
+            std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
             uint32_t n = 0;
-            for (uint64_t id : active_) orderHost_[n++] = records_[id].tableIndex;
+            for (const auto& r : ranked) orderHost_[n++] = r.second;
             sliceWords_[0] = n;
             sliceWords_[1] = 0;
             sliceWords_[2] = cfg_.max_slice_iterations;
@@ -742,6 +755,7 @@ namespace pt
         int device_;
         gpt_server_config cfg_;
         int threads_ = 128, occupancy_ = 10;
+        bool shortestFirst_ = true;
         uint32_t refill_ = 16;
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;

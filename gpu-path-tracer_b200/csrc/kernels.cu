@@ -81,6 +81,121 @@ namespace pt
         int sp;
     };
 
+    // Triangles [first, first + count) of a leaf (leaf order). Returns false when an any-hit query
+    // found an occluder (traversal over); closest hit keeps the best hit in st.hit.
+    template <bool ANY>
+    __device__ __forceinline__ bool leaf_tests(const SceneView& sc, TraversalState& st, uint32_t first, uint32_t count, bool& occluded,
+                                               uint32_t& tests)
+    {
+        tests += count;
+        for (uint32_t k = 0; k < count; k++)
+        {
+            const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
+            const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+            float t, u, v;
+            if (!intersect_triangle(a, b, c, st.ray, t, u, v)) continue;
+            if (ANY)
+            {
+                if (t >= st.ray.tmin && t < st.hit.t)
+                {
+                    occluded = true;
+                    return false;
+                }
+            }
+            else
+            {
+                const uint32_t orig = __float_as_uint(a.w);
+                if (better_hit(t, orig, st.ray.tmin, st.hit))
+                {
+                    st.hit.t = t;
+                    st.hit.tri = orig;
+                    st.hit.u = u;
+                    st.hit.v = v;
+                    st.hit.model = __float_as_uint(b.w);
+                }
+            }
+        }
+        return true;
+    }
+
+    // Slab test of one FP32 box of a binary node against [tmin, tmax]. Each per-axis distance is one
+    // subtraction and one multiplication by the rounded reciprocal (at most 3 roundings, relative error
+    // below 2^-21); entry distances are lowered and exit distances raised by 2^-20 of their magnitude,
+    // so a box the exact arithmetic would hit is never culled. tnear: the widened entry distance.
+    __device__ __forceinline__ bool slab_fp32(float lx, float ly, float lz, float hx, float hy, float hz, const RayPre& r, float tmax,
+                                              float& tnear)
+    {
+        const float kEps = 9.5367431640625e-07f;  // 2^-20
+        const float ax = (lx - r.o.x) * r.invd.x, bx = (hx - r.o.x) * r.invd.x;
+        const float ay = (ly - r.o.y) * r.invd.y, by = (hy - r.o.y) * r.invd.y;
+        const float az = (lz - r.o.z) * r.invd.z, bz = (hz - r.o.z) * r.invd.z;
+        float nx = fminf(ax, bx), fx = fmaxf(ax, bx);
+        float ny = fminf(ay, by), fy = fmaxf(ay, by);
+        float nz = fminf(az, bz), fz = fmaxf(az, bz);
+        nx = nx - fabsf(nx) * kEps;
+        ny = ny - fabsf(ny) * kEps;
+        nz = nz - fabsf(nz) * kEps;
+        fx = fx + fabsf(fx) * kEps;
+        fy = fy + fabsf(fy) * kEps;
+        fz = fz + fabsf(fz) * kEps;
+        const float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, r.tmin));
+        const float tf = fminf(fminf(fx, fy), fminf(fz, tmax));
+        tnear = tn;
+        return tn <= tf;
+    }
+
+    // Binary FP32 BVH: visit one node (two child boxes) or pop the next node. Leaf children that the
+    // ray enters are tested at once; of two internal children the nearer is visited next and the
+    // farther pushed. Stack entries are node indices. Returns false when traversal is over.
+    template <bool ANY>
+    __device__ __forceinline__ bool traverse_step_binary(const SceneView& sc, TraversalState& st, uint32_t* stack, int stackCap,
+                                                         bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
+    {
+        uint32_t node;
+        if (st.pending != kInvalid)
+        {
+            node = st.pending;
+            st.pending = kInvalid;
+        }
+        else
+        {
+            if (st.sp == 0) return false;
+            node = stack[--st.sp];
+        }
+        const uint4* nw = sc.nodes2[node].w;
+        visits++;
+        const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
+        float tn0, tn1;
+        const bool h0 = ((w3.z >> 24) & 1u) &&
+                        slab_fp32(__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z), __uint_as_float(w0.w),
+                                  __uint_as_float(w1.x), __uint_as_float(w1.y), st.ray, st.hit.t, tn0);
+        const bool h1 = ((w3.z >> 25) & 1u) &&
+                        slab_fp32(__uint_as_float(w1.z), __uint_as_float(w1.w), __uint_as_float(w2.x), __uint_as_float(w2.y),
+                                  __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, st.hit.t, tn1);
+        const uint32_t leafMask = (w3.z >> 16) & 3u;
+        if (h0 && (leafMask & 1u))
+            if (!leaf_tests<ANY>(sc, st, w3.x, w3.z & 0xFFu, occluded, tests)) return false;
+        if (h1 && (leafMask & 2u))
+            if (!leaf_tests<ANY>(sc, st, w3.y, (w3.z >> 8) & 0xFFu, occluded, tests)) return false;
+        const bool in0 = h0 && !(leafMask & 1u), in1 = h1 && !(leafMask & 2u);
+        if (in0 && in1)
+        {
+            if (st.sp >= stackCap)
+            {
+                atomicOr(errorFlags, static_cast<uint32_t>(kErrStackOverflow));
+                return false;
+            }
+            const bool first0 = tn0 <= tn1;
+            stack[st.sp++] = first0 ? w3.y : w3.x;
+            st.pending = first0 ? w3.x : w3.y;
+        }
+        else if (in0)
+            st.pending = w3.x;
+        else if (in1)
+            st.pending = w3.y;
+        return true;
+    }
+
     // Visit one node or pop the next child group. Returns false when traversal is over.
     // ANY: stops at the first triangle with tmin <= t < tmax.
     template <bool ANY>
@@ -120,34 +235,7 @@ namespace pt
             const uint32_t slot = i ^ st.ray.oct;
             const uint32_t first = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
             const uint32_t count = __ldg(reinterpret_cast<const unsigned char*>(&nw[6]) + slot);
-            tests += count;
-            for (uint32_t k = 0; k < count; k++)
-            {
-                const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
-                const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
-                float t, u, v;
-                if (!intersect_triangle(a, b, c, st.ray, t, u, v)) continue;
-                if (ANY)
-                {
-                    if (t >= st.ray.tmin && t < st.hit.t)
-                    {
-                        occluded = true;
-                        return false;
-                    }
-                }
-                else
-                {
-                    const uint32_t orig = __float_as_uint(a.w);
-                    if (better_hit(t, orig, st.ray.tmin, st.hit))
-                    {
-                        st.hit.t = t;
-                        st.hit.tri = orig;
-                        st.hit.u = u;
-                        st.hit.v = v;
-                        st.hit.model = __float_as_uint(b.w);
-                    }
-                }
-            }
+            if (!leaf_tests<ANY>(sc, st, first, count, occluded, tests)) return false;
         }
         if (innerSlots)
         {
@@ -283,12 +371,25 @@ namespace pt
     // idle the warp takes that many new rays with one atomic (ballot + popc + shuffle), so lanes
     // that finished early are refilled instead of idling until the slowest ray of the warp ends.
     // Traversal stack: STACK entries per thread in shared memory, entry = node << 8 | child mask.
-    template <int STACK, bool ANY, int MINB, class Work>
+    // BINARY: the binary FP32 BVH with a per-thread stack of kMaxStack entries in local memory (the
+    // plain format); otherwise the BVH8 with the shared-memory stack.
+    template <int STACK, bool ANY, int MINB, bool BINARY, class Work>
     __global__ void __launch_bounds__(128, MINB) trace_kernel(Work work, uint32_t refill, uint32_t* errorFlags)
     {
         extern __shared__ uint32_t smem[];
-        uint32_t* stack = smem + threadIdx.x;
-        const uint32_t stride = blockDim.x;
+        uint32_t localStack[BINARY ? kMaxStack : 1];
+        uint32_t* stack;
+        uint32_t stride;
+        if constexpr (BINARY)
+        {
+            stack = localStack;
+            stride = 1;
+        }
+        else
+        {
+            stack = smem + threadIdx.x;
+            stride = blockDim.x;
+        }
         Counters* ctr = work.counters();
         phase_begin(ctr, Work::kPhase);
         const uint32_t n = work.count();
@@ -340,7 +441,12 @@ namespace pt
                 bool more = true;
 #pragma unroll 1
                 for (int k = 0; k < 4 && more; k++)
-                    more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags, visits, tests);
+                {
+                    if constexpr (BINARY)
+                        more = traverse_step_binary<ANY>(work.sc, st, stack, STACK, occluded, errorFlags, visits, tests);
+                    else
+                        more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags, visits, tests);
+                }
                 if (!more)
                 {
                     work.finish(index, tag, st.hit, occluded);
@@ -1642,7 +1748,15 @@ namespace pt
         cudaError_t launch_trace_t(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
         {
             const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
-            trace_kernel<STACK, ANY, MINB, Work><<<blocks, threads, smem, s>>>(w, refill, err);
+            trace_kernel<STACK, ANY, MINB, false, Work><<<blocks, threads, smem, s>>>(w, refill, err);
+            return cudaGetLastError();
+        }
+
+        // Binary FP32 BVH (local-memory stack of kMaxStack entries, no shared memory).
+        template <bool ANY, class Work>
+        cudaError_t launch_trace_binary(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
+        {
+            trace_kernel<kMaxStack, ANY, 1, true, Work><<<blocks, threads, 0, s>>>(w, refill, err);
             return cudaGetLastError();
         }
 
@@ -1669,7 +1783,7 @@ namespace pt
         {
             int perSm = 0;
             const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<STACK, false, MINB, WavefrontClosest>, threads, smem);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<STACK, false, MINB, false, WavefrontClosest>, threads, smem);
             return perSm;
         }
 
@@ -1682,11 +1796,17 @@ namespace pt
         }
     }
 
-    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy)
+    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy, uint32_t bvhFormat)
     {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         int perSm;
+        if (bvhFormat == kBvh2Fp32)
+        {
+            perSm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<kMaxStack, false, 1, true, WavefrontClosest>, threads, 0);
+            return sms * (perSm < 1 ? 1 : perSm);
+        }
         if (depth <= 8) perSm = resident_blocks_m<8>(occupancy, threads);
         else if (depth <= 16) perSm = resident_blocks_m<16>(occupancy, threads);
         else if (depth <= 32) perSm = resident_blocks_m<32>(occupancy, threads);
@@ -1714,8 +1834,12 @@ namespace pt
     {
         cudaError_t e;
         WavefrontClosest wc{L.scene, L.wf, nullptr};
+        const bool binary = L.bvhFormat == kBvh2Fp32;
         if (L.traceStart && (e = cudaEventRecord(L.traceStart, s)) != cudaSuccess) return e;
-        e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+        if (binary)
+            e = launch_trace_binary<false>(wc, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+        else
+            e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
         if (L.traceStop && (e = cudaEventRecord(L.traceStop, s)) != cudaSuccess) return e;
         for (uint32_t m = 0; m < kModelCount; m++)
@@ -1726,7 +1850,10 @@ namespace pt
         if (L.nee && L.scene.lightCount > 0)
         {
             WavefrontShadow ws{L.scene, L.wf, nullptr};
-            e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            if (binary)
+                e = launch_trace_binary<true>(ws, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            else
+                e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
         regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
@@ -1808,9 +1935,15 @@ namespace pt
     }
 
     cudaError_t launch_batch_trace(const SceneView& sc, uint32_t root, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
-                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s)
+                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t s,
+                                   uint32_t bvhFormat)
     {
         BatchRays b{sc, rays, n, cursor, triOut, uvtOut, occOut, root};
+        if (bvhFormat == kBvh2Fp32)
+        {
+            if (occOut) return launch_trace_binary<true>(b, blocks, threads, 32, errorFlags, s);
+            return launch_trace_binary<false>(b, blocks, threads, 32, errorFlags, s);
+        }
         if (occOut) return launch_trace<true>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
         return launch_trace<false>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
     }

@@ -21,6 +21,7 @@ namespace pt
         int occupancy;             // traversal kernel variant: 1, 10 or 12 resident blocks per SM targeted
         int shadeBlocks;
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
+        uint32_t bvhFormat;        // kBvh8Quantised or kBvh2Fp32 (scene.nodes2 must be present)
         cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
         cudaEvent_t traceStop;
     };
@@ -42,7 +43,7 @@ namespace pt
         bool graphLoop;
     };
 
-    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy);
+    int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy, uint32_t bvhFormat = kBvh8Quantised);
     cudaError_t launch_engine_init(const Wavefront& wf, const EngineView& ev, uint32_t pool, cudaStream_t stream);
     cudaError_t launch_engine_iteration(const EngineLaunch& launch, cudaStream_t stream);
     cudaError_t launch_rebase_field(uint32_t* base, uint32_t n, uint32_t strideWords, uint32_t offset, bool skipInvalid, cudaStream_t stream);
@@ -52,7 +53,8 @@ namespace pt
     cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t stream);
     cudaError_t launch_clear(uint32_t* framebuffer, uint32_t n, uint32_t value, cudaStream_t stream);
     cudaError_t launch_batch_trace(const SceneView& scene, uint32_t root, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
-                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t stream);
+                                   float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t stream,
+                                   uint32_t bvhFormat = kBvh8Quantised);
     cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
                                        const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t stream);
     cudaError_t launch_light_build(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,

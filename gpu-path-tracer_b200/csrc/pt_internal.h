@@ -52,6 +52,25 @@ namespace pt
     };
     static_assert(sizeof(Node8) == 128, "BVH8 node is 128 bytes");
 
+    // Binary BVH node with FP32 child boxes, 64 bytes = 4 x uint4 (the plain format, compared with the
+    // quantised BVH8 on the same binned-SAH binary tree the BVH8 is collapsed from).
+    //  w[0] = lo0.x, lo0.y, lo0.z, hi0.x      (float bits; child boxes padded and rounded outward)
+    //  w[1] = hi0.y, hi0.z, lo1.x, lo1.y
+    //  w[2] = lo1.z, hi1.x, hi1.y, hi1.z
+    //  w[3] = ref0, ref1, count0 | count1 << 8 | leafMask << 16 | validMask << 24, 0
+    // ref: internal child -> node index, leaf child -> first triangle (leaf order, shared with BVH8).
+    struct __align__(16) Node2
+    {
+        uint4 w[4];
+    };
+    static_assert(sizeof(Node2) == 64, "binary BVH node is 64 bytes");
+
+    enum BvhFormat : uint32_t
+    {
+        kBvh8Quantised = 0,
+        kBvh2Fp32 = 1,
+    };
+
     struct __align__(16) MaterialDev  // == gpt_material
     {
         uint32_t model;
@@ -88,6 +107,8 @@ namespace pt
         uint32_t nodeCount;
         uint32_t triangleCount;
         uint32_t depth;           // BVH8 depth (stack entries needed)
+        const Node2* nodes2;      // binary FP32 BVH of the same scene (frame renderer only), nullptr if absent
+        uint32_t depth2;          // binary BVH depth
     };
 
     // Per resident scene: where its BVH8 starts in the packed node array and its slice of the

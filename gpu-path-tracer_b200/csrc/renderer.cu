@@ -126,7 +126,7 @@ namespace pt
 
     // Scene upload of Renderer::InitializeSceneBuffers (Renderer.cpp:292-306): validation, image textures,
     // BVH8 (host), shading records, light list and alias table (device).
-    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out)
+    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary)
     {
         if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
             d.material_count == 0)
@@ -179,7 +179,7 @@ namespace pt
         Bvh8 bvh;
         try
         {
-            bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+            bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), withBinary);
         }
         catch (const std::exception& e)
         {
@@ -197,6 +197,15 @@ namespace pt
         PT_TRY(scene->materials.allocate(static_cast<size_t>(d.material_count) * sizeof(MaterialDev)));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes.get<void>(), bvh.nodes.data(), bvh.nodes.size() * sizeof(Node8), cudaMemcpyHostToDevice, stream));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
+        if (withBinary)
+        {
+            if (bvh.depth2 > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "Binary BVH deeper than the traversal stack");
+            scene->nodeCount2 = static_cast<uint32_t>(bvh.nodes2.size());
+            scene->depth2 = bvh.depth2;
+            PT_TRY(scene->nodes2.allocate(bvh.nodes2.size() * sizeof(Node2)));
+            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes2.get<void>(), bvh.nodes2.data(), bvh.nodes2.size() * sizeof(Node2),
+                                                       cudaMemcpyHostToDevice, stream));
+        }
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materials.get<void>(), d.materials, static_cast<size_t>(d.material_count) * sizeof(MaterialDev), cudaMemcpyHostToDevice, stream));
         // Vertex attributes go up once; shading records, lights and the alias table are built on the device.
         DeviceBuffer pos, nrm, tan, uv, mid;
@@ -359,7 +368,7 @@ namespace pt
             if (rendering_.load()) return Status::Err(GPT_ERR_STATE, "Cannot upload a scene while rendering");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             std::unique_ptr<SceneGpu> scene;
-            PT_TRY(BuildScene(d, stream_, scene));
+            PT_TRY(BuildScene(d, stream_, scene, true));
             releaseGraph();
             scene->version = ++sceneVersion_;
             scene_ = std::move(scene);
@@ -374,6 +383,7 @@ namespace pt
             int traceThreads;
             uint32_t refill;
             int occupancy;
+            uint32_t bvh;
         };
 
         Status resolveConfig(const gpt_render_settings& s, FrameConfig& c) const
@@ -395,6 +405,10 @@ namespace pt
             if (c.traceThreads != 64 && c.traceThreads != 128) c.traceThreads = 128;
             c.refill = s.trace_refill ? std::min(32u, std::max(1u, s.trace_refill)) : 16u;
             c.occupancy = s.trace_occupancy == 0 ? 10 : (s.trace_occupancy >= 12 ? 12 : (s.trace_occupancy >= 10 ? 10 : 1));
+            if (s.bvh_format > GPT_BVH2_FP32) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown BVH format");
+            c.bvh = s.bvh_format == GPT_BVH2_FP32 ? kBvh2Fp32 : kBvh8Quantised;
+            if (c.bvh == kBvh2Fp32 && !scene_->nodeCount2)
+                return Status::Err(GPT_ERR_STATE, "The scene has no binary BVH");
             return Status::Ok();
         }
 
@@ -449,8 +463,9 @@ namespace pt
             L.nee = c.nee != 0;
             L.traceThreads = c.traceThreads;
             L.occupancy = c.occupancy;
-            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy);
+            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
+            L.bvhFormat = c.bvh;
             L.shadeBlocks = sms * 8;
             L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -489,8 +504,9 @@ namespace pt
             L.nee = c.nee != 0;
             L.traceThreads = c.traceThreads;
             L.occupancy = c.occupancy;
-            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy);
+            L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
+            L.bvhFormat = c.bvh;
             L.shadeBlocks = sms * 8;
             L.graphLoop = false;
             L.traceStart = traceStart_;
@@ -517,8 +533,8 @@ namespace pt
         std::string key(const FrameConfig& c) const
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool, c.nee,
-                          c.traceThreads, c.refill, c.occupancy, width_, height_, static_cast<void*>(accumulation_.get<void>()),
+            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
+                          c.nee, c.traceThreads, c.refill, c.occupancy, c.bvh, width_, height_, static_cast<void*>(accumulation_.get<void>()),
                           static_cast<void*>(framebuffer_.get<void>()));
             return buf;
         }
@@ -628,29 +644,29 @@ namespace pt
                 for (uint32_t occ : occupancies)
                     for (uint32_t refill : refills)
                         for (uint32_t tb : blocks)
-                        {
-                            trial.pool_size = pool;
-                            trial.trace_occupancy = occ;
-                            trial.trace_refill = refill;
-                            trial.trace_block = tb;
-                            float ms = 1e30f;
-                            for (int rep = 0; rep < 2; rep++)
                             {
-                                gpt_frame_stats st{};
-                                PT_TRY(RenderFrame(cam, trial, &st, false));
-                                if (rep) ms = st.device_ms;
+                                trial.pool_size = pool;
+                                trial.trace_occupancy = occ;
+                                trial.trace_refill = refill;
+                                trial.trace_block = tb;
+                                float ms = 1e30f;
+                                for (int rep = 0; rep < 2; rep++)
+                                {
+                                    gpt_frame_stats st{};
+                                    PT_TRY(RenderFrame(cam, trial, &st, false));
+                                    if (rep) ms = st.device_ms;
+                                }
+                                tried++;
+                                if (ms < bestMs)
+                                {
+                                    bestMs = ms;
+                                    best = base;
+                                    best.pool_size = pool;
+                                    best.trace_occupancy = occ;
+                                    best.trace_refill = refill;
+                                    best.trace_block = tb;
+                                }
                             }
-                            tried++;
-                            if (ms < bestMs)
-                            {
-                                bestMs = ms;
-                                best = base;
-                                best.pool_size = pool;
-                                best.trace_occupancy = occ;
-                                best.trace_refill = refill;
-                                best.trace_block = tb;
-                            }
-                        }
             }
             return Status::Ok();
         }
@@ -673,7 +689,7 @@ namespace pt
         }
 
         // ---------------------------------------------------------------- batch traversal
-        Status Intersect(const float* rays, uint32_t n, uint32_t* tri, float* uvt, uint8_t* occ, cudaStream_t s)
+        Status Intersect(const float* rays, uint32_t n, uint32_t* tri, float* uvt, uint8_t* occ, cudaStream_t s, uint32_t bvh = kBvh8Quantised)
         {
             if (!scene_) return Status::Err(GPT_ERR_NO_SCENE, "No scene has been uploaded");
             if (n == 0) return Status::Ok();
@@ -683,8 +699,9 @@ namespace pt
             uint32_t* cursor = cursor_.get<uint32_t>();
             PT_CUDA("cudaMemsetAsync", cudaMemsetAsync(cursor, 0, 8, st));
             const SceneView sv = scene_->view();
-            const int blocks = trace_grid_blocks(device_, 128, sv.depth, 1);
-            PT_CUDA("intersect", launch_batch_trace(sv, 0u, rays, n, cursor, tri, uvt, occ, blocks, 128, cursor + 1, st));
+            if (bvh == kBvh2Fp32 && !sv.nodes2) return Status::Err(GPT_ERR_STATE, "The scene has no binary BVH");
+            const int blocks = trace_grid_blocks(device_, 128, sv.depth, 1, bvh);
+            PT_CUDA("intersect", launch_batch_trace(sv, 0u, rays, n, cursor, tri, uvt, occ, blocks, 128, cursor + 1, st, bvh));
             uint32_t err = 0;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&err, cursor + 1, 4, cudaMemcpyDeviceToHost, st));
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(st));
@@ -1057,6 +1074,27 @@ extern "C"
         return Report(r, r->impl->Intersect(rays, n, nullptr, nullptr, occluded_out, static_cast<cudaStream_t>(stream)));
     }
 
+    int gpt_intersect_closest_binary(gpt_renderer* r, const float* rays, uint32_t n, uint32_t* tri_out, float* uvt_out, void* stream)
+    {
+        if (!r) return GPT_ERR_INVALID_ARGUMENT;
+        return Report(r, r->impl->Intersect(rays, n, tri_out, uvt_out, nullptr, static_cast<cudaStream_t>(stream), pt::kBvh2Fp32));
+    }
+
+    int gpt_intersect_any_binary(gpt_renderer* r, const float* rays, uint32_t n, uint8_t* occluded_out, void* stream)
+    {
+        if (!r || !occluded_out) return GPT_ERR_INVALID_ARGUMENT;
+        return Report(r, r->impl->Intersect(rays, n, nullptr, nullptr, occluded_out, static_cast<cudaStream_t>(stream), pt::kBvh2Fp32));
+    }
+
+    int gpt_scene_info_binary(const gpt_renderer* r, uint32_t* node_count, uint32_t* depth)
+    {
+        if (!r) return GPT_ERR_INVALID_ARGUMENT;
+        if (!r->impl->scene_) return GPT_ERR_NO_SCENE;
+        if (node_count) *node_count = r->impl->scene_->nodeCount2;
+        if (depth) *depth = r->impl->scene_->depth2;
+        return GPT_OK;
+    }
+
     int gpt_scene_info(const gpt_renderer* r, uint32_t* node_count, uint32_t* depth, uint32_t* light_count, uint32_t* triangle_count)
     {
         if (!r) return GPT_ERR_INVALID_ARGUMENT;
@@ -1091,7 +1129,7 @@ extern "C"
         try
         {
             pt::Bvh8 b = pt::BuildBvh8(d->positions, models.data(), d->triangle_count,
-                                       static_cast<int>(std::max(1u, std::thread::hardware_concurrency())));
+                                       static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), true);
             pt::Bvh8Check c = pt::CheckBvh8(b, d->positions, d->triangle_count);
             if (node_count) *node_count = static_cast<uint32_t>(b.nodes.size());
             if (depth) *depth = b.depth;

@@ -93,9 +93,10 @@ namespace pt
 
     struct SceneGpu
     {
-        DeviceBuffer nodes, tris, shading, materials, lights, bins, materialTextures, entry;
+        DeviceBuffer nodes, tris, shading, materials, lights, bins, materialTextures, entry, nodes2;
         std::vector<std::unique_ptr<TextureObject>> textures;
         uint32_t nodeCount = 0, triangleCount = 0, depth = 0, lightCount = 0, materialCount = 0;
+        uint32_t nodeCount2 = 0, depth2 = 0;  // binary FP32 BVH, built when the scene is uploaded with it
         bool modelPresent[kModelCount] = {};
         uint64_t version = 0;
         SceneView view() const
@@ -112,6 +113,8 @@ namespace pt
             v.nodeCount = nodeCount;
             v.triangleCount = triangleCount;
             v.depth = depth;
+            v.nodes2 = nodeCount2 ? nodes2.get<Node2>() : nullptr;
+            v.depth2 = depth2;
             return v;
         }
     };
@@ -119,6 +122,6 @@ namespace pt
     // Minimal PNG writer (zlib deflate) for SaveRenderedFrame (Renderer.cpp:649-675): RGBA8, rows
     // flipped vertically like Import::FlipVertically.
     // Validates a scene description and builds its device copy: image textures, BVH8 (host build),
-    // shading records, light list and alias table.
-    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out);
+    // shading records, light list and alias table; with `withBinary` also the binary FP32 BVH.
+    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary = false);
 }

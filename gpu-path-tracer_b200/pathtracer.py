@@ -61,9 +61,13 @@ class gpt_render_settings(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("samples_per_pixel", ctypes.c_uint32),
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
-                ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32)]
+                ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
+                ("bvh_format", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 LOOP_GRAPH, LOOP_HOST = 0, 1
+BVH8_Q8, BVH2_FP32 = 0, 1
+SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST = 1, 2
+NODE_BYTES = {BVH8_Q8: 128, BVH2_FP32: 64}
 
 
 class gpt_frame_stats(ctypes.Structure):
@@ -79,7 +83,7 @@ class gpt_server_config(ctypes.Structure):
     _fields_ = [("pool_size", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_active_jobs", ctypes.c_uint32),
                 ("ring_passes", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_uint64), ("trace_block", ctypes.c_uint32),
                 ("trace_refill", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
-                ("max_slice_iterations", ctypes.c_uint32)]
+                ("max_slice_iterations", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class gpt_job_desc(ctypes.Structure):
@@ -146,8 +150,14 @@ _SIGNATURES = [
                                              ctypes.c_void_p, ctypes.c_void_p]),
     ("gpt_intersect_any", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
                                          ctypes.c_void_p]),
+    ("gpt_intersect_closest_binary", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                    ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpt_intersect_any_binary", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                                                ctypes.c_void_p]),
     ("gpt_scene_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    ("gpt_scene_info_binary", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
+                                             ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_bvh8_check", ctypes.c_int, [ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
@@ -259,7 +269,10 @@ class Renderer:
         n, d, l, t = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
         self._check(self.L.gpt_scene_info(self.h, ctypes.byref(n), ctypes.byref(d), ctypes.byref(l), ctypes.byref(t)),
                     "gpt_scene_info")
-        return dict(nodes=n.value, depth=d.value, lights=l.value, triangles=t.value)
+        n2, d2 = ctypes.c_uint32(), ctypes.c_uint32()
+        self._check(self.L.gpt_scene_info_binary(self.h, ctypes.byref(n2), ctypes.byref(d2)), "gpt_scene_info_binary")
+        return dict(nodes=n.value, depth=d.value, lights=l.value, triangles=t.value, binary_nodes=n2.value,
+                    binary_depth=d2.value)
 
     def alias_table(self) -> np.ndarray:
         lights = self.scene_info()["lights"]
@@ -270,10 +283,11 @@ class Renderer:
 
     def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                     rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0) -> dict:
+                     rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0,
+                     bvh_format: int = BVH8_Q8) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
-                                 trace_refill, rng_offset, loop_mode, trace_occupancy)
+                                 trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, 0)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")
@@ -289,7 +303,7 @@ class Renderer:
     def autotune(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True) -> dict:
         """Measured tuning knobs for this workload: pool_size, trace_occupancy, trace_refill, trace_block."""
         cam = camera_struct(camera12)
-        base = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, 0, 0, 0, 0, 0, LOOP_GRAPH, 0)
+        base = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, 0, 0, 0, 0, 0, LOOP_GRAPH, 0, BVH8_Q8, 0)
         best = gpt_render_settings()
         ms = ctypes.c_float()
         n = ctypes.c_uint32()
@@ -336,34 +350,35 @@ class Renderer:
             self.L.gpt_unlock_frame(self.h)
 
     # -- ray batches on device memory (torch tensors as plumbing) --
-    def intersect_closest(self, rays_dev, tri_dev, uvt_dev, stream=None):
+    def intersect_closest(self, rays_dev, tri_dev, uvt_dev, stream=None, bvh_format: int = BVH8_Q8):
         n = rays_dev.shape[0]
-        self._check(self.L.gpt_intersect_closest(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
-                                                 ctypes.c_void_p(tri_dev.data_ptr()), ctypes.c_void_p(uvt_dev.data_ptr()),
-                                                 ctypes.c_void_p(stream)), "gpt_intersect_closest")
+        name = "gpt_intersect_closest_binary" if bvh_format == BVH2_FP32 else "gpt_intersect_closest"
+        self._check(getattr(self.L, name)(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
+                                          ctypes.c_void_p(tri_dev.data_ptr()), ctypes.c_void_p(uvt_dev.data_ptr()),
+                                          ctypes.c_void_p(stream)), name)
 
-    def intersect_any(self, rays_dev, occ_dev, stream=None):
+    def intersect_any(self, rays_dev, occ_dev, stream=None, bvh_format: int = BVH8_Q8):
         n = rays_dev.shape[0]
-        self._check(self.L.gpt_intersect_any(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
-                                             ctypes.c_void_p(occ_dev.data_ptr()), ctypes.c_void_p(stream)),
-                    "gpt_intersect_any")
+        name = "gpt_intersect_any_binary" if bvh_format == BVH2_FP32 else "gpt_intersect_any"
+        self._check(getattr(self.L, name)(self.h, ctypes.c_void_p(rays_dev.data_ptr()), n,
+                                          ctypes.c_void_p(occ_dev.data_ptr()), ctypes.c_void_p(stream)), name)
 
-    def trace_closest_np(self, rays: np.ndarray):
+    def trace_closest_np(self, rays: np.ndarray, bvh_format: int = BVH8_Q8):
         """Closest hits of a host ray batch [n, 8]: returns (tri [n] uint32, uvt [n, 3] float32)."""
         import torch
         r = torch.from_numpy(np.ascontiguousarray(rays, dtype=np.float32)).cuda()
         tri = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
         uvt = torch.empty((rays.shape[0], 3), dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
-        self.intersect_closest(r, tri, uvt)
+        self.intersect_closest(r, tri, uvt, bvh_format=bvh_format)
         return tri.cpu().numpy().view(np.uint32), uvt.cpu().numpy()
 
-    def trace_any_np(self, rays: np.ndarray):
+    def trace_any_np(self, rays: np.ndarray, bvh_format: int = BVH8_Q8):
         import torch
         r = torch.from_numpy(np.ascontiguousarray(rays, dtype=np.float32)).cuda()
         occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
         torch.cuda.synchronize()
-        self.intersect_any(r, occ)
+        self.intersect_any(r, occ, bvh_format=bvh_format)
         return occ.cpu().numpy()
 
     # -- asynchronous simulation (StartSimulation / StopRendering / ResumeSimulation) --
@@ -503,10 +518,10 @@ class Server:
 
     def __init__(self, device: int = 0, pool_size: int = 0, max_jobs: int = 0, max_active_jobs: int = 0,
                  ring_passes: int = 0, hbm_budget_bytes: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                 trace_occupancy: int = 0, max_slice_iterations: int = 0):
+                 trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0):
         self.L = lib()
         cfg = gpt_server_config(pool_size, max_jobs, max_active_jobs, ring_passes, hbm_budget_bytes, trace_block,
-                                trace_refill, trace_occupancy, max_slice_iterations)
+                                trace_refill, trace_occupancy, max_slice_iterations, schedule, 0)
         h = ctypes.c_void_p()
         rc = self.L.gpt_server_create(ctypes.byref(h), device, ctypes.byref(cfg))
         if rc != 0:

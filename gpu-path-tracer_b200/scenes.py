@@ -464,6 +464,25 @@ def sphere_field(n_spheres: int = 64, level: int = 5, n_lights: int = 256, seed:
     return _assemble(parts, mats, name or f"spheres-{n_spheres}x{level}", cam)
 
 
+# name: (spheres, subdivision level, emissive triangles, seed). Level-5 spheres have 20,480
+# triangles, level-4 ones 5,120; every field adds a 2-triangle ground plane.
+SPHERE_FIELDS = {
+    "spheres-1m": (64, 5, 256, 2),
+    "spheres-10k": (2, 4, 16, 3),
+    "spheres-200k": (10, 5, 64, 4),
+    "spheres-2m": (100, 5, 256, 5),
+    "spheres-8m": (400, 5, 4096, 6),
+    "spheres-small": (4, 3, 8, 7),
+    # resident scenes of the served workload (50k-4M triangles)
+    "spheres-50k": (10, 4, 32, 8),
+    "spheres-100k": (5, 5, 32, 9),
+    "spheres-250k": (12, 5, 64, 10),
+    "spheres-500k": (25, 5, 128, 11),
+    "spheres-3m": (150, 5, 256, 12),
+    "spheres-4m": (200, 5, 256, 13),
+}
+
+
 def config_scene(name: str) -> Scene:
     """Named workloads: 'cornell' (36 tris), 'spheres-1m' (64 spheres, 1.31 M tris),
     'spheres-10k', 'spheres-200k', 'spheres-2m', 'spheres-8m'."""
@@ -473,15 +492,7 @@ def config_scene(name: str) -> Scene:
         return cornell_all_models(1)
     if name == "cornell-textured":
         return cornell_textured(1)
-    table = {
-        "spheres-1m": (64, 5, 256, 2),
-        "spheres-10k": (2, 4, 16, 3),
-        "spheres-200k": (10, 5, 64, 4),
-        "spheres-2m": (100, 5, 256, 5),
-        "spheres-8m": (400, 5, 4096, 6),
-        "spheres-small": (4, 3, 8, 7),
-    }
-    n, lvl, nl, seed = table[name]
+    n, lvl, nl, seed = SPHERE_FIELDS[name]
     return sphere_field(n, lvl, nl, seed, name=name)
 
 

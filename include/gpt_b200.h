@@ -131,10 +131,16 @@ typedef struct gpt_render_settings {
                                      iteration and reads the loop condition after it (the reference's structure) */
     uint32_t trace_occupancy;     /* traversal kernel variant: 0/1 = registers unconstrained, 10 or 12 = that many
                                      resident 128-thread blocks per SM targeted (fewer registers, more warps) */
+    uint32_t bvh_format;          /* GPT_BVH8_Q8 (default): 8-wide BVH, 8-bit quantised child boxes, 128-B nodes;
+                                     GPT_BVH2_FP32: the binary BVH it is collapsed from, FP32 child boxes, 64-B nodes,
+                                     local-memory stack (the plain format; same hits, bit for bit) */
+    uint32_t reserved;
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
 #define GPT_LOOP_HOST 1u
+#define GPT_BVH8_Q8 0u
+#define GPT_BVH2_FP32 1u
 
 typedef struct gpt_frame_stats {
     uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */
@@ -142,7 +148,7 @@ typedef struct gpt_frame_stats {
     uint64_t samples;             /* paths rendered */
     uint64_t rays;                /* extension + camera rays traced (closest hit) */
     uint64_t shadow_rays;         /* NEE shadow rays traced (any hit) */
-    uint64_t node_visits[2];      /* BVH8 nodes visited: [0] closest-hit, [1] shadow traversal */
+    uint64_t node_visits[2];      /* BVH nodes visited (of the frame's bvh_format): [0] closest-hit, [1] shadow traversal */
     uint64_t triangle_tests[2];   /* triangles tested:   [0] closest-hit, [1] shadow traversal */
     float device_ms;              /* CUDA-event time of the frame graph on the render stream */
     float phase_ms[4];            /* device time per phase, summed over iterations: closest-hit traversal,
@@ -236,18 +242,29 @@ int gpt_intersect_closest(gpt_renderer* renderer, const float* rays, uint32_t n,
 int gpt_intersect_any(gpt_renderer* renderer, const float* rays, uint32_t n, uint8_t* occluded_out,
                       void* stream);
 
+/* The same queries against the binary FP32 BVH of the scene (the plain format; GPT_BVH2_FP32).
+ * They return the same triangles, (u, v, t) and occlusion bits as the BVH8 queries. */
+int gpt_intersect_closest_binary(gpt_renderer* renderer, const float* rays, uint32_t n, uint32_t* tri_out,
+                                 float* uvt_out, void* stream);
+int gpt_intersect_any_binary(gpt_renderer* renderer, const float* rays, uint32_t n, uint8_t* occluded_out,
+                             void* stream);
+
 /* Scene statistics after upload: BVH8 node count, tree depth, light count, triangle count. */
 int gpt_scene_info(const gpt_renderer* renderer, uint32_t* node_count, uint32_t* depth, uint32_t* light_count,
                    uint32_t* triangle_count);
+/* Node count and depth of the scene's binary FP32 BVH (HostBvh.cpp:22-100 builds the reference's
+ * binary tree by median splits; this one is the binned-SAH tree the BVH8 is collapsed from). */
+int gpt_scene_info_binary(const gpt_renderer* renderer, uint32_t* node_count, uint32_t* depth);
 /* The light alias table built on the device, [lights][4] words (q, p, alias, value)
  * (AliasTableView.hpp:8-14). */
 int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
 
 /*
- * Host-side validation of the BVH8 builder (no device work): builds the wide BVH for a scene and
- * checks in exact arithmetic that every quantised child box contains its subtree, and that every
- * triangle sits in exactly one leaf. Replaces nothing in the reference; it pins the structural
- * guarantee behind HostBvh.cpp:37-48's padded bounds for the quantised tree.
+ * Host-side validation of the BVH builder (no device work): builds the wide BVH and the binary FP32
+ * BVH for a scene and checks in exact arithmetic that every quantised BVH8 child box and every
+ * binary child box contains its subtree, and that every triangle sits in exactly one leaf of each
+ * tree (violations and misplaced triangles of both trees are summed). Replaces nothing in the
+ * reference; it pins the structural guarantee behind HostBvh.cpp:37-48's padded bounds.
  */
 int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* depth,
                    uint64_t* containment_violations, uint64_t* misplaced_triangles);
@@ -296,7 +313,9 @@ void gpt_obj_free(gpt_obj_scene* scene);
  * Admission accounting per job: 64 bytes per path the job may have in flight (min(ring passes x
  * pixels, pool)) plus its framebuffers (pass ring 12 B, Kahan accumulator 32 B, RGBA8 4 B per
  * pixel and pass). Jobs are admitted in submission order; a job larger than the whole budget is
- * refused at submission with GPT_ERR_CAPACITY. All gpt_server_* calls are thread-safe.
+ * refused at submission with GPT_ERR_CAPACITY. Among admitted jobs, idle path slots go first to
+ * the job with the fewest samples left (or to the oldest, by gpt_server_config.schedule); the order
+ * changes which job finishes first, never an image. All gpt_server_* calls are thread-safe.
  */
 typedef struct gpt_server gpt_server;
 
@@ -310,7 +329,13 @@ typedef struct gpt_server_config {
     uint32_t trace_refill;
     uint32_t trace_occupancy;
     uint32_t max_slice_iterations; /* wavefront iterations per graph launch at most (0 = 4096) */
+    uint32_t schedule;             /* which active job gets idle path slots first: 0/GPT_SCHEDULE_SHORTEST_FIRST = the
+                                      job with the fewest samples left, GPT_SCHEDULE_OLDEST_FIRST = submission order */
+    uint32_t reserved;
 } gpt_server_config;
+
+#define GPT_SCHEDULE_SHORTEST_FIRST 1u
+#define GPT_SCHEDULE_OLDEST_FIRST 2u
 
 typedef struct gpt_job_desc {
     uint32_t scene;                /* id from gpt_server_add_scene */

@@ -107,6 +107,26 @@ def test_mixed_jobs_match_alone(resident, frame_renderers):
         srv.close()
 
 
+@pytest.mark.parametrize("schedule", [pathtracer.SCHEDULE_SHORTEST_FIRST, pathtracer.SCHEDULE_OLDEST_FIRST])
+def test_schedule_orders_completion_not_images(resident, frame_renderers, schedule):
+    """Shortest-first hands idle slots to the job with the fewest samples left: a small job
+    submitted after a large one finishes first. Either policy gives the same images."""
+    srv, ids = make_server(resident, pool_size=4096, schedule=schedule)
+    try:
+        big = ("spheres-small", 128, 128, 64, 12, True, 0)
+        small = ("cornell-all", 16, 16, 1, 6, True, 0)
+        j_big = submit(srv, ids, resident, big)
+        j_small = submit(srv, ids, resident, small)
+        check_job(srv, j_small, frame_renderers, resident, small)
+        check_job(srv, j_big, frame_renderers, resident, big)
+        if schedule == pathtracer.SCHEDULE_SHORTEST_FIRST:
+            assert srv.poll(j_small)["done_s"] < srv.poll(j_big)["done_s"]
+    finally:
+        srv.close()
+    with pytest.raises(pathtracer.GptError):
+        pathtracer.Server(0, schedule=3)
+
+
 def test_tiny_pool_and_single_pass_ring(resident, frame_renderers):
     # 512 slots and one pass buffer per job: jobs wait on each other's slots and on their own folds
     srv, ids = make_server(resident, pool_size=512, ring_passes=1)
