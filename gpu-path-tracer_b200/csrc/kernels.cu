@@ -73,30 +73,45 @@ namespace pt
     __device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
 
     // ------------------------------------------------------------------ traversal
+    // Registers of a ray in flight. Values a traversal step reads rarely live in the thread's slot
+    // of shared memory instead (ColdSlot), which keeps the node test free of register spills.
     struct TraversalState
     {
         RayPre ray;
-        HitRecord hit;
+        float hitT;        // closest hit so far (tMax of the query until a hit)
+        uint32_t hitTri;   // input index of that triangle, kInvalid when none
         uint32_t pending;  // node to visit next, kInvalid when the stack decides
         int sp;
+    };
+
+    // Shared-memory slot of one thread: [0] = direction xyz, tag; [1] = hit u, v, model, queue index.
+    struct ColdSlot
+    {
+        float4* p;
+        __device__ float3 direction() const
+        {
+            const float4 a = p[0];
+            return make_float3(a.x, a.y, a.z);
+        }
     };
 
     // Triangles [first, first + count) of a leaf (leaf order). Returns false when an any-hit query
     // found an occluder (traversal over); closest hit keeps the best hit in st.hit.
     template <bool ANY>
-    __device__ __forceinline__ bool leaf_tests(const SceneView& sc, TraversalState& st, uint32_t first, uint32_t count, bool& occluded,
-                                               uint32_t& tests)
+    __device__ __forceinline__ bool leaf_tests(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t first, uint32_t count,
+                                               bool& occluded, uint32_t& tests)
     {
         tests += count;
+        const float3 d = cold.direction();
         for (uint32_t k = 0; k < count; k++)
         {
             const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
             const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
             float t, u, v;
-            if (!intersect_triangle(a, b, c, st.ray, t, u, v)) continue;
+            if (!intersect_triangle(a, b, c, st.ray.o, d, t, u, v)) continue;
             if (ANY)
             {
-                if (t >= st.ray.tmin && t < st.hit.t)
+                if (t >= st.ray.tmin && t < st.hitT)
                 {
                     occluded = true;
                     return false;
@@ -105,13 +120,13 @@ namespace pt
             else
             {
                 const uint32_t orig = __float_as_uint(a.w);
-                if (better_hit(t, orig, st.ray.tmin, st.hit))
+                if (better_hit(t, orig, st.ray.tmin, st.hitT, st.hitTri))
                 {
-                    st.hit.t = t;
-                    st.hit.tri = orig;
-                    st.hit.u = u;
-                    st.hit.v = v;
-                    st.hit.model = __float_as_uint(b.w);
+                    st.hitT = t;
+                    st.hitTri = orig;
+                    cold.p[1].x = u;
+                    cold.p[1].y = v;
+                    cold.p[1].z = b.w;  // shading model bits
                 }
             }
         }
@@ -148,7 +163,7 @@ namespace pt
     // ray enters are tested at once; of two internal children the nearer is visited next and the
     // farther pushed. Stack entries are node indices. Returns false when traversal is over.
     template <bool ANY>
-    __device__ __forceinline__ bool traverse_step_binary(const SceneView& sc, TraversalState& st, uint32_t* stack, int stackCap,
+    __device__ __forceinline__ bool traverse_step_binary(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, int stackCap,
                                                          bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
     {
         uint32_t node;
@@ -168,15 +183,15 @@ namespace pt
         float tn0, tn1;
         const bool h0 = ((w3.z >> 24) & 1u) &&
                         slab_fp32(__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z), __uint_as_float(w0.w),
-                                  __uint_as_float(w1.x), __uint_as_float(w1.y), st.ray, st.hit.t, tn0);
+                                  __uint_as_float(w1.x), __uint_as_float(w1.y), st.ray, st.hitT, tn0);
         const bool h1 = ((w3.z >> 25) & 1u) &&
                         slab_fp32(__uint_as_float(w1.z), __uint_as_float(w1.w), __uint_as_float(w2.x), __uint_as_float(w2.y),
-                                  __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, st.hit.t, tn1);
+                                  __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, st.hitT, tn1);
         const uint32_t leafMask = (w3.z >> 16) & 3u;
         if (h0 && (leafMask & 1u))
-            if (!leaf_tests<ANY>(sc, st, w3.x, w3.z & 0xFFu, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, w3.x, w3.z & 0xFFu, occluded, tests)) return false;
         if (h1 && (leafMask & 2u))
-            if (!leaf_tests<ANY>(sc, st, w3.y, (w3.z >> 8) & 0xFFu, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, w3.y, (w3.z >> 8) & 0xFFu, occluded, tests)) return false;
         const bool in0 = h0 && !(leafMask & 1u), in1 = h1 && !(leafMask & 2u);
         if (in0 && in1)
         {
@@ -199,7 +214,7 @@ namespace pt
     // Visit one node or pop the next child group. Returns false when traversal is over.
     // ANY: stops at the first triangle with tmin <= t < tmax.
     template <bool ANY>
-    __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, uint32_t* stack, uint32_t stride,
+    __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, uint32_t stride,
                                                   int stackCap, bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
     {
         uint32_t node;
@@ -225,7 +240,7 @@ namespace pt
         const uint4* nw = sc.nodes[node].w;
         visits++;
         const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3), w6 = ldg4(nw + 6);
-        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, w6, st.ray, st.hit.t);
+        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, w6, st.ray, st.hitT);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
         uint32_t leafOrder = permute_mask(hitSlots & w6.z, st.ray.oct);
         while (leafOrder)
@@ -235,7 +250,7 @@ namespace pt
             const uint32_t slot = i ^ st.ray.oct;
             const uint32_t first = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
             const uint32_t count = __ldg(reinterpret_cast<const unsigned char*>(&nw[6]) + slot);
-            if (!leaf_tests<ANY>(sc, st, first, count, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, first, count, occluded, tests)) return false;
         }
         if (innerSlots)
         {
@@ -373,13 +388,15 @@ namespace pt
     // Traversal stack: STACK entries per thread in shared memory, entry = node << 8 | child mask.
     // BINARY: the binary FP32 BVH with a per-thread stack of kMaxStack entries in local memory (the
     // plain format); otherwise the BVH8 with the shared-memory stack.
+    // Shared memory: [cold slots: 2 x float4 per thread][BVH8 stack: STACK words per thread].
     template <int STACK, bool ANY, int MINB, bool BINARY, class Work>
     __global__ void __launch_bounds__(128, MINB) trace_kernel(Work work, uint32_t refill, uint32_t* errorFlags)
     {
-        extern __shared__ uint32_t smem[];
+        extern __shared__ float4 smem4[];
         uint32_t localStack[BINARY ? kMaxStack : 1];
         uint32_t* stack;
         uint32_t stride;
+        const ColdSlot cold{smem4 + 2u * threadIdx.x};
         if constexpr (BINARY)
         {
             stack = localStack;
@@ -387,7 +404,7 @@ namespace pt
         }
         else
         {
-            stack = smem + threadIdx.x;
+            stack = reinterpret_cast<uint32_t*>(smem4 + 2u * blockDim.x) + threadIdx.x;
             stride = blockDim.x;
         }
         Counters* ctr = work.counters();
@@ -397,7 +414,6 @@ namespace pt
         const uint32_t lane = lane_id();
         const unsigned laneMaskLt = (1u << lane) - 1u;
         TraversalState st;
-        uint32_t index = 0, tag = 0;
         bool active = false;
         bool exhausted = false;
         for (;;)
@@ -416,14 +432,13 @@ namespace pt
                     {
                         float3 o, d;
                         float tmin, tmax;
+                        uint32_t tag;
                         work.load(i, o, d, tmin, tmax, tag);
-                        index = i;
+                        cold.p[0] = make_float4(d.x, d.y, d.z, __uint_as_float(tag));
+                        cold.p[1] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(i));
                         st.ray = make_ray(o, d, tmin);
-                        st.hit.t = tmax;
-                        st.hit.tri = kInvalid;
-                        st.hit.u = 0.0f;
-                        st.hit.v = 0.0f;
-                        st.hit.model = 0;
+                        st.hitT = tmax;
+                        st.hitTri = kInvalid;
                         st.pending = work.root(tag);
                         st.sp = 0;
                         active = true;
@@ -443,13 +458,20 @@ namespace pt
                 for (int k = 0; k < 4 && more; k++)
                 {
                     if constexpr (BINARY)
-                        more = traverse_step_binary<ANY>(work.sc, st, stack, STACK, occluded, errorFlags, visits, tests);
+                        more = traverse_step_binary<ANY>(work.sc, st, cold, stack, STACK, occluded, errorFlags, visits, tests);
                     else
-                        more = traverse_step<ANY>(work.sc, st, stack, stride, STACK, occluded, errorFlags, visits, tests);
+                        more = traverse_step<ANY>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, visits, tests);
                 }
                 if (!more)
                 {
-                    work.finish(index, tag, st.hit, occluded);
+                    const float4 c0 = cold.p[0], c1 = cold.p[1];
+                    HitRecord h;
+                    h.t = st.hitT;
+                    h.tri = st.hitTri;
+                    h.u = c1.x;
+                    h.v = c1.y;
+                    h.model = __float_as_uint(c1.z);
+                    work.finish(__float_as_uint(c1.w), __float_as_uint(c0.w), h, occluded);
                     active = false;
                 }
             }
@@ -1741,13 +1763,15 @@ namespace pt
     // ------------------------------------------------------------------ host launchers
     namespace
     {
+        constexpr size_t kColdBytes = 2 * sizeof(float4);  // shared-memory cold slot per traversal thread
+
         // Traversal kernel variants: stack capacity (>= BVH8 depth) x occupancy target. MINB is the
         // minimum resident 128-thread blocks per SM the compiler must allow (1 = registers unconstrained,
         // 10 = <= 48 registers, 12 = <= 40 registers); the best one is measured, not assumed.
         template <int STACK, bool ANY, int MINB, class Work>
         cudaError_t launch_trace_t(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
         {
-            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
+            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t) + kColdBytes * threads;
             trace_kernel<STACK, ANY, MINB, false, Work><<<blocks, threads, smem, s>>>(w, refill, err);
             return cudaGetLastError();
         }
@@ -1756,7 +1780,7 @@ namespace pt
         template <bool ANY, class Work>
         cudaError_t launch_trace_binary(const Work& w, int blocks, int threads, uint32_t refill, uint32_t* err, cudaStream_t s)
         {
-            trace_kernel<kMaxStack, ANY, 1, true, Work><<<blocks, threads, 0, s>>>(w, refill, err);
+            trace_kernel<kMaxStack, ANY, 1, true, Work><<<blocks, threads, kColdBytes * threads, s>>>(w, refill, err);
             return cudaGetLastError();
         }
 
@@ -1782,7 +1806,7 @@ namespace pt
         int resident_blocks(int threads)
         {
             int perSm = 0;
-            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t);
+            const size_t smem = static_cast<size_t>(STACK) * threads * sizeof(uint32_t) + kColdBytes * threads;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<STACK, false, MINB, false, WavefrontClosest>, threads, smem);
             return perSm;
         }
@@ -1804,7 +1828,8 @@ namespace pt
         if (bvhFormat == kBvh2Fp32)
         {
             perSm = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<kMaxStack, false, 1, true, WavefrontClosest>, threads, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, trace_kernel<kMaxStack, false, 1, true, WavefrontClosest>, threads,
+                                                          kColdBytes * threads);
             return sms * (perSm < 1 ? 1 : perSm);
         }
         if (depth <= 8) perSm = resident_blocks_m<8>(occupancy, threads);

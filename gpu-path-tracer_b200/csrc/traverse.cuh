@@ -6,9 +6,11 @@
 
 namespace pt
 {
+    // Per-ray values the node tests need (the direction itself is only needed by triangle tests,
+    // which take it separately).
     struct RayPre
     {
-        float3 o, d, invd;
+        float3 o, invd;
         float tmin;
         uint32_t oct;   // bit k set when the ray's k-th direction component is negative
     };
@@ -24,7 +26,6 @@ namespace pt
     {
         RayPre r;
         r.o = o;
-        r.d = d;
         r.tmin = tmin;
         r.invd = make_float3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
         r.oct = (r.invd.x < 0.0f ? 1u : 0u) | (r.invd.y < 0.0f ? 2u : 0u) | (r.invd.z < 0.0f ? 4u : 0u);
@@ -104,20 +105,20 @@ namespace pt
     // Moller-Trumbore with the reference's determinant cull and inclusive edges
     // (Intersect.cu:25-61), one IEEE rounding per operator. Returns false on a miss;
     // on a barycentric hit returns true with t, u, v (the caller applies the t range).
-    PT_HD bool intersect_triangle(float4 a, float4 b, float4 c, const RayPre& r, float& t, float& u, float& v)
+    PT_HD bool intersect_triangle(float4 a, float4 b, float4 c, float3 o, float3 d, float& t, float& u, float& v)
     {
         const float3 v0 = make_float3(a.x, a.y, a.z);
         const float3 e1 = make_float3(b.x, b.y, b.z);
         const float3 e2 = make_float3(c.x, c.y, c.z);
-        const float3 p = cross(r.d, e2);
+        const float3 p = cross(d, e2);
         const float det = dot(e1, p);
         if (fabsf(det) < 1e-7f) return false;
         const float invDet = 1.0f / det;
-        const float3 s = r.o - v0;
+        const float3 s = o - v0;
         u = dot(s, p) * invDet;
         if (u < 0.0f || u > 1.0f) return false;
         const float3 q = cross(s, e1);
-        v = dot(r.d, q) * invDet;
+        v = dot(d, q) * invDet;
         if (v < 0.0f || u + v > 1.0f) return false;
         t = dot(e2, q) * invDet;
         return true;
@@ -133,8 +134,8 @@ namespace pt
 
     // Closest-hit acceptance with the deterministic tie rule: the smaller input index wins
     // at a bit-identical t.
-    PT_HD bool better_hit(float t, uint32_t orig, float tmin, const HitRecord& h)
+    PT_HD bool better_hit(float t, uint32_t orig, float tmin, float bestT, uint32_t bestTri)
     {
-        return t >= tmin && (t < h.t || (t == h.t && h.tri != kInvalid && orig < h.tri));
+        return t >= tmin && (t < bestT || (t == bestT && bestTri != kInvalid && orig < bestTri));
     }
 }
