@@ -304,7 +304,7 @@ namespace pt
                     if (c.leaf())
                     {
                         if (c.count > 255) throw std::runtime_error("BVH leaf larger than 255 triangles");
-                        childRef[s] = c.first;
+                        childRef[s] = c.first | (c.count << 24);  // first triangle (24 bits), count (8 bits)
                         counts[s] = static_cast<uint8_t>(c.count);
                         leafMask |= static_cast<uint8_t>(1u << s);
                     }
@@ -493,6 +493,7 @@ namespace pt
     Bvh8 BuildBvh8(const float* positions, const uint32_t* models, uint32_t n, int threads, bool withBinary)
     {
         if (n == 0) throw std::runtime_error("scene has no triangles");
+        if (n > kMaxTriangles) throw std::runtime_error("scene has more than 2^24 triangles");
         BinaryBuilder b;
         b.pos = positions;
         b.n = n;
@@ -589,9 +590,10 @@ namespace pt
                         clo[k] = DBL_MAX;
                         chi[k] = -DBL_MAX;
                     }
+                    if ((child[s] >> 24) != counts[s]) cs.violations++;
                     for (uint32_t j = 0; j < counts[s]; j++)
                     {
-                        const uint32_t t = cs.b.order[child[s] + j];
+                        const uint32_t t = cs.b.order[(child[s] & 0xFFFFFFu) + j];
                         cs.seen[t]++;
                         cs.leafTriangles++;
                         for (int v = 0; v < 3; v++)

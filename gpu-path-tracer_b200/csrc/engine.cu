@@ -135,8 +135,8 @@ namespace pt
             if (p.entry.size() >= kMaxScenes) return Status::Err(GPT_ERR_CAPACITY, "At most 256 resident scenes");
             if (static_cast<uint64_t>(p.nodeCount) + s.nodeCount >= (1ull << 24))
                 return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^24 BVH8 nodes");
-            if (static_cast<uint64_t>(p.triangleCount) + s.triangleCount >= 0xFFFFFFFFull)
-                return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^32-1 triangles");
+            if (static_cast<uint64_t>(p.triangleCount) + s.triangleCount > kMaxTriangles)
+                return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^24 triangles");
             DeviceBuffer nn, nt, ns, nm, nl, nb, ntex, ne;
             PT_TRY(Grow(nn, p.nodes, size_t(p.nodeCount) * sizeof(Node8), s.nodes, size_t(s.nodeCount) * sizeof(Node8), st));
             PT_TRY(Grow(nt, p.tris, size_t(p.triangleCount) * 48, s.tris, size_t(s.triangleCount) * 48, st));

@@ -239,18 +239,17 @@ namespace pt
         }
         const uint4* nw = sc.nodes[node].w;
         visits++;
-        const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3), w6 = ldg4(nw + 6);
-        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, w6, st.ray, st.hitT);
+        const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
+        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, st.ray, st.hitT);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
-        uint32_t leafOrder = permute_mask(hitSlots & w6.z, st.ray.oct);
+        uint32_t leafOrder = permute_mask(hitSlots & ~(w0.w >> 24), st.ray.oct);
         while (leafOrder)
         {
             const uint32_t i = static_cast<uint32_t>(__ffs(leafOrder) - 1);
             leafOrder &= leafOrder - 1u;
             const uint32_t slot = i ^ st.ray.oct;
-            const uint32_t first = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
-            const uint32_t count = __ldg(reinterpret_cast<const unsigned char*>(&nw[6]) + slot);
-            if (!leaf_tests<ANY>(sc, st, cold, first, count, occluded, tests)) return false;
+            const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
+            if (!leaf_tests<ANY>(sc, st, cold, ref & 0xFFFFFFu, ref >> 24, occluded, tests)) return false;
         }
         if (innerSlots)
         {

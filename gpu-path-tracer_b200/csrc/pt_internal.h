@@ -33,6 +33,7 @@ namespace pt
     constexpr uint32_t kSlotMask = (1u << kSlotBits) - 1u;
     constexpr uint32_t kMaxPool = 1u << kSlotBits;
     constexpr uint32_t kMaxScenes = 256;
+    constexpr uint32_t kMaxTriangles = 1u << 24;  // leaf references hold 24-bit triangle positions
     constexpr uint32_t kMaxJobs = 65536;
     constexpr uint32_t kMaxRing = 256;
 
@@ -41,9 +42,12 @@ namespace pt
     //  w[1] = qlo.x[0..7] (x,y words), qlo.y[0..7] (z,w words)
     //  w[2] = qlo.z[0..7], qhi.x[0..7]
     //  w[3] = qhi.y[0..7], qhi.z[0..7]
-    //  w[4], w[5] = child[0..7]: internal -> node index, leaf -> first triangle (leaf order)
-    //  w[6] = count[0..7] (bytes, leaf triangle counts), leafMask, 0
+    //  w[4], w[5] = child[0..7]: internal -> node index, leaf -> first triangle (leaf order, bits 0-23)
+    //               | triangle count << 24
+    //  w[6] = count[0..7] (bytes, leaf triangle counts), leafMask, 0   (builder and checker only)
     //  w[7] = reserved
+    // Empty slots hold inverted boxes (lo 255, hi 0) and child reference 0. A node visit reads w[0..3]
+    // (64 bytes); a leaf or a pop reads one child reference.
     // Child slots are assigned by octant, so that visiting slot (i ^ rayOctant) for i = 0..7
     // is an approximate front-to-back order.
     struct __align__(16) Node8

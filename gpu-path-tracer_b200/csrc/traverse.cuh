@@ -59,8 +59,9 @@ namespace pt
     // Slab test of the 8 quantised children against [tmin, tmax]. The computed entry
     // distance is lowered and the exit distance raised by 2^-20 of the node's scale in ray
     // space, so the test is conservative for every child box (a box the exact arithmetic
-    // would hit is never culled). Returns the hit mask in slot order.
-    PT_HD uint32_t intersect_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, uint4 w6, const RayPre& r, float tmax)
+    // would hit is never culled). Returns the hit mask in slot order. Empty slots hold inverted
+    // boxes and are almost always culled; one that passes has a zero child reference (no work).
+    PT_HD uint32_t intersect_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, const RayPre& r, float tmax)
     {
         const float px = as_float(w0.x), py = as_float(w0.y), pz = as_float(w0.z);
         const float sx = as_float((w0.w & 0xFFu) << 23);
@@ -98,8 +99,7 @@ namespace pt
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
             hit |= (tn <= tf ? 1u : 0u) << s;
         }
-        const uint32_t valid = (w0.w >> 24) | (w6.z & 0xFFu);
-        return hit & valid;
+        return hit;
     }
 
     // Moller-Trumbore with the reference's determinant cull and inclusive edges

@@ -87,7 +87,7 @@ enum gpt_texture_slot {
  * vertex data, already transformed. All pointers are host memory.
  */
 typedef struct gpt_scene_desc {
-    uint32_t triangle_count;
+    uint32_t triangle_count;       /* at most 2^24 (16,777,216) */
     const float* positions;       /* [T][3][3] world positions */
     const float* normals;         /* [T][3][3] world normals */
     const float* tangents;        /* [T][3][4] world tangent xyz + handedness sign */
