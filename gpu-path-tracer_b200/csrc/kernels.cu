@@ -1866,10 +1866,28 @@ namespace pt
             e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
         if (L.traceStop && (e = cudaEventRecord(L.traceStop, s)) != cudaSuccess) return e;
-        for (uint32_t m = 0; m < kModelCount; m++)
+        uint32_t models = 0;
+        for (uint32_t m = 0; m < kModelCount; m++) models += L.modelPresent[m] ? 1u : 0u;
+        if (L.shadeFork && models > 1)
         {
-            if (!L.modelPresent[m]) continue;
-            if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
+            // the per-model shading kernels touch disjoint queue entries and push with atomics: run them side by side
+            if ((e = cudaEventRecord(L.shadeFork, s)) != cudaSuccess) return e;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                if (!L.modelPresent[m]) continue;
+                if ((e = cudaStreamWaitEvent(L.shadeStreams[m], L.shadeFork, 0)) != cudaSuccess) return e;
+                if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, L.shadeStreams[m])) != cudaSuccess) return e;
+                if ((e = cudaEventRecord(L.shadeJoin[m], L.shadeStreams[m])) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(s, L.shadeJoin[m], 0)) != cudaSuccess) return e;
+            }
+        }
+        else
+        {
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                if (!L.modelPresent[m]) continue;
+                if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
+            }
         }
         if (L.nee && L.scene.lightCount > 0)
         {

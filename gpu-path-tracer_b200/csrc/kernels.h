@@ -24,6 +24,11 @@ namespace pt
         uint32_t bvhFormat;        // kBvh8Quantised or kBvh2Fp32 (scene.nodes2 must be present)
         cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
         cudaEvent_t traceStop;
+        // Optional fork/join: the shading kernels of the models present run on their own streams,
+        // concurrently (parallel branches when captured into the frame graph). nullptr = in order.
+        cudaEvent_t shadeFork;
+        cudaEvent_t shadeJoin[kModelCount];
+        cudaStream_t shadeStreams[kModelCount];
     };
 
     // One iteration of the job engine over all resident scenes and active jobs.

@@ -268,6 +268,12 @@ namespace pt
             if (traceStop_) cudaEventDestroy(traceStop_);
             if (stopEvent_) cudaEventDestroy(stopEvent_);
             if (hostMapped_) cudaFreeHost(hostMapped_);
+            if (shadeFork_) cudaEventDestroy(shadeFork_);
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                if (shadeJoin_[m]) cudaEventDestroy(shadeJoin_[m]);
+                if (shadeStreams_[m]) cudaStreamDestroy(shadeStreams_[m]);
+            }
             if (stream_) cudaStreamDestroy(stream_);
         }
 
@@ -275,6 +281,12 @@ namespace pt
         {
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+            PT_CUDA("cudaEventCreateWithFlags", cudaEventCreateWithFlags(&shadeFork_, cudaEventDisableTiming));
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&shadeStreams_[m], cudaStreamNonBlocking));
+                PT_CUDA("cudaEventCreateWithFlags", cudaEventCreateWithFlags(&shadeJoin_[m], cudaEventDisableTiming));
+            }
             PT_CUDA("cudaEventCreate", cudaEventCreate(&startEvent_));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&stopEvent_));
             PT_CUDA("cudaHostAlloc", cudaHostAlloc(&hostMapped_, 64, cudaHostAllocMapped));
@@ -466,6 +478,12 @@ namespace pt
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
             L.bvhFormat = c.bvh;
+            L.shadeFork = shadeFork_;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                L.shadeJoin[m] = shadeJoin_[m];
+                L.shadeStreams[m] = shadeStreams_[m];
+            }
             L.shadeBlocks = sms * 8;
             L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -507,6 +525,12 @@ namespace pt
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
             L.bvhFormat = c.bvh;
+            L.shadeFork = shadeFork_;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                L.shadeJoin[m] = shadeJoin_[m];
+                L.shadeStreams[m] = shadeStreams_[m];
+            }
             L.shadeBlocks = sms * 8;
             L.graphLoop = false;
             L.traceStart = traceStart_;
@@ -840,6 +864,9 @@ namespace pt
         cudaStream_t stream_ = nullptr;
         cudaEvent_t startEvent_ = nullptr, stopEvent_ = nullptr;
         cudaEvent_t traceStart_ = nullptr, traceStop_ = nullptr;
+        cudaEvent_t shadeFork_ = nullptr;
+        cudaEvent_t shadeJoin_[kModelCount] = {};
+        cudaStream_t shadeStreams_[kModelCount] = {};
         void* hostMapped_ = nullptr;
         void* hostMappedDev_ = nullptr;
         static constexpr uint32_t kDefaultPool = 1u << 20;
