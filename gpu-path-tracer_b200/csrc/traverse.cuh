@@ -113,9 +113,14 @@ namespace pt
         const float3 p = cross(d, e2);
         const float det = dot(e1, p);
         if (fabsf(det) < 1e-7f) return false;
-        const float invDet = 1.0f / det;
         const float3 s = o - v0;
-        u = dot(s, p) * invDet;
+        const float sp = dot(s, p);
+        // u = sp * (1/det) is negative when sp and det have opposite signs and the product does not
+        // round to zero; with |sp| > 1e-20 and |det| < 1e20 its magnitude exceeds 1e-40, so the
+        // reference's u < 0 rejection is decided here without the division (same outcome, bit for bit).
+        if (fabsf(sp) > 1e-20f && fabsf(det) < 1e20f && (sp < 0.0f) != (det < 0.0f)) return false;
+        const float invDet = 1.0f / det;
+        u = sp * invDet;
         if (u < 0.0f || u > 1.0f) return false;
         const float3 q = cross(s, e1);
         v = dot(d, q) * invDet;
