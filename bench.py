@@ -233,20 +233,23 @@ def traversal_summary(st, node_bytes):
 
 
 def plain_form(renderer, cam, W, H, spp, depth, frames=2):
-    """The plain single-job FP32 wavefront form of a frame: binary FP32 BVH (64-B nodes, local-memory
-    stack), warps refilled only when all 32 lanes are idle, host-driven iteration loop with a flag
-    read per iteration, 1,048,576 path slots (the reference's pool), no autotuning. Same images bit
-    for bit as the optimised form."""
+    """The plain single-job FP32 wavefront form of a frame: the reference's wavefront structure on this
+    project's kernels. Binary FP32 BVH (64-B nodes, local-memory stack), warps refilled only when all
+    32 lanes are idle, finished paths regenerated from a queue in finishing order, shading kernels one
+    after another, host-driven iteration loop with a flag read per iteration, 1,048,576 path slots (the
+    reference's pool), no autotuning. Same images bit for bit as the optimised form."""
     import pathtracer
     settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
-                    loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32)
+                    loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32,
+                    wavefront_layout=pathtracer.WAVEFRONT_QUEUES)
     renderer.render_frame(cam, W, H, spp, depth, True, **settings)
     stats = [renderer.render_frame(cam, W, H, spp, depth, True, **settings) for _ in range(frames)]
     ms = sum(s["device_ms"] for s in stats) / frames
     return {"value": stats[0]["samples"] / (ms / 1000.0), "unit": "paths/s", "ms_per_frame": ms,
             "iterations": stats[0]["iterations"], "settings": {k: v for k, v in settings.items()},
             "traversal": traversal_summary(stats[-1], pathtracer.NODE_BYTES[pathtracer.BVH2_FP32]),
-            "what": "binary FP32 BVH, warps refilled only when all lanes are idle, host-driven loop, 1,048,576 slots, no autotune"}
+            "what": "binary FP32 BVH, warps refilled only when all lanes are idle, regeneration queue, shading in sequence, "
+                    "host-driven loop, 1,048,576 slots, no autotune"}
 
 
 def cornell_section(knobs):
@@ -335,7 +338,8 @@ def batched_section(knobs):
             renderers[n] = pathtracer.Renderer(0)
             renderers[n].upload_scene(s)
         plain_settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
-                              loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32)
+                              loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32,
+                              wavefront_layout=pathtracer.WAVEFRONT_QUEUES)
         for mode, settings in (("frames_one_at_a_time", dict(knobs)), ("plain_form_one_at_a_time", plain_settings)):
             for j in warm:
                 renderers[j.scene].render_frame(j.camera, j.width, j.height, j.spp, j.depth, True, **settings)

@@ -264,6 +264,22 @@ namespace pt
         return true;
     }
 
+    // A path left its slot: counted for the iteration and recorded for regeneration, in the finished-slot
+    // bitmap (frame renderer) or the regeneration queue (job engine).
+    __device__ __forceinline__ void path_finished(const Wavefront& wf, Counters* ctr, uint32_t slot)
+    {
+        if (wf.regenBits != nullptr)
+        {
+            agg_push(&ctr->regenCount);
+            atomicOr(&wf.regenBits[slot >> 5], 1u << (slot & 31u));
+        }
+        else
+        {
+            const uint32_t pos = agg_push(&ctr->regenCount);
+            wf.regen[pos] = slot;
+        }
+    }
+
     // Work sources of the persistent traversal kernel.
     struct WavefrontClosest
     {
@@ -295,8 +311,7 @@ namespace pt
             }
             else
             {
-                const uint32_t pos = agg_push(&wf.ctr->regenCount);
-                wf.regen[pos] = slot & kSlotMask;
+                path_finished(wf, wf.ctr, slot & kSlotMask);
             }
         }
     };
@@ -551,6 +566,7 @@ namespace pt
         c->regenCount = 0;
         c->traceCursor = 0;
         c->shadowCursor = 0;
+        c->regenCursor = 0;
         c->iteration = 0;
         c->done = gen == 0 ? 1u : 0u;
         c->errorFlags = 0;
@@ -576,6 +592,67 @@ namespace pt
         const uint32_t n = wf.ctr->rayCount[0];
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
             start_path(job, 0, wf, i, i, 0, i);
+        if (wf.regenBits != nullptr)
+            for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (wf.capacity + 31u) >> 5; i += gridDim.x * blockDim.x)
+                wf.regenBits[i] = 0u;
+    }
+
+    // Regeneration from the finished-slot bitmap: each warp takes a tile of 32 bitmap words (1,024
+    // slots), reserves new samples for the tile's finished paths with one atomic, and walks the words in
+    // slot order, so the slot records of finished and new paths are read and written in address order
+    // (the queue holds them in the order paths finished, i.e. scattered). The set of new samples, their
+    // ray-queue positions and every sample's result are those of the queue-driven regeneration; only
+    // which slot a new sample lands in differs.
+    __global__ void regen_bits_kernel(Wavefront wf, const JobView* jobPtr)
+    {
+        Counters* ctr = wf.ctr;
+        phase_begin(ctr, 3);
+        const unsigned long long launched = ctr->launched;
+        const unsigned long long remaining = jobPtr->totalSamples - launched;
+        const uint32_t regenerate = static_cast<uint32_t>(remaining < ctr->regenCount ? remaining : ctr->regenCount);
+        const uint32_t nxt = ctr->cur ^ 1u;
+        const uint32_t base = ctr->rayCount[nxt];
+        float* out = jobPtr->sampleRadiance;
+        const uint32_t words = (wf.capacity + 31u) >> 5;
+        const uint32_t tiles = (words + 31u) >> 5;
+        const uint32_t lane = lane_id();
+        const uint32_t lanesBelow = (1u << lane) - 1u;
+        const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps)
+        {
+            const uint32_t wi = tile * 32u + lane;
+            const uint32_t bits = wi < words ? wf.regenBits[wi] : 0u;
+            if (bits) wf.regenBits[wi] = 0u;
+            const uint32_t count = static_cast<uint32_t>(__popc(bits));
+            uint32_t incl = count;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (static_cast<int>(lane) >= o) incl += v;
+            }
+            const uint32_t tileTotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            if (tileTotal == 0) continue;
+            uint32_t first = 0;
+            if (lane == 0) first = atomicAdd(&ctr->regenCursor, tileTotal);
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            const uint32_t excl = incl - count;
+            for (uint32_t j = 0; j < 32; j++)
+            {
+                const uint32_t w = __shfl_sync(0xFFFFFFFFu, bits, j);
+                const uint32_t offset = __shfl_sync(0xFFFFFFFFu, excl, j);
+                if (!((w >> lane) & 1u)) continue;
+                const uint32_t slot = (tile * 32u + j) * 32u + lane;
+                const float4 L = wf.slotL[slot];
+                const uint32_t sample = wf.slotSample[slot];
+                float* dst = out + static_cast<size_t>(sample) * 3;
+                dst[0] = L.x;
+                dst[1] = L.y;
+                dst[2] = L.z;
+                const uint32_t k = first + offset + static_cast<uint32_t>(__popc(w & lanesBelow));
+                if (k < regenerate) start_path(*jobPtr, 0, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
+            }
+        }
+        phase_end(ctr, 3);
     }
 
     // ------------------------------------------------------------------ shading (MaterialEval.cu)
@@ -1166,11 +1243,7 @@ namespace pt
                 wf.shD[pos] = make_float4(sh.direction.x, sh.direction.y, sh.direction.z, sh.tMax);
                 wf.shL[pos] = make_float4(sh.radiance.x, sh.radiance.y, sh.radiance.z, 0.0f);
             }
-            if (terminated)
-            {
-                const uint32_t pos = agg_push(&ctr->regenCount);
-                wf.regen[pos] = slot;
-            }
+            if (terminated) path_finished(wf, ctr, slot);
             else
             {
                 // SpawnScatteredRay (:148-156)
@@ -1249,6 +1322,7 @@ namespace pt
         c->regenCount = 0;
         c->traceCursor = 0;
         c->shadowCursor = 0;
+        c->regenCursor = 0;
         c->iteration += 1;
         const bool cancelled = wf.cancel != nullptr && *wf.cancel != 0u;
         // Every path ends within depthLimit iterations, so the frame needs at most
@@ -1898,7 +1972,10 @@ namespace pt
                 e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
-        regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
+        if (L.wf.regenBits != nullptr)
+            regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
+        else
+            regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         advance_kernel<<<1, 1, 0, s>>>(L.wf, L.job, L.handle, L.graphLoop);
         return cudaGetLastError();

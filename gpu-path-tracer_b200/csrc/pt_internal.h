@@ -196,6 +196,7 @@ namespace pt
         uint32_t regenCount;
         uint32_t traceCursor;
         uint32_t shadowCursor;
+        uint32_t regenCursor;     // new samples handed out by the bitmap regeneration of the iteration
         uint32_t iteration;
         uint32_t done;
         uint32_t errorFlags;
@@ -223,6 +224,7 @@ namespace pt
         float4* shD;
         float4* shL;
         uint32_t* regen;
+        uint32_t* regenBits;      // frame renderer: bit per slot set when its path finished (nullptr: regen queue)
         float4* slotT;            // throughput xyz, w = bits(depth | delta << 8)
         float4* slotL;            // radiance xyz, w = bits(rng stream position)
         uint32_t* slotSample;

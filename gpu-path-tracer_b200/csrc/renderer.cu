@@ -340,6 +340,8 @@ namespace pt
             PT_TRY(shD_.allocate(P * 16));
             PT_TRY(shL_.allocate(P * 16));
             PT_TRY(regen_.allocate(P * 4));
+            PT_TRY(regenBits_.allocate((P + 31) / 32 * 4));
+            PT_CUDA("cudaMemsetAsync", cudaMemsetAsync(regenBits_.get<void>(), 0, (P + 31) / 32 * 4, stream_));
             PT_TRY(slotT_.allocate(P * 16));
             PT_TRY(slotL_.allocate(P * 16));
             PT_TRY(slotSample_.allocate(P * 4));
@@ -348,7 +350,7 @@ namespace pt
             return Status::Ok();
         }
 
-        Wavefront wavefront() const
+        Wavefront wavefront(bool queues = false) const
         {
             Wavefront w{};
             for (int q = 0; q < 2; q++)
@@ -362,6 +364,7 @@ namespace pt
             w.shD = shD_.get<float4>();
             w.shL = shL_.get<float4>();
             w.regen = regen_.get<uint32_t>();
+            w.regenBits = queues ? nullptr : regenBits_.get<uint32_t>();
             w.slotT = slotT_.get<float4>();
             w.slotL = slotL_.get<float4>();
             w.slotSample = slotSample_.get<uint32_t>();
@@ -396,6 +399,7 @@ namespace pt
             uint32_t refill;
             int occupancy;
             uint32_t bvh;
+            bool queues;   // the reference's wavefront structure (regeneration queue, shading in sequence)
         };
 
         Status resolveConfig(const gpt_render_settings& s, FrameConfig& c) const
@@ -421,6 +425,8 @@ namespace pt
             c.bvh = s.bvh_format == GPT_BVH2_FP32 ? kBvh2Fp32 : kBvh8Quantised;
             if (c.bvh == kBvh2Fp32 && !scene_->nodeCount2)
                 return Status::Err(GPT_ERR_STATE, "The scene has no binary BVH");
+            if (s.wavefront_layout > GPT_WAVEFRONT_QUEUES) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown wavefront layout");
+            c.queues = s.wavefront_layout == GPT_WAVEFRONT_QUEUES;
             return Status::Ok();
         }
 
@@ -438,7 +444,7 @@ namespace pt
             int sms = 0;
             PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
             const SceneView sv = scene_->view();
-            const Wavefront wf = wavefront();
+            const Wavefront wf = wavefront(c.queues);
             const JobView* jobDev = job_.get<JobView>();
             // prologue and resolve as captured child graphs
             cudaGraph_t pro = nullptr, res = nullptr;
@@ -478,7 +484,7 @@ namespace pt
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
             L.bvhFormat = c.bvh;
-            L.shadeFork = shadeFork_;
+            L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
             {
                 L.shadeJoin[m] = shadeJoin_[m];
@@ -508,7 +514,7 @@ namespace pt
             int sms = 0;
             PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
             const SceneView sv = scene_->view();
-            const Wavefront wf = wavefront();
+            const Wavefront wf = wavefront(c.queues);
             const JobView* jobDev = job_.get<JobView>();
             if (!traceStart_) PT_CUDA("cudaEventCreate", cudaEventCreate(&traceStart_));
             if (!traceStop_) PT_CUDA("cudaEventCreate", cudaEventCreate(&traceStop_));
@@ -525,7 +531,7 @@ namespace pt
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
             L.bvhFormat = c.bvh;
-            L.shadeFork = shadeFork_;
+            L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
             {
                 L.shadeJoin[m] = shadeJoin_[m];
@@ -557,8 +563,9 @@ namespace pt
         std::string key(const FrameConfig& c) const
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
-                          c.nee, c.traceThreads, c.refill, c.occupancy, c.bvh, width_, height_, static_cast<void*>(accumulation_.get<void>()),
+            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%d/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
+                          c.nee, c.traceThreads, c.refill, c.occupancy, c.bvh, c.queues ? 1 : 0, width_, height_,
+                          static_cast<void*>(accumulation_.get<void>()),
                           static_cast<void*>(framebuffer_.get<void>()));
             return buf;
         }
@@ -872,7 +879,7 @@ namespace pt
         static constexpr uint32_t kDefaultPool = 1u << 20;
         static constexpr uint32_t kLogCapacity = 1u << 16;
         uint32_t pool_ = 0;
-        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regen_, slotT_, slotL_, slotSample_, queueLog_;
+        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regen_, regenBits_, slotT_, slotL_, slotSample_, queueLog_;
         DeviceBuffer counters_, job_, cursor_, accumulation_, framebuffer_, sampleRadiance_;
         JobView hostJob_{};
         Counters hostCounters_{};

@@ -62,10 +62,11 @@ class gpt_render_settings(ctypes.Structure):
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
                 ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
-                ("bvh_format", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("bvh_format", ctypes.c_uint32), ("wavefront_layout", ctypes.c_uint32)]
 
 LOOP_GRAPH, LOOP_HOST = 0, 1
 BVH8_Q8, BVH2_FP32 = 0, 1
+WAVEFRONT_B200, WAVEFRONT_QUEUES = 0, 1
 SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST = 1, 2
 NODE_BYTES = {BVH8_Q8: 128, BVH2_FP32: 64}
 
@@ -284,10 +285,10 @@ class Renderer:
     def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
                      rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0,
-                     bvh_format: int = BVH8_Q8) -> dict:
+                     bvh_format: int = BVH8_Q8, wavefront_layout: int = WAVEFRONT_B200) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
-                                 trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, 0)
+                                 trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, wavefront_layout)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")

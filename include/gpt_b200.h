@@ -134,13 +134,19 @@ typedef struct gpt_render_settings {
     uint32_t bvh_format;          /* GPT_BVH8_Q8 (default): 8-wide BVH, 8-bit quantised child boxes, 128-B nodes;
                                      GPT_BVH2_FP32: the binary BVH it is collapsed from, FP32 child boxes, 64-B nodes,
                                      local-memory stack (the plain format; same hits, bit for bit) */
-    uint32_t reserved;
+    uint32_t wavefront_layout;    /* GPT_WAVEFRONT_B200 (default): finished slots are regenerated from a bitmap in
+                                     slot order and the per-model shading kernels run side by side;
+                                     GPT_WAVEFRONT_QUEUES: the reference's structure, a queue of finished slots in the
+                                     order paths ended (RegenQueue, PathGeneration.cu:74-102) and the shading kernels
+                                     one after another (Renderer.cpp:540-566). Same results, bit for bit. */
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
 #define GPT_LOOP_HOST 1u
 #define GPT_BVH8_Q8 0u
 #define GPT_BVH2_FP32 1u
+#define GPT_WAVEFRONT_B200 0u
+#define GPT_WAVEFRONT_QUEUES 1u
 
 typedef struct gpt_frame_stats {
     uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */

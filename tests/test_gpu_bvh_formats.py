@@ -58,9 +58,10 @@ def test_binary_bvh_frames_bit_identical(gpu_renderer, scene_factory, oracle_sce
     cam = scenes.scene_camera(s, w, h)
     a = gpu_renderer.render_frame(cam, w, h, spp, depth, True, pool_size=5000, bvh_format=P.BVH8_Q8)
     rad_a, log_a, fb_a = gpu_renderer.sample_radiance(), gpu_renderer.queue_log(), gpu_renderer.framebuffer()
-    # the plain configuration: binary FP32 BVH, warps refilled only when all lanes are idle, host loop
+    # the plain configuration: binary FP32 BVH, warps refilled only when all lanes are idle, the
+    # reference's queue structure (regeneration queue, shading in sequence), host loop
     b = gpu_renderer.render_frame(cam, w, h, spp, depth, True, pool_size=5000, bvh_format=P.BVH2_FP32,
-                                  trace_refill=32, loop_mode=loop)
+                                  trace_refill=32, loop_mode=loop, wavefront_layout=P.WAVEFRONT_QUEUES)
     rad_b, log_b, fb_b = gpu_renderer.sample_radiance(), gpu_renderer.queue_log(), gpu_renderer.framebuffer()
     assert a["iterations"] == b["iterations"]
     assert np.array_equal(log_a, log_b)
@@ -80,3 +81,23 @@ def test_binary_bvh_unknown_format_is_rejected(gpu_renderer, scene_factory):
         gpu_renderer.render_frame(cam, 8, 8, 1, 2, True, bvh_format=7)
     assert e.value.code == 1
 
+
+
+@pytest.mark.parametrize("loop", [P.LOOP_GRAPH, P.LOOP_HOST])
+def test_wavefront_layouts_bit_identical(gpu_renderer, scene_factory, loop):
+    """Bitmap regeneration in slot order with concurrent shading (GPT_WAVEFRONT_B200) and the
+    reference's queue structure (GPT_WAVEFRONT_QUEUES) hand out the same samples per iteration:
+    identical queue sizes, iteration counts and per-sample radiance, with a pool far smaller than
+    the frame so that slots are reused many times."""
+    s = scene_factory("cornell-all")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 80, 60)
+    a = gpu_renderer.render_frame(cam, 80, 60, 16, 10, True, pool_size=3000, loop_mode=loop, wavefront_layout=P.WAVEFRONT_B200)
+    rad_a, log_a = gpu_renderer.sample_radiance(), gpu_renderer.queue_log()
+    b = gpu_renderer.render_frame(cam, 80, 60, 16, 10, True, pool_size=3000, loop_mode=loop, wavefront_layout=P.WAVEFRONT_QUEUES)
+    rad_b, log_b = gpu_renderer.sample_radiance(), gpu_renderer.queue_log()
+    assert a["iterations"] == b["iterations"] > 10
+    assert np.array_equal(log_a, log_b)
+    assert np.array_equal(rad_a.view(np.uint32), rad_b.view(np.uint32))
+    with pytest.raises(P.GptError):
+        gpu_renderer.render_frame(cam, 8, 8, 1, 2, True, wavefront_layout=2)
