@@ -71,6 +71,8 @@ def parse():
     ap.add_argument("--sections", default="all",
                     help="comma list of extra one-GPU sections: plain,cornell,batched,serving,precision (all/none)")
     ap.add_argument("--serve-jobs", type=int, default=48, help="jobs per arrival rate in the serving section")
+    ap.add_argument("--no-reference-build", action="store_true",
+                    help="skip timing the reference's own kernels (oracle/_ref) on the same frame")
     ap.add_argument("--serve-rates", default="20,50,100", help="Poisson arrival rates (jobs/s) of the serving section")
     return ap.parse_args()
 
@@ -583,7 +585,7 @@ def b200_arm(args):
     }
     if clocks:
         line["clocks"] = clocks
-    if world == 1 and not args.profile_case:
+    if world == 1 and not args.profile_case and not args.no_reference_build:
         try:
             import ref_harness
         except ImportError:

@@ -1463,6 +1463,96 @@ namespace pt
         e->segmentCount = segments;
     }
 
+    // A finished path writes its radiance into its job's pass ring and counts towards the pass.
+    __device__ __forceinline__ void engine_retire_path(const Wavefront& wf, const EngineView& ev, uint32_t slot)
+    {
+        const uint32_t j = __float_as_uint(wf.slotT[slot].w) >> 16;
+        JobView& J = ev.jobs[j];
+        const uint32_t sample = wf.slotSample[slot];
+        const uint32_t pixel = sample / J.spp;
+        const uint32_t pass = sample - pixel * J.spp;
+        const uint32_t r = pass % J.ring;
+        const float4 L = wf.slotL[slot];
+        float* dst = J.sampleRadiance + (static_cast<size_t>(r) * J.pixels + pixel) * 3;
+        dst[0] = L.x;
+        dst[1] = L.y;
+        dst[2] = L.z;
+        agg_increment_keyed(&J.passDone[r], (j << 8) | r);
+    }
+
+    // Planned launch k of the iteration starts in `slot` (the plan's segments map k to a job and launch index).
+    __device__ __forceinline__ void engine_start_launch(const Wavefront& wf, const EngineView& ev, uint32_t k, uint32_t slot,
+                                                        uint32_t segmentCount, uint32_t nxt, uint32_t base)
+    {
+        uint32_t lo = 0, hi = segmentCount - 1u;
+        while (lo < hi)
+        {
+            const uint32_t mid = (lo + hi + 1u) >> 1;
+            if (ev.segments[mid].start <= k) lo = mid;
+            else hi = mid - 1u;
+        }
+        const LaunchSegment sg = ev.segments[lo];
+        const JobView& J = ev.jobs[sg.job];
+        const uint64_t g = sg.first + (k - sg.start);
+        const uint32_t pass = static_cast<uint32_t>(g / J.pixels);
+        const uint32_t pixel = static_cast<uint32_t>(g - static_cast<uint64_t>(pass) * J.pixels);
+        start_path(J, sg.job, wf, slot, pixel * J.spp + pass, nxt, base + k);
+    }
+
+    // Job-engine regeneration from the finished-slot bitmap (same tiling as regen_bits_kernel): the
+    // finished slot of rank k takes planned launch k, or goes onto the free list when k >= the plan;
+    // launches beyond the finished slots take slots from the free list.
+    __global__ void engine_regen_bits_kernel(Wavefront wf, EngineView ev)
+    {
+        Counters* ctr = wf.ctr;
+        phase_begin(ctr, 3);
+        const uint32_t n = ctr->regenCount;
+        const EngineCtl* e = ev.ctl;
+        const uint32_t launch = e->launchCount;
+        const uint32_t freeCount = e->freeCount;
+        const uint32_t segmentCount = e->segmentCount;
+        const uint32_t nxt = ctr->cur ^ 1u;
+        const uint32_t base = ctr->rayCount[nxt];
+        const uint32_t words = (wf.capacity + 31u) >> 5;
+        const uint32_t tiles = (words + 31u) >> 5;
+        const uint32_t lane = lane_id();
+        const uint32_t lanesBelow = (1u << lane) - 1u;
+        const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+        for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps)
+        {
+            const uint32_t wi = tile * 32u + lane;
+            const uint32_t bits = wi < words ? wf.regenBits[wi] : 0u;
+            if (bits) wf.regenBits[wi] = 0u;
+            const uint32_t count = static_cast<uint32_t>(__popc(bits));
+            uint32_t incl = count;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (static_cast<int>(lane) >= o) incl += v;
+            }
+            const uint32_t tileTotal = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            if (tileTotal == 0) continue;
+            uint32_t first = 0;
+            if (lane == 0) first = atomicAdd(&ctr->regenCursor, tileTotal);
+            first = __shfl_sync(0xFFFFFFFFu, first, 0);
+            const uint32_t excl = incl - count;
+            for (uint32_t j = 0; j < 32; j++)
+            {
+                const uint32_t w = __shfl_sync(0xFFFFFFFFu, bits, j);
+                const uint32_t offset = __shfl_sync(0xFFFFFFFFu, excl, j);
+                if (!((w >> lane) & 1u)) continue;
+                const uint32_t slot = (tile * 32u + j) * 32u + lane;
+                engine_retire_path(wf, ev, slot);
+                const uint32_t k = first + offset + static_cast<uint32_t>(__popc(w & lanesBelow));
+                if (k < launch) engine_start_launch(wf, ev, k, slot, segmentCount, nxt, base);
+                else ev.freeList[freeCount + (k - launch)] = slot;
+            }
+        }
+        for (uint32_t k = n + blockIdx.x * blockDim.x + threadIdx.x; k < launch; k += gridDim.x * blockDim.x)
+            engine_start_launch(wf, ev, k, ev.freeList[freeCount - 1u - (k - n)], segmentCount, nxt, base);
+        phase_end(ctr, 3);
+    }
+
     // Finished paths write their radiance into their job's ring; planned samples start in the
     // finished slots first, then in slots popped from the free list; finished slots left over are
     // pushed onto the free list.
@@ -1583,6 +1673,7 @@ namespace pt
         c->regenCount = 0;
         c->traceCursor = 0;
         c->shadowCursor = 0;
+        c->regenCursor = 0;
         c->iteration += 1;
         e->launchCount = 0;
         e->segmentCount = 0;
@@ -2007,7 +2098,10 @@ namespace pt
         }
         plan_kernel<<<1, 1, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        engine_regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
+        if (L.wf.regenBits != nullptr)
+            engine_regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
+        else
+            engine_regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         fold_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
