@@ -47,7 +47,7 @@ import numpy as np  # noqa: E402
 WORKLOAD = dict(workload="spheres-1m", scene="spheres-1m", triangles=1310978, width=1920, height=1080, spp=64,
                 depth=12, nee=True, lights=256, pool=1 << 20)
 TRACE_ALGO_BYTES_PER_RAY = 32 + 16 + 4   # ray record read, hit record write, queue index write
-NODE_BYTES = 128
+NODE_BYTES = 64 + 4   # a BVH8 node visit reads the 64-byte header (boxes, origin, scales, masks) and its 4-byte reference
 TRIANGLE_BYTES = 48
 
 
@@ -100,12 +100,12 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per launch of the closest-hit traversal kernel from the committed ncu summary."""
+def profile_dram_bytes_per_ray():
+    """DRAM bytes per ray of the closest-hit traversal kernel, from the committed ncu capture of one
+    full-pool launch of this workload (dram__bytes_read.sum + dram__bytes_write.sum over its rays)."""
     path = os.path.join(ROOT, "profiles", "trace_closest_spheres1m.json")
     if os.path.exists(path):
-        d = json.load(open(path))
-        return d.get("dram_bytes_per_launch_full_size")
+        return json.load(open(path)).get("dram_bytes_per_ray")
     return None
 
 
@@ -543,7 +543,8 @@ def b200_arm(args):
     per_launch_s = ev["trace_event_ms"] / 1000.0 / ev["iterations"]
     achieved = per_launch_bytes / per_launch_s / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic()
+    dram_per_ray = profile_dram_bytes_per_ray()
+    traffic = dram_per_ray * rays / iters if dram_per_ray else None
     launches = sum(s["kernel_launches"] for s in stats)
 
     if dist:
@@ -571,6 +572,7 @@ def b200_arm(args):
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": per_launch_bytes,
                      "bytes_model": f"{TRACE_ALGO_BYTES_PER_RAY} B/ray (ray in, hit out, queue index) + {NODE_BYTES} B/node visited + {TRIANGLE_BYTES} B/triangle tested",
+                     "traffic_source": "ncu DRAM bytes per ray of a full-pool launch (profiles/trace_closest_spheres1m.json) x this run's rays per launch",
                      "node_visits_per_ray": visits / max(rays, 1), "triangle_tests_per_ray": tests / max(rays, 1),
                      "avg_launch_ms": per_launch_s * 1000.0,
                      "avg_launch_ms_source": "CUDA events around each closest-hit launch of one host-looped frame of the same workload",

@@ -68,7 +68,7 @@ LOOP_GRAPH, LOOP_HOST = 0, 1
 BVH8_Q8, BVH2_FP32 = 0, 1
 WAVEFRONT_B200, WAVEFRONT_QUEUES = 0, 1
 SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST = 1, 2
-NODE_BYTES = {BVH8_Q8: 128, BVH2_FP32: 64}
+NODE_BYTES = {BVH8_Q8: 64 + 4, BVH2_FP32: 64}  # bytes a node visit reads: BVH8 header + its child reference; the whole binary node
 
 
 class gpt_frame_stats(ctypes.Structure):
