@@ -34,6 +34,7 @@ namespace pt
         constexpr uint32_t kDefaultSliceIterations = 4096;
         constexpr uint64_t kPathStateBytes = 64;  // admission accounting per path a job may have in flight
         constexpr size_t kArenaAlign = 256;
+        constexpr size_t kStagingBytes = 16u << 20;  // pinned staging for copying finished images out
 
         size_t align_up(size_t v) { return (v + kArenaAlign - 1) / kArenaAlign * kArenaAlign; }
 
@@ -251,7 +252,9 @@ namespace pt
             if (startEvent_) cudaEventDestroy(startEvent_);
             if (stopEvent_) cudaEventDestroy(stopEvent_);
             if (pinned_) cudaFreeHost(pinned_);
+            if (staging_) cudaFreeHost(staging_);
             if (hostMapped_) cudaFreeHost(hostMapped_);
+            if (copyStream_) cudaStreamDestroy(copyStream_);
             if (stream_) cudaStreamDestroy(stream_);
         }
 
@@ -260,6 +263,8 @@ namespace pt
             if (cfg_.schedule > GPT_SCHEDULE_OLDEST_FIRST) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+            PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking));
+            PT_CUDA("cudaHostAlloc", cudaHostAlloc(&staging_, kStagingBytes, cudaHostAllocDefault));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&startEvent_));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&stopEvent_));
             PT_CUDA("cudaHostAlloc", cudaHostAlloc(&hostMapped_, 64, cudaHostAllocMapped));
@@ -575,7 +580,8 @@ namespace pt
             }
             while (!pending_.empty())
             {
-                if (cfg_.max_active_jobs && active_.size() >= cfg_.max_active_jobs) break;
+                // jobs whose images are still being copied out count as active (one at a time means no overlap at all)
+                if (cfg_.max_active_jobs && active_.size() + toCopy_.size() >= cfg_.max_active_jobs) break;
                 if (freeTable_.empty()) break;
                 JobRecord& J = records_[pending_.front()];
                 if (admitted_ + J.admittedBytes > cfg_.hbm_budget_bytes) break;
@@ -642,8 +648,9 @@ namespace pt
             return Status::Ok();
         }
 
-        // Without mu_: one graph launch, then the counters and the job table come back.
-        Status runSlice()
+        // Under mu_: one graph launch, then the counters and the job table come back (queued on the
+        // render stream; waitSlice collects them).
+        Status launchSlice()
         {
             if (!graphExec_) PT_TRY(buildGraph());
             PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
@@ -652,6 +659,12 @@ namespace pt
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(hostCounters_, counters_.get<void>(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(hostCtl_, ctl_.get<void>(), sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_));
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(mirror_, jobs_.get<void>(), size_t(cfg_.max_jobs) * sizeof(JobView), cudaMemcpyDeviceToHost, stream_));
+            return Status::Ok();
+        }
+
+        // Without mu_: waits for the slice launched by launchSlice.
+        Status waitSlice()
+        {
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
             float ms = 0.0f;
             PT_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, startEvent_, stopEvent_));
@@ -663,8 +676,9 @@ namespace pt
             return Status::Ok();
         }
 
-        // Under mu_: progress of running jobs; finished jobs hand their image to the host and free
-        // their table entry, arena range and budget share.
+        // Under mu_: progress of running jobs. Finished jobs leave the active list and wait in toCopy_
+        // for their images to reach host memory; their table entry and arena range stay theirs until
+        // then (the device no longer touches a finished job's buffers).
         Status retire()
         {
             for (size_t i = 0; i < active_.size();)
@@ -678,22 +692,47 @@ namespace pt
                     continue;
                 }
                 if (J.cancelApplied)
-                {
                     finish(J, GPT_JOB_CANCELLED);
-                    active_.erase(active_.begin() + static_cast<std::ptrdiff_t>(i));
-                    continue;
-                }
-                J.rgba.resize(J.pixels);
-                PT_CUDA("cudaMemcpy", cudaMemcpy(J.rgba.data(), J.view.framebuffer, size_t(J.pixels) * 4, cudaMemcpyDeviceToHost));
-                if (J.desc.keep_accumulation)
+                else
                 {
-                    // the accumulator holds (sum, compensation) pairs; the sums are the accumulation
-                    J.accumulation.resize(size_t(J.pixels) * 4);
-                    PT_CUDA("cudaMemcpy2D", cudaMemcpy2D(J.accumulation.data(), 16, J.view.accum, 32, 16, J.pixels, cudaMemcpyDeviceToHost));
+                    J.rgba.resize(J.pixels);
+                    if (J.desc.keep_accumulation) J.accumulation.resize(size_t(J.pixels) * 4);
+                    toCopy_.push_back(J.id);
                 }
-                finish(J, GPT_JOB_DONE);
                 active_.erase(active_.begin() + static_cast<std::ptrdiff_t>(i));
-                completed_++;
+            }
+            return Status::Ok();
+        }
+
+        // Without mu_: images (and accumulations) of finished jobs to host memory through pinned
+        // staging on the copy stream, while the next slice runs on the render stream.
+        Status copyImages(const std::vector<JobRecord*>& jobs)
+        {
+            char* st = static_cast<char*>(staging_);
+            for (JobRecord* J : jobs)
+            {
+                // RGBA8 image in chunks of the fixed staging buffer
+                const char* src = reinterpret_cast<const char*>(J->view.framebuffer);
+                char* dst = reinterpret_cast<char*>(J->rgba.data());
+                for (size_t done = 0, total = size_t(J->pixels) * 4; done < total;)
+                {
+                    const size_t n = std::min(kStagingBytes, total - done);
+                    PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(st, src + done, n, cudaMemcpyDeviceToHost, copyStream_));
+                    PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(copyStream_));
+                    std::memcpy(dst + done, st, n);
+                    done += n;
+                }
+                if (!J->desc.keep_accumulation) continue;
+                // the accumulator holds (sum, compensation) pairs per pixel; the sums are the accumulation
+                const size_t rows = kStagingBytes / 16;
+                for (size_t px = 0; px < J->pixels;)
+                {
+                    const size_t n = std::min(rows, size_t(J->pixels) - px);
+                    PT_CUDA("cudaMemcpy2DAsync", cudaMemcpy2DAsync(st, 16, J->view.accum + 2 * px, 32, 16, n, cudaMemcpyDeviceToHost, copyStream_));
+                    PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(copyStream_));
+                    std::memcpy(J->accumulation.data() + 4 * px, st, n * 16);
+                    px += n;
+                }
             }
             return Status::Ok();
         }
@@ -725,13 +764,16 @@ namespace pt
             cudaStreamSynchronize(stream_);
         }
 
+        // Scheduler thread. Per round: admit waiting jobs and launch a slice; while it runs, copy out
+        // the images of the jobs the previous slice finished and hand them to their waiters; then
+        // collect the slice's results.
         void Run()
         {
             cudaSetDevice(device_);
             std::unique_lock<std::mutex> lock(mu_);
             for (;;)
             {
-                cv_.wait(lock, [&] { return stop_ || !pending_.empty() || !active_.empty(); });
+                cv_.wait(lock, [&] { return stop_ || !pending_.empty() || !active_.empty() || !toCopy_.empty(); });
                 if (stop_) break;
                 // cleared before the queue is read: a job submitted from now on rings again
                 *static_cast<volatile uint32_t*>(hostMapped_) = 0u;
@@ -741,9 +783,30 @@ namespace pt
                     failActive(st);
                     continue;
                 }
-                if (active_.empty()) continue;
+                const bool run = !active_.empty();
+                if (run && !(st = launchSlice()).ok())
+                {
+                    failActive(st);
+                    continue;
+                }
+                std::vector<JobRecord*> batch;
+                for (uint64_t id : toCopy_) batch.push_back(&records_[id]);
+                toCopy_.clear();
+                if (!batch.empty())
+                {
+                    lock.unlock();
+                    const Status cs = copyImages(batch);
+                    lock.lock();
+                    if (!cs.ok()) lastError_ = cs.message;
+                    for (JobRecord* J : batch)
+                    {
+                        finish(*J, cs.ok() ? GPT_JOB_DONE : GPT_JOB_FAILED);
+                        if (cs.ok()) completed_++;
+                    }
+                }
+                if (!run) continue;
                 lock.unlock();
-                st = runSlice();
+                st = waitSlice();
                 lock.lock();
                 if (!st.ok())
                 {
@@ -762,6 +825,9 @@ namespace pt
         uint32_t refill_ = 16;
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;
+        cudaStream_t copyStream_ = nullptr;  // images of finished jobs to host memory, beside the running slice
+        void* staging_ = nullptr;            // pinned staging of those copies, kStagingBytes
+        std::vector<uint64_t> toCopy_;       // finished jobs whose images are not on the host yet
         cudaEvent_t startEvent_ = nullptr, stopEvent_ = nullptr;
         void* hostMapped_ = nullptr;     // [0] doorbell, [16..31] progress
         void* hostMappedDev_ = nullptr;
