@@ -332,6 +332,8 @@ def batched_section(knobs):
         dev_ms = st["device_ms"] - before["device_ms"]
         out[mode] = {"paths_per_second": total / wall, "device_paths_per_second": total / (dev_ms / 1000.0),
                      "wall_s": wall, "device_s": dev_ms / 1000.0, "slices": st["slices"] - before["slices"],
+                     "iterations": st["iterations"] - before["iterations"],
+                     "phase_ms": {k: st["phase_ms"][k] - before["phase_ms"][k] for k in st["phase_ms"]},
                      "admitted_high_water_bytes": st["admitted_high_water"]}
     # one frame at a time through gpt_render_frame: optimised (BVH8, graph loop) and plain form
     renderers = {}

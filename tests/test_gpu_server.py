@@ -202,3 +202,39 @@ def test_nee_without_emitters_matches_oracle(resident, frame_renderers):
     r.render_frame(cam, 24, 24, 4, 6, True)
     assert np.array_equal(r.sample_radiance().view(np.uint32), o["sample_radiance"].view(np.uint32))
     assert np.array_equal(r.framebuffer().reshape(-1), o["framebuffer"])
+
+
+def test_batched_mix_sample_matches_frames(scene_factory):
+    """A scaled-down sample of the 64-job batched mix (its scenes, seeded cameras, spp and depths,
+    resolutions divided by 8) rendered together through the server: every image equals the frame
+    renderer's for the same job, bit for bit."""
+    import workloads
+    names = ("spheres-10k", "spheres-200k")
+    jobs = [j for j in workloads.batched_jobs() if j.scene in names][:8]
+    assert len(jobs) >= 4
+    resident = {n: scene_factory(n) for n in names}
+    srv = pathtracer.Server(0, pool_size=1 << 18, hbm_budget_bytes=BUDGET)
+    renderers = {}
+    try:
+        ids = {n: srv.add_scene(s) for n, s in resident.items()}
+        small = []
+        for j in jobs:
+            w, h = max(8, j.width // 8), max(8, j.height // 8)
+            cam = workloads.orbit_camera(np.random.default_rng(len(small)), w, h)
+            small.append((j.scene, w, h, j.spp, j.depth, cam))
+        jids = [srv.submit(ids[n], cam, w, h, spp, depth, True, keep_accumulation=True) for n, w, h, spp, depth, cam in small]
+        for n in names:
+            renderers[n] = pathtracer.Renderer(0)
+            renderers[n].upload_scene(resident[n])
+        for jid, (n, w, h, spp, depth, cam) in zip(jids, small):
+            st = srv.wait(jid, 300)
+            assert st["state"] == "done", srv.last_error()
+            fb, acc = srv.result(jid, accumulation=True)
+            r = renderers[n]
+            r.render_frame(cam, w, h, spp, depth, True)
+            assert np.array_equal(acc.view(np.uint32), r.accumulation().reshape(-1, 4).view(np.uint32)), (n, w, h, spp)
+            assert np.array_equal(fb, r.framebuffer().reshape(-1))
+    finally:
+        srv.close()
+        for r in renderers.values():
+            r.close()
