@@ -79,12 +79,17 @@ namespace pt
     {
         RayPre ray;
         float hitT;        // closest hit so far (tMax of the query until a hit)
-        uint32_t hitTri;   // input index of that triangle, kInvalid when none
-        uint32_t pending;  // node to visit next, kInvalid when the stack decides
+        uint32_t pending;  // binary BVH: node to visit next, kInvalid when the stack decides
         int sp;
     };
 
-    // Shared-memory slot of one thread: [0] = direction xyz, tag; [1] = hit u, v, model, queue index.
+    // Traversal work of a lane: node visits in bits 0-15, triangle tests in bits 16-31 (flushed to
+    // the frame counters before either field can overflow).
+    constexpr uint32_t kVisit = 1u;
+    constexpr uint32_t kTestShift = 16;
+
+    // Shared-memory slot of one thread: [0] = direction xyz, tag; [1] = hit u, v,
+    // triangle | model << 24 (kInvalid while there is no hit), queue index.
     struct ColdSlot
     {
         float4* p;
@@ -99,9 +104,9 @@ namespace pt
     // found an occluder (traversal over); closest hit keeps the best hit in st.hit.
     template <bool ANY>
     __device__ __forceinline__ bool leaf_tests(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t first, uint32_t count,
-                                               bool& occluded, uint32_t& tests)
+                                               bool& occluded, uint32_t& work)
     {
-        tests += count;
+        work += count << kTestShift;
         const float3 d = cold.direction();
         for (uint32_t k = 0; k < count; k++)
         {
@@ -119,14 +124,23 @@ namespace pt
             }
             else
             {
-                const uint32_t orig = __float_as_uint(a.w);
-                if (better_hit(t, orig, st.ray.tmin, st.hitT, st.hitTri))
+                // better_hit with the best triangle read from shared memory: it matters only at a tie
+                if (t >= st.ray.tmin && t <= st.hitT)
                 {
-                    st.hitT = t;
-                    st.hitTri = orig;
-                    cold.p[1].x = u;
-                    cold.p[1].y = v;
-                    cold.p[1].z = b.w;  // shading model bits
+                    const uint32_t orig = __float_as_uint(a.w);
+                    bool better = t < st.hitT;
+                    if (!better)
+                    {
+                        const uint32_t best = __float_as_uint(cold.p[1].z);
+                        better = best != kInvalid && orig < (best & 0xFFFFFFu);
+                    }
+                    if (better)
+                    {
+                        st.hitT = t;
+                        cold.p[1].x = u;
+                        cold.p[1].y = v;
+                        cold.p[1].z = __uint_as_float(orig | (__float_as_uint(b.w) << 24));  // triangle, shading model
+                    }
                 }
             }
         }
@@ -164,7 +178,7 @@ namespace pt
     // farther pushed. Stack entries are node indices. Returns false when traversal is over.
     template <bool ANY>
     __device__ __forceinline__ bool traverse_step_binary(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, int stackCap,
-                                                         bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
+                                                         bool& occluded, uint32_t* errorFlags, uint32_t& work)
     {
         uint32_t node;
         if (st.pending != kInvalid)
@@ -178,7 +192,7 @@ namespace pt
             node = stack[--st.sp];
         }
         const uint4* nw = sc.nodes2[node].w;
-        visits++;
+        work += kVisit;
         const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
         float tn0, tn1;
         const bool h0 = ((w3.z >> 24) & 1u) &&
@@ -189,9 +203,9 @@ namespace pt
                                   __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, st.hitT, tn1);
         const uint32_t leafMask = (w3.z >> 16) & 3u;
         if (h0 && (leafMask & 1u))
-            if (!leaf_tests<ANY>(sc, st, cold, w3.x, w3.z & 0xFFu, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, w3.x, w3.z & 0xFFu, occluded, work)) return false;
         if (h1 && (leafMask & 2u))
-            if (!leaf_tests<ANY>(sc, st, cold, w3.y, (w3.z >> 8) & 0xFFu, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, w3.y, (w3.z >> 8) & 0xFFu, occluded, work)) return false;
         const bool in0 = h0 && !(leafMask & 1u), in1 = h1 && !(leafMask & 2u);
         if (in0 && in1)
         {
@@ -215,20 +229,22 @@ namespace pt
     // ANY: stops at the first triangle with tmin <= t < tmax.
     template <bool ANY>
     __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, uint32_t stride,
-                                                  int stackCap, bool& occluded, uint32_t* errorFlags, uint32_t& visits, uint32_t& tests)
+                                                  int stackCap, bool& occluded, uint32_t* errorFlags, uint32_t& work)
     {
+        // stack entry = node << 8 | child slots still to visit (traversal order); an entry with no
+        // slots is a node to visit itself (the root a ray starts with)
+        if (st.sp == 0) return false;
+        uint32_t* top = stack + static_cast<uint32_t>(st.sp - 1) * stride;
+        const uint32_t entry = *top;
         uint32_t node;
-        if (st.pending != kInvalid)
+        uint32_t m = entry & 0xFFu;
+        if (m == 0)
         {
-            node = st.pending;
-            st.pending = kInvalid;
+            node = entry >> 8;
+            st.sp--;
         }
         else
         {
-            if (st.sp == 0) return false;
-            uint32_t* top = stack + static_cast<uint32_t>(st.sp - 1) * stride;
-            const uint32_t entry = *top;
-            uint32_t m = entry & 0xFFu;
             const uint32_t i = static_cast<uint32_t>(__ffs(m) - 1);
             m &= m - 1u;
             if (m == 0) st.sp--;
@@ -238,7 +254,7 @@ namespace pt
             node = __ldg(childRefs + (i ^ st.ray.oct));
         }
         const uint4* nw = sc.nodes[node].w;
-        visits++;
+        work += kVisit;
         const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
         const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, st.ray, st.hitT);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
@@ -249,7 +265,7 @@ namespace pt
             leafOrder &= leafOrder - 1u;
             const uint32_t slot = i ^ st.ray.oct;
             const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
-            if (!leaf_tests<ANY>(sc, st, cold, ref & 0xFFFFFFu, ref >> 24, occluded, tests)) return false;
+            if (!leaf_tests<ANY>(sc, st, cold, ref & 0xFFFFFFu, ref >> 24, occluded, work)) return false;
         }
         if (innerSlots)
         {
@@ -424,9 +440,8 @@ namespace pt
         Counters* ctr = work.counters();
         phase_begin(ctr, Work::kPhase);
         const uint32_t n = work.count();
-        uint32_t visits = 0, tests = 0;
+        uint32_t counts = 0;  // node visits | triangle tests << 16
         const uint32_t lane = lane_id();
-        const unsigned laneMaskLt = (1u << lane) - 1u;
         TraversalState st;
         bool active = false;
         bool exhausted = false;
@@ -441,6 +456,8 @@ namespace pt
                 if (base >= n) exhausted = true;
                 if (!active)
                 {
+                    unsigned laneMaskLt;
+                    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(laneMaskLt));
                     const uint32_t i = base + static_cast<uint32_t>(__popc(idle & laneMaskLt));
                     if (i < n)
                     {
@@ -449,12 +466,19 @@ namespace pt
                         uint32_t tag;
                         work.load(i, o, d, tmin, tmax, tag);
                         cold.p[0] = make_float4(d.x, d.y, d.z, __uint_as_float(tag));
-                        cold.p[1] = make_float4(0.0f, 0.0f, 0.0f, __uint_as_float(i));
+                        cold.p[1] = make_float4(0.0f, 0.0f, __uint_as_float(kInvalid), __uint_as_float(i));
                         st.ray = make_ray(o, d, tmin);
                         st.hitT = tmax;
-                        st.hitTri = kInvalid;
-                        st.pending = work.root(tag);
-                        st.sp = 0;
+                        if constexpr (BINARY)
+                        {
+                            st.pending = work.root(tag);
+                            st.sp = 0;
+                        }
+                        else
+                        {
+                            stack[0] = work.root(tag) << 8;
+                            st.sp = 1;
+                        }
                         active = true;
                     }
                 }
@@ -472,27 +496,35 @@ namespace pt
                 for (int k = 0; k < 4 && more; k++)
                 {
                     if constexpr (BINARY)
-                        more = traverse_step_binary<ANY>(work.sc, st, cold, stack, STACK, occluded, errorFlags, visits, tests);
+                        more = traverse_step_binary<ANY>(work.sc, st, cold, stack, STACK, occluded, errorFlags, counts);
                     else
-                        more = traverse_step<ANY>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, visits, tests);
+                        more = traverse_step<ANY>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, counts);
                 }
                 if (!more)
                 {
                     const float4 c0 = cold.p[0], c1 = cold.p[1];
+                    const uint32_t best = __float_as_uint(c1.z);
                     HitRecord h;
                     h.t = st.hitT;
-                    h.tri = st.hitTri;
+                    h.tri = best == kInvalid ? kInvalid : (best & 0xFFFFFFu);
                     h.u = c1.x;
                     h.v = c1.y;
-                    h.model = __float_as_uint(c1.z);
+                    h.model = best == kInvalid ? 0u : (best >> 24);
                     work.finish(__float_as_uint(c1.w), __float_as_uint(c0.w), h, occluded);
                     active = false;
+                }
+                // a step adds at most 8 x 255 tests: flush the packed counters well before a field overflows
+                if (ctr != nullptr && (counts & 0x80008000u))
+                {
+                    atomicAdd(&ctr->nodeVisits[ANY ? 1 : 0], static_cast<unsigned long long>(counts & 0xFFFFu));
+                    atomicAdd(&ctr->triTests[ANY ? 1 : 0], static_cast<unsigned long long>(counts >> kTestShift));
+                    counts = 0;
                 }
             }
         }
         if (ctr != nullptr)
         {
-            unsigned long long v = visits, t = tests;
+            unsigned long long v = counts & 0xFFFFu, t = counts >> kTestShift;
             for (int o = 16; o > 0; o >>= 1)
             {
                 v += __shfl_down_sync(0xFFFFFFFFu, v, o);
