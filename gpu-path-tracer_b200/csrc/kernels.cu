@@ -102,10 +102,12 @@ namespace pt
 
     // Triangles [first, first + count) of a leaf (leaf order). Returns false when an any-hit query
     // found an occluder (traversal over); closest hit keeps the best hit in st.hit.
-    template <bool ANY>
+    // FIXED: the query's tMin is the wavefront's constant kMinT (no register holds it).
+    template <bool ANY, bool FIXED>
     __device__ __forceinline__ bool leaf_tests(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t first, uint32_t count,
                                                bool& occluded, uint32_t& work)
     {
+        const float tmin = FIXED ? kMinT : st.ray.tmin;
         work += count << kTestShift;
         const float3 d = cold.direction();
         for (uint32_t k = 0; k < count; k++)
@@ -116,7 +118,7 @@ namespace pt
             if (!intersect_triangle(a, b, c, st.ray.o, d, t, u, v)) continue;
             if (ANY)
             {
-                if (t >= st.ray.tmin && t < st.hitT)
+                if (t >= tmin && t < st.hitT)
                 {
                     occluded = true;
                     return false;
@@ -125,7 +127,7 @@ namespace pt
             else
             {
                 // better_hit with the best triangle read from shared memory: it matters only at a tie
-                if (t >= st.ray.tmin && t <= st.hitT)
+                if (t >= tmin && t <= st.hitT)
                 {
                     const uint32_t orig = __float_as_uint(a.w);
                     bool better = t < st.hitT;
@@ -151,8 +153,8 @@ namespace pt
     // subtraction and one multiplication by the rounded reciprocal (at most 3 roundings, relative error
     // below 2^-21); entry distances are lowered and exit distances raised by 2^-20 of their magnitude,
     // so a box the exact arithmetic would hit is never culled. tnear: the widened entry distance.
-    __device__ __forceinline__ bool slab_fp32(float lx, float ly, float lz, float hx, float hy, float hz, const RayPre& r, float tmax,
-                                              float& tnear)
+    __device__ __forceinline__ bool slab_fp32(float lx, float ly, float lz, float hx, float hy, float hz, const RayPre& r, float tmin,
+                                              float tmax, float& tnear)
     {
         const float kEps = 9.5367431640625e-07f;  // 2^-20
         const float ax = (lx - r.o.x) * r.invd.x, bx = (hx - r.o.x) * r.invd.x;
@@ -167,7 +169,7 @@ namespace pt
         fx = fx + fabsf(fx) * kEps;
         fy = fy + fabsf(fy) * kEps;
         fz = fz + fabsf(fz) * kEps;
-        const float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, r.tmin));
+        const float tn = fmaxf(fmaxf(nx, ny), fmaxf(nz, tmin));
         const float tf = fminf(fminf(fx, fy), fminf(fz, tmax));
         tnear = tn;
         return tn <= tf;
@@ -176,7 +178,7 @@ namespace pt
     // Binary FP32 BVH: visit one node (two child boxes) or pop the next node. Leaf children that the
     // ray enters are tested at once; of two internal children the nearer is visited next and the
     // farther pushed. Stack entries are node indices. Returns false when traversal is over.
-    template <bool ANY>
+    template <bool ANY, bool FIXED>
     __device__ __forceinline__ bool traverse_step_binary(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, int stackCap,
                                                          bool& occluded, uint32_t* errorFlags, uint32_t& work)
     {
@@ -197,15 +199,15 @@ namespace pt
         float tn0, tn1;
         const bool h0 = ((w3.z >> 24) & 1u) &&
                         slab_fp32(__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z), __uint_as_float(w0.w),
-                                  __uint_as_float(w1.x), __uint_as_float(w1.y), st.ray, st.hitT, tn0);
+                                  __uint_as_float(w1.x), __uint_as_float(w1.y), st.ray, FIXED ? kMinT : st.ray.tmin, st.hitT, tn0);
         const bool h1 = ((w3.z >> 25) & 1u) &&
                         slab_fp32(__uint_as_float(w1.z), __uint_as_float(w1.w), __uint_as_float(w2.x), __uint_as_float(w2.y),
-                                  __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, st.hitT, tn1);
+                                  __uint_as_float(w2.z), __uint_as_float(w2.w), st.ray, FIXED ? kMinT : st.ray.tmin, st.hitT, tn1);
         const uint32_t leafMask = (w3.z >> 16) & 3u;
         if (h0 && (leafMask & 1u))
-            if (!leaf_tests<ANY>(sc, st, cold, w3.x, w3.z & 0xFFu, occluded, work)) return false;
+            if (!leaf_tests<ANY, FIXED>(sc, st, cold, w3.x, w3.z & 0xFFu, occluded, work)) return false;
         if (h1 && (leafMask & 2u))
-            if (!leaf_tests<ANY>(sc, st, cold, w3.y, (w3.z >> 8) & 0xFFu, occluded, work)) return false;
+            if (!leaf_tests<ANY, FIXED>(sc, st, cold, w3.y, (w3.z >> 8) & 0xFFu, occluded, work)) return false;
         const bool in0 = h0 && !(leafMask & 1u), in1 = h1 && !(leafMask & 2u);
         if (in0 && in1)
         {
@@ -227,7 +229,7 @@ namespace pt
 
     // Visit one node or pop the next child group. Returns false when traversal is over.
     // ANY: stops at the first triangle with tmin <= t < tmax.
-    template <bool ANY>
+    template <bool ANY, bool FIXED>
     __device__ __forceinline__ bool traverse_step(const SceneView& sc, TraversalState& st, ColdSlot cold, uint32_t* stack, uint32_t stride,
                                                   int stackCap, bool& occluded, uint32_t* errorFlags, uint32_t& work)
     {
@@ -256,7 +258,7 @@ namespace pt
         const uint4* nw = sc.nodes[node].w;
         work += kVisit;
         const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
-        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, st.ray, st.hitT);
+        const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, st.ray, FIXED ? kMinT : st.ray.tmin, st.hitT);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
         uint32_t leafOrder = permute_mask(hitSlots & ~(w0.w >> 24), st.ray.oct);
         while (leafOrder)
@@ -265,7 +267,7 @@ namespace pt
             leafOrder &= leafOrder - 1u;
             const uint32_t slot = i ^ st.ray.oct;
             const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(&nw[4]) + slot);
-            if (!leaf_tests<ANY>(sc, st, cold, ref & 0xFFFFFFu, ref >> 24, occluded, work)) return false;
+            if (!leaf_tests<ANY, FIXED>(sc, st, cold, ref & 0xFFFFFFu, ref >> 24, occluded, work)) return false;
         }
         if (innerSlots)
         {
@@ -303,6 +305,7 @@ namespace pt
         Wavefront wf;
         const SceneEntry* scenes;  // nullptr: one scene rooted at node 0
         static constexpr int kPhase = 0;
+        static constexpr bool kFixedTmin = true;   // every wavefront ray starts at kMinT
         __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
         __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->rayCount[wf.ctr->cur]; }
@@ -347,6 +350,7 @@ namespace pt
         Wavefront wf;
         const SceneEntry* scenes;
         static constexpr int kPhase = 2;
+        static constexpr bool kFixedTmin = true;
         __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
         __device__ Counters* counters() const { return wf.ctr; }
         __device__ uint32_t count() const { return wf.ctr->shadowCount; }
@@ -385,6 +389,7 @@ namespace pt
         uint8_t* occOut;
         uint32_t rootNode;
         static constexpr int kPhase = 0;
+        static constexpr bool kFixedTmin = false;  // per-ray tMin of the caller's batch
         __device__ uint32_t root(uint32_t) const { return rootNode; }
         __device__ Counters* counters() const { return nullptr; }
         __device__ uint32_t count() const { return n; }
@@ -496,9 +501,9 @@ namespace pt
                 for (int k = 0; k < 4 && more; k++)
                 {
                     if constexpr (BINARY)
-                        more = traverse_step_binary<ANY>(work.sc, st, cold, stack, STACK, occluded, errorFlags, counts);
+                        more = traverse_step_binary<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, STACK, occluded, errorFlags, counts);
                     else
-                        more = traverse_step<ANY>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, counts);
+                        more = traverse_step<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, counts);
                 }
                 if (!more)
                 {

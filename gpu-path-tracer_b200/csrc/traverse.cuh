@@ -61,7 +61,7 @@ namespace pt
     // space, so the test is conservative for every child box (a box the exact arithmetic
     // would hit is never culled). Returns the hit mask in slot order. Empty slots hold inverted
     // boxes and are almost always culled; one that passes has a zero child reference (no work).
-    PT_HD uint32_t intersect_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, const RayPre& r, float tmax)
+    PT_HD uint32_t intersect_children(uint4 w0, uint4 w1, uint4 w2, uint4 w3, const RayPre& r, float tmin, float tmax)
     {
         const float px = as_float(w0.x), py = as_float(w0.y), pz = as_float(w0.z);
         const float sx = as_float((w0.w & 0xFFu) << 23);
@@ -95,7 +95,7 @@ namespace pt
             const float tfx = fma_hd(byte_to_float(fxl, fxh, s), ax, bfx);
             const float tfy = fma_hd(byte_to_float(fyl, fyh, s), ay, bfy);
             const float tfz = fma_hd(byte_to_float(fzl, fzh, s), az, bfz);
-            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, r.tmin));
+            const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
             const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
             hit |= (tn <= tf ? 1u : 0u) << s;
         }
