@@ -232,7 +232,9 @@ namespace pt
             if (!cfg_.max_slice_iterations) cfg_.max_slice_iterations = kDefaultSliceIterations;
             cfg_.ring_passes = std::min(cfg_.ring_passes, kMaxRing);
             threads_ = cfg_.trace_block == 64 ? 64 : 128;
-            refill_ = cfg_.trace_refill ? std::min(32u, std::max(1u, cfg_.trace_refill)) : 16u;
+            refill_ = (cfg_.trace_refill & 0xFFu) ? std::min(32u, std::max(1u, cfg_.trace_refill & 0xFFu)) : 16u;
+            refillShadow_ = ((cfg_.trace_refill >> 8) & 0xFFu) ? std::min(32u, std::max(1u, (cfg_.trace_refill >> 8) & 0xFFu))
+                                                                : std::max(1u, refill_ / 2u);
             occupancy_ = cfg_.trace_occupancy == 0 ? 10 : (cfg_.trace_occupancy >= 12 ? 12 : (cfg_.trace_occupancy >= 10 ? 10 : 1));
             shortestFirst_ = cfg_.schedule != GPT_SCHEDULE_OLDEST_FIRST;
             t0_ = std::chrono::steady_clock::now();
@@ -552,6 +554,7 @@ namespace pt
             L.occupancy = occupancy_;
             L.traceBlocks = trace_grid_blocks(device_, threads_, pack_.depth, occupancy_);
             L.refill = refill_;
+            L.refillShadow = refillShadow_;
             L.shadeBlocks = sms * 8;
             L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -822,7 +825,7 @@ namespace pt
         gpt_server_config cfg_;
         int threads_ = 128, occupancy_ = 10;
         bool shortestFirst_ = true;
-        uint32_t refill_ = 16;
+        uint32_t refill_ = 16, refillShadow_ = 8;
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;
         cudaStream_t copyStream_ = nullptr;  // images of finished jobs to host memory, beside the running slice

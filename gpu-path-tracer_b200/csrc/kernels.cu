@@ -2117,9 +2117,9 @@ namespace pt
         {
             WavefrontShadow ws{L.scene, L.wf, nullptr};
             if (binary)
-                e = launch_trace_binary<true>(ws, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+                e = launch_trace_binary<true>(ws, L.traceBlocks, L.traceThreads, L.refillShadow, &L.wf.ctr->errorFlags, s);
             else
-                e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+                e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refillShadow, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
         if (L.wf.regenBits != nullptr)
@@ -2152,7 +2152,7 @@ namespace pt
         if (L.anyLights)
         {
             WavefrontShadow ws{L.scene, L.wf, L.ev.scenes};
-            e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
+            e = launch_trace<true>(ws, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refillShadow, &L.wf.ctr->errorFlags, s);
             if (e != cudaSuccess) return e;
         }
         plan_kernel<<<1, 1, 0, s>>>(L.wf, L.ev);

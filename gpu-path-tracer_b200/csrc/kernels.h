@@ -18,6 +18,7 @@ namespace pt
         int traceBlocks;
         int traceThreads;
         uint32_t refill;
+        uint32_t refillShadow;     // the same threshold for the shadow-ray (any-hit) traversal
         int occupancy;             // traversal kernel variant: 1, 10 or 12 resident blocks per SM targeted
         int shadeBlocks;
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
@@ -43,6 +44,7 @@ namespace pt
         int traceBlocks;
         int traceThreads;
         uint32_t refill;
+        uint32_t refillShadow;
         int occupancy;
         int shadeBlocks;
         bool graphLoop;

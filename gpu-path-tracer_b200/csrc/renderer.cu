@@ -396,7 +396,7 @@ namespace pt
             uint32_t width, height, spp, spa, depth, nee, pool;
             uint64_t totalSamples;
             int traceThreads;
-            uint32_t refill;
+            uint32_t refill, refillShadow;
             int occupancy;
             uint32_t bvh;
             bool queues;   // the reference's wavefront structure (regeneration queue, shading in sequence)
@@ -419,7 +419,10 @@ namespace pt
                 return Status::Err(GPT_ERR_CAPACITY, "A frame is limited to 2^32-1 samples (per-sample radiance capture)");
             c.traceThreads = s.trace_block ? static_cast<int>(s.trace_block) : 128;
             if (c.traceThreads != 64 && c.traceThreads != 128) c.traceThreads = 128;
-            c.refill = s.trace_refill ? std::min(32u, std::max(1u, s.trace_refill)) : 16u;
+            // bits 0-7: closest-hit traversal (0 = 16); bits 8-15: shadow rays (0 = half the closest-hit value)
+            c.refill = (s.trace_refill & 0xFFu) ? std::min(32u, std::max(1u, s.trace_refill & 0xFFu)) : 16u;
+            c.refillShadow = ((s.trace_refill >> 8) & 0xFFu) ? std::min(32u, std::max(1u, (s.trace_refill >> 8) & 0xFFu))
+                                                              : std::max(1u, c.refill / 2u);
             c.occupancy = s.trace_occupancy == 0 ? 10 : (s.trace_occupancy >= 12 ? 12 : (s.trace_occupancy >= 10 ? 10 : 1));
             if (s.bvh_format > GPT_BVH2_FP32) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown BVH format");
             c.bvh = s.bvh_format == GPT_BVH2_FP32 ? kBvh2Fp32 : kBvh8Quantised;
@@ -483,6 +486,7 @@ namespace pt
             L.occupancy = c.occupancy;
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
+            L.refillShadow = c.refillShadow;
             L.bvhFormat = c.bvh;
             L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
@@ -530,6 +534,7 @@ namespace pt
             L.occupancy = c.occupancy;
             L.traceBlocks = trace_grid_blocks(device_, c.traceThreads, sv.depth, c.occupancy, c.bvh);
             L.refill = c.refill;
+            L.refillShadow = c.refillShadow;
             L.bvhFormat = c.bvh;
             L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
@@ -564,7 +569,7 @@ namespace pt
         {
             char buf[256];
             std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%d/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
-                          c.nee, c.traceThreads, c.refill, c.occupancy, c.bvh, c.queues ? 1 : 0, width_, height_,
+                          c.nee, c.traceThreads, c.refill | (c.refillShadow << 8), c.occupancy, c.bvh, c.queues ? 1 : 0, width_, height_,
                           static_cast<void*>(accumulation_.get<void>()),
                           static_cast<void*>(framebuffer_.get<void>()));
             return buf;
@@ -698,6 +703,29 @@ namespace pt
                                     best.trace_block = tb;
                                 }
                             }
+            }
+            // shadow rays tune their own refill threshold with the other knobs fixed
+            const uint32_t closestRefill = best.trace_refill & 0xFFu;
+            for (uint32_t shadowRefill : {2u, 4u, 8u, 16u})
+            {
+                trial = best;
+                trial.samples_per_pixel = std::min<uint32_t>(std::max(base.samples_per_pixel, 1u), 4u);
+                trial.max_samples = 0;
+                trial.loop_mode = GPT_LOOP_GRAPH;
+                trial.trace_refill = closestRefill | (shadowRefill << 8);
+                float ms = 1e30f;
+                for (int rep = 0; rep < 2; rep++)
+                {
+                    gpt_frame_stats st{};
+                    PT_TRY(RenderFrame(cam, trial, &st, false));
+                    if (rep) ms = st.device_ms;
+                }
+                tried++;
+                if (ms < bestMs)
+                {
+                    bestMs = ms;
+                    best.trace_refill = trial.trace_refill;
+                }
             }
             return Status::Ok();
         }

@@ -124,7 +124,8 @@ typedef struct gpt_render_settings {
     uint32_t pool_size;           /* path slots; 0 = 1,048,576 (PathTracerDefaults.hpp:9) */
     uint64_t max_samples;         /* 0 = the whole frame; else render only sample indices [0, max_samples) */
     uint32_t trace_block;         /* 0 = default threads per block of the traversal kernels (64 or 128) */
-    uint32_t trace_refill;        /* 0 = default; idle lanes a warp waits for before fetching new rays */
+    uint32_t trace_refill;        /* idle lanes a traversal warp waits for before fetching new rays: bits 0-7 for
+                                     closest-hit rays (0 = 16), bits 8-15 for shadow rays (0 = half the former) */
     uint64_t rng_offset;          /* added to every sample index to form its Philox subsequence (0 = the reference's streams) */
     uint32_t loop_mode;           /* GPT_LOOP_GRAPH (default): the whole frame is one CUDA graph whose conditional WHILE
                                      node repeats the iteration on the device; GPT_LOOP_HOST: the host launches each
