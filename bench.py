@@ -241,7 +241,7 @@ def plain_form(renderer, cam, W, H, spp, depth, frames=2):
     after another, host-driven iteration loop with a flag read per iteration, 1,048,576 path slots (the
     reference's pool), no autotuning. Same images bit for bit as the optimised form."""
     import pathtracer
-    settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
+    settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32 | (32 << 8), trace_block=128,
                     loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32,
                     wavefront_layout=pathtracer.WAVEFRONT_QUEUES)
     renderer.render_frame(cam, W, H, spp, depth, True, **settings)
@@ -341,7 +341,7 @@ def batched_section(knobs):
         for n, s in resident.items():
             renderers[n] = pathtracer.Renderer(0)
             renderers[n].upload_scene(s)
-        plain_settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32, trace_block=128,
+        plain_settings = dict(pool_size=1 << 20, trace_occupancy=1, trace_refill=32 | (32 << 8), trace_block=128,
                               loop_mode=pathtracer.LOOP_HOST, bvh_format=pathtracer.BVH2_FP32,
                               wavefront_layout=pathtracer.WAVEFRONT_QUEUES)
         for mode, settings in (("frames_one_at_a_time", dict(knobs)), ("plain_form_one_at_a_time", plain_settings)):

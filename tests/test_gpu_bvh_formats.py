@@ -61,7 +61,7 @@ def test_binary_bvh_frames_bit_identical(gpu_renderer, scene_factory, oracle_sce
     # the plain configuration: binary FP32 BVH, warps refilled only when all lanes are idle, the
     # reference's queue structure (regeneration queue, shading in sequence), host loop
     b = gpu_renderer.render_frame(cam, w, h, spp, depth, True, pool_size=5000, bvh_format=P.BVH2_FP32,
-                                  trace_refill=32, loop_mode=loop, wavefront_layout=P.WAVEFRONT_QUEUES)
+                                  trace_refill=32 | (32 << 8), loop_mode=loop, wavefront_layout=P.WAVEFRONT_QUEUES)
     rad_b, log_b, fb_b = gpu_renderer.sample_radiance(), gpu_renderer.queue_log(), gpu_renderer.framebuffer()
     assert a["iterations"] == b["iterations"]
     assert np.array_equal(log_a, log_b)
