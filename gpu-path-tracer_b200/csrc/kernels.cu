@@ -751,8 +751,15 @@ namespace pt
         s.normal = b0 * f3(n0) + b1 * f3(n1) + b2 * f3(n2);
         const float4 t0 = ldg4(rec + 3), t1 = ldg4(rec + 4), t2 = ldg4(rec + 5);
         s.tangent = b0 * t0 + b1 * t1 + b2 * t2;
-        const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
-        s.uv = b0 * make_float2(u01.x, u01.y) + b1 * make_float2(u01.z, u01.w) + b2 * make_float2(u2.x, u2.y);
+        // uv only feeds texture lookups: without image textures every slot is a constant, so the
+        // record's last 32 bytes are not read
+        if (sc.textures != nullptr)
+        {
+            const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
+            s.uv = b0 * make_float2(u01.x, u01.y) + b1 * make_float2(u01.z, u01.w) + b2 * make_float2(u2.x, u2.y);
+        }
+        else
+            s.uv = make_float2(0.0f, 0.0f);
         return s;
     }
 
@@ -1175,8 +1182,12 @@ namespace pt
                     const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
                     const uint32_t mat = __float_as_uint(__ldg(&rec[6].w));
                     const float b0 = 1.0f - h4.y - h4.z;
-                    const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
-                    const float2 uv = b0 * make_float2(u01.x, u01.y) + h4.y * make_float2(u01.z, u01.w) + h4.z * make_float2(u2.x, u2.y);
+                    float2 uv = make_float2(0.0f, 0.0f);
+                    if (sc.textures != nullptr)
+                    {
+                        const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
+                        uv = b0 * make_float2(u01.x, u01.y) + h4.y * make_float2(u01.z, u01.w) + h4.z * make_float2(u2.x, u2.y);
+                    }
                     const float3 em = slot_rgb(sc, mat, 4, uv, sc.materials[mat].emission);
                     const float3 c = T * em;
                     L4.x = L4.x + c.x;
