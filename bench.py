@@ -499,12 +499,20 @@ def b200_arm(args):
                  trace_refill=tuned.get("trace_refill", args.trace_refill),
                  trace_block=tuned.get("trace_block", args.trace_block))
 
+    exchange = [torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] if world > 1 else None
+
     def step():
         st = renderer.render_frame(cam, W, H, spp, depth, True, rng_offset=rng_offset, loop_mode=loop_mode, **knobs)
         if world > 1:
-            host = renderer.accumulation()
-            accum.copy_(torch.from_numpy(host))
+            # the frame's accumulation straight into the collective's buffer (device to device), then one
+            # all-reduce over NCCL; both timed with CUDA events on torch's stream and added to the step
+            cur = torch.cuda.current_stream()
+            exchange[0].record(cur)
+            renderer.copy_accumulation_to(accum, stream=cur.cuda_stream)
             multigpu.combine_accumulation(accum, dist)
+            exchange[1].record(cur)
+            exchange[1].synchronize()
+            st["device_ms"] += exchange[0].elapsed_time(exchange[1])
         return st
 
     for _ in range(args.warmup):

@@ -1105,6 +1105,17 @@ extern "C"
         return Report(r, pt::CudaStatus("cudaMemcpy", e));
     }
 
+    int gpt_copy_accumulation_device(gpt_renderer* r, float* dst, size_t pixel_count, void* stream)
+    {
+        if (!r || !dst) return GPT_ERR_INVALID_ARGUMENT;
+        if (pixel_count > r->impl->lastPixels_) return GPT_ERR_CAPACITY;
+        cudaSetDevice(r->impl->device_);
+        cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : r->impl->stream_;
+        cudaError_t e = cudaMemcpyAsync(dst, r->impl->accumulation_.get<void>(), pixel_count * 16, cudaMemcpyDeviceToDevice, s);
+        if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(s);
+        return Report(r, pt::CudaStatus("cudaMemcpyAsync", e));
+    }
+
     int gpt_read_sample_radiance(gpt_renderer* r, float* out, uint64_t count)
     {
         if (!r || !out) return GPT_ERR_INVALID_ARGUMENT;

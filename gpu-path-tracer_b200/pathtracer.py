@@ -145,6 +145,7 @@ _SIGNATURES = [
     ("gpt_read_framebuffer", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_accumulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_sample_radiance", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
+    ("gpt_copy_accumulation_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
     ("gpt_read_queue_log", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_intersect_closest", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
@@ -322,6 +323,11 @@ class Renderer:
         out = np.zeros((self.width * self.height, 4), dtype=np.float32)
         self._check(self.L.gpt_read_accumulation(self.h, _ptr(out), self.width * self.height), "gpt_read_accumulation")
         return out
+
+    def copy_accumulation_to(self, dst_dev, stream=None):
+        """The last frame's [pixels, 4] float32 accumulation into a device tensor of the same GPU."""
+        self._check(self.L.gpt_copy_accumulation_device(self.h, ctypes.c_void_p(dst_dev.data_ptr()), self.width * self.height,
+                                                        ctypes.c_void_p(stream)), "gpt_copy_accumulation_device")
 
     def sample_radiance(self) -> np.ndarray:
         out = np.zeros((self.total_samples, 3), dtype=np.float32)

@@ -232,6 +232,11 @@ int gpt_read_framebuffer(gpt_renderer* renderer, uint32_t* rgba, size_t pixel_co
 int gpt_read_accumulation(gpt_renderer* renderer, float* rgba32f, size_t pixel_count);
 /* Per-sample (per-path) radiance of the last frame, [samples][3], in sample-index order. */
 int gpt_read_sample_radiance(gpt_renderer* renderer, float* rgb, uint64_t sample_count);
+/* The last frame's float4 accumulation into a device buffer of the same GPU (for a collective across
+ * ranks without a round trip through host memory). stream NULL: the renderer's stream, synchronised
+ * before returning; else the copy is queued on `stream` after the frame (gpt_render_frame returns
+ * only after its frame has finished). */
+int gpt_copy_accumulation_device(gpt_renderer* renderer, float* device_rgba32f, size_t pixel_count, void* stream);
 /* Per-iteration queue sizes of the last frame: rows of 9 words (rays, 6 material queues,
  * shadow rays, regenerated/terminated paths), as the reference's queues hold them. */
 int gpt_read_queue_log(gpt_renderer* renderer, uint32_t* rows, uint32_t max_rows, uint32_t* row_count);

@@ -290,3 +290,22 @@ def test_rng_offset_shards_match_oracle(gpu_renderer, scene_factory, oracle_scen
     ref = o.render(cam, 48, 48, 16, 10, True, rng_offset=off)
     assert np.array_equal(gpu_renderer.sample_radiance().view(np.uint32), ref["sample_radiance"].view(np.uint32))
     assert np.array_equal(gpu_renderer.queue_log(), ref["queue_log"])
+
+
+def test_copy_accumulation_device_matches_host_read(gpu_renderer, scene_factory):
+    """gpt_copy_accumulation_device (the multi-GPU exchange's source) copies the same float4
+    accumulation gpt_read_accumulation returns, on the renderer's stream or on a caller's stream."""
+    import torch
+    s = scene_factory("cornell")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 40, 30)
+    gpu_renderer.render_frame(cam, 40, 30, 4, 6, True)
+    host = gpu_renderer.accumulation()
+    dev = torch.full((40 * 30, 4), -1.0, dtype=torch.float32, device="cuda")
+    gpu_renderer.copy_accumulation_to(dev)
+    assert np.array_equal(dev.cpu().numpy().view(np.uint32), host.view(np.uint32))
+    dev2 = torch.zeros_like(dev)
+    cur = torch.cuda.current_stream()
+    gpu_renderer.copy_accumulation_to(dev2, stream=cur.cuda_stream)
+    cur.synchronize()
+    assert np.array_equal(dev2.cpu().numpy().view(np.uint32), host.view(np.uint32))
