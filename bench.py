@@ -433,11 +433,10 @@ def precision_section(knobs):
         # the BVH8 frame again for its buffers: per-pixel Kahan sums and the per-sample radiance
         r.render_frame(cam, W, H, spp, depth, True, **knobs)
         kahan = r.accumulation()[:, :3].astype(np.float64)
+        fp64 = r.accumulation_fp64()  # FP64 sums of the same samples, on the device
         rad = r.sample_radiance().reshape(W * H, spp, 3)
-        fp64 = np.zeros((W * H, 3), dtype=np.float64)
         naive = np.zeros((W * H, 3), dtype=np.float32)
-        for k in range(spp):  # sample order, as the resolve kernel sums
-            fp64 += rad[:, k, :].astype(np.float64)
+        for k in range(spp):  # plain FP32 summation in sample order, for comparison
             naive += rad[:, k, :]
         del rad
         ref = fp64 / spp

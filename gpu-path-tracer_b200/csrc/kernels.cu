@@ -1809,6 +1809,27 @@ namespace pt
         }
     }
 
+    // The FP64 reference accumulation of a frame: per pixel, the sum of its per-sample radiance in FP64,
+    // in sample order (the same order the FP32 Kahan resolve uses), for measuring the FP32 accumulation
+    // error on the device. sums: [pixels][3].
+    __global__ void resolve_fp64_kernel(const JobView* jobPtr, double* sums)
+    {
+        const JobView job = *jobPtr;
+        const uint32_t pixels = job.width * job.height;
+        for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < pixels; p += gridDim.x * blockDim.x)
+        {
+            double acc[3] = {0.0, 0.0, 0.0};
+            const uint64_t first = static_cast<uint64_t>(p) * job.spp;
+            for (uint32_t k = 0; k < job.spp; k++)
+            {
+                const uint64_t si = first + k;
+                if (si >= job.totalSamples) break;
+                for (int ch = 0; ch < 3; ch++) acc[ch] += static_cast<double>(job.sampleRadiance[si * 3 + ch]);
+            }
+            for (int ch = 0; ch < 3; ch++) sums[static_cast<size_t>(p) * 3 + ch] = acc[ch];
+        }
+    }
+
     __global__ void clear_kernel(uint32_t* framebuffer, uint32_t n, uint32_t value)  // ClearKernel (Image.cu:7-13)
     {
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) framebuffer[i] = value;
@@ -2207,6 +2228,12 @@ namespace pt
     cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t s)
     {
         resolve_kernel<<<blocks, 128, 0, s>>>(job, accumulation, framebuffer);
+        return cudaGetLastError();
+    }
+
+    cudaError_t launch_resolve_fp64(const JobView* job, double* sums, int blocks, cudaStream_t s)
+    {
+        resolve_fp64_kernel<<<blocks, 128, 0, s>>>(job, sums);
         return cudaGetLastError();
     }
 

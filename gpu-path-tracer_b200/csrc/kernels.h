@@ -58,6 +58,7 @@ namespace pt
     cudaError_t launch_iteration(const IterationLaunch& launch, cudaStream_t stream);
     cudaError_t launch_frame_prologue(const Wavefront& wf, const JobView* job, uint32_t pool, int blocks, cudaStream_t stream);
     cudaError_t launch_resolve(const JobView* job, float4* accumulation, uint32_t* framebuffer, int blocks, cudaStream_t stream);
+    cudaError_t launch_resolve_fp64(const JobView* job, double* sums, int blocks, cudaStream_t stream);
     cudaError_t launch_clear(uint32_t* framebuffer, uint32_t n, uint32_t value, cudaStream_t stream);
     cudaError_t launch_batch_trace(const SceneView& scene, uint32_t root, const float* rays, uint32_t n, uint32_t* cursor, uint32_t* triOut,
                                    float* uvtOut, uint8_t* occOut, int blocks, int threads, uint32_t* errorFlags, cudaStream_t stream,

@@ -1105,6 +1105,23 @@ extern "C"
         return Report(r, pt::CudaStatus("cudaMemcpy", e));
     }
 
+    int gpt_read_accumulation_fp64(gpt_renderer* r, double* out, size_t pixel_count)
+    {
+        if (!r || !out) return GPT_ERR_INVALID_ARGUMENT;
+        if (pixel_count > r->impl->lastPixels_ || !r->impl->lastTotalSamples_) return GPT_ERR_CAPACITY;
+        cudaSetDevice(r->impl->device_);
+        pt::DeviceBuffer sums;
+        pt::Status st = sums.allocate(pixel_count * 3 * sizeof(double));
+        if (!st.ok()) return Report(r, st);
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, r->impl->device_);
+        cudaError_t e = pt::launch_resolve_fp64(r->impl->job_.get<pt::JobView>(), sums.get<double>(), sms * 8, r->impl->stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out, sums.get<void>(), pixel_count * 3 * sizeof(double), cudaMemcpyDeviceToHost, r->impl->stream_);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(r->impl->stream_);
+        return Report(r, pt::CudaStatus("resolve fp64", e));
+    }
+
     int gpt_copy_accumulation_device(gpt_renderer* r, float* dst, size_t pixel_count, void* stream)
     {
         if (!r || !dst) return GPT_ERR_INVALID_ARGUMENT;

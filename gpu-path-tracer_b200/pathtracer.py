@@ -146,6 +146,7 @@ _SIGNATURES = [
     ("gpt_read_accumulation", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_sample_radiance", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
     ("gpt_copy_accumulation_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    ("gpt_read_accumulation_fp64", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t]),
     ("gpt_read_queue_log", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
                                           ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_intersect_closest", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
@@ -322,6 +323,12 @@ class Renderer:
     def accumulation(self) -> np.ndarray:
         out = np.zeros((self.width * self.height, 4), dtype=np.float32)
         self._check(self.L.gpt_read_accumulation(self.h, _ptr(out), self.width * self.height), "gpt_read_accumulation")
+        return out
+
+    def accumulation_fp64(self) -> np.ndarray:
+        """[pixels, 3] float64: the last frame's samples summed per pixel in FP64 on the device."""
+        out = np.zeros((self.width * self.height, 3), dtype=np.float64)
+        self._check(self.L.gpt_read_accumulation_fp64(self.h, _ptr(out), self.width * self.height), "gpt_read_accumulation_fp64")
         return out
 
     def copy_accumulation_to(self, dst_dev, stream=None):

@@ -237,6 +237,10 @@ int gpt_read_sample_radiance(gpt_renderer* renderer, float* rgb, uint64_t sample
  * before returning; else the copy is queued on `stream` after the frame (gpt_render_frame returns
  * only after its frame has finished). */
 int gpt_copy_accumulation_device(gpt_renderer* renderer, float* device_rgba32f, size_t pixel_count, void* stream);
+/* The last frame's FP64 reference accumulation: per pixel, its samples' radiance summed in FP64 on
+ * the device in sample order, [pixels][3] doubles, for measuring the FP32 Kahan accumulation against
+ * it. No counterpart in the reference, which accumulates with float atomics (Common.hpp:8-16). */
+int gpt_read_accumulation_fp64(gpt_renderer* renderer, double* rgb64, size_t pixel_count);
 /* Per-iteration queue sizes of the last frame: rows of 9 words (rays, 6 material queues,
  * shadow rays, regenerated/terminated paths), as the reference's queues hold them. */
 int gpt_read_queue_log(gpt_renderer* renderer, uint32_t* rows, uint32_t max_rows, uint32_t* row_count);

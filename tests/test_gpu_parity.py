@@ -309,3 +309,21 @@ def test_copy_accumulation_device_matches_host_read(gpu_renderer, scene_factory)
     gpu_renderer.copy_accumulation_to(dev2, stream=cur.cuda_stream)
     cur.synchronize()
     assert np.array_equal(dev2.cpu().numpy().view(np.uint32), host.view(np.uint32))
+
+
+def test_fp64_reference_accumulation_on_device(gpu_renderer, scene_factory):
+    """gpt_read_accumulation_fp64 sums every pixel's samples in FP64 in sample order: equal, bit for bit,
+    to the same sum taken on the host from the per-sample radiance; the FP32 Kahan accumulation stays
+    within a few FP32 ulps of it."""
+    s = scene_factory("cornell-all")
+    gpu_renderer.upload_scene(s)
+    cam = scenes.scene_camera(s, 48, 40)
+    gpu_renderer.render_frame(cam, 48, 40, 16, 8, True)
+    fp64 = gpu_renderer.accumulation_fp64()
+    rad = gpu_renderer.sample_radiance().reshape(48 * 40, 16, 3)
+    ref = np.zeros((48 * 40, 3), dtype=np.float64)
+    for k in range(16):
+        ref += rad[:, k, :].astype(np.float64)
+    assert np.array_equal(fp64.view(np.uint64), ref.view(np.uint64))
+    kahan = gpu_renderer.accumulation()[:, :3].astype(np.float64)
+    assert np.all(np.abs(kahan - fp64) <= 4 * np.spacing(np.abs(fp64).astype(np.float32)).astype(np.float64) + 1e-30)
