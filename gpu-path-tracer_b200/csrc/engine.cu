@@ -283,7 +283,6 @@ namespace pt
             PT_TRY(shO_.allocate(P * 16));
             PT_TRY(shD_.allocate(P * 16));
             PT_TRY(shL_.allocate(P * 16));
-            PT_TRY(regen_.allocate(P * 4));
             PT_TRY(regenBits_.allocate((P + 31) / 32 * 4));
             PT_CUDA("cudaMemsetAsync", cudaMemsetAsync(regenBits_.get<void>(), 0, (P + 31) / 32 * 4, stream_));
             PT_TRY(slotT_.allocate(P * 16));
@@ -492,8 +491,7 @@ namespace pt
             w.shO = shO_.get<float4>();
             w.shD = shD_.get<float4>();
             w.shL = shL_.get<float4>();
-            w.regen = regen_.get<uint32_t>();
-            w.regenBits = regenBits_.get<uint32_t>();
+            w.regenBits = regenBits_.get<uint32_t>();  // the engine always regenerates from the bitmap
             w.slotT = slotT_.get<float4>();
             w.slotL = slotL_.get<float4>();
             w.slotSample = slotSample_.get<uint32_t>();
@@ -841,7 +839,7 @@ namespace pt
         JobView* mirror_ = nullptr;
         uint32_t* orderHost_ = nullptr;
         uint32_t* sliceWords_ = nullptr;
-        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regen_, regenBits_, slotT_, slotL_, slotSample_, freeList_;
+        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regenBits_, slotT_, slotL_, slotSample_, freeList_;
         DeviceBuffer counters_, ctl_, jobs_, order_, segments_;
         ScenePack pack_;
         Arena arena_;

@@ -1623,63 +1623,6 @@ namespace pt
         phase_end(ctr, 3);
     }
 
-    // Finished paths write their radiance into their job's ring; planned samples start in the
-    // finished slots first, then in slots popped from the free list; finished slots left over are
-    // pushed onto the free list.
-    __global__ void engine_regen_kernel(Wavefront wf, EngineView ev)
-    {
-        Counters* ctr = wf.ctr;
-        phase_begin(ctr, 3);
-        const uint32_t n = ctr->regenCount;
-        const EngineCtl* e = ev.ctl;
-        const uint32_t launch = e->launchCount;
-        const uint32_t freeCount = e->freeCount;
-        const uint32_t segmentCount = e->segmentCount;
-        const uint32_t nxt = ctr->cur ^ 1u;
-        const uint32_t base = ctr->rayCount[nxt];
-        const uint32_t total = n > launch ? n : launch;
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-        {
-            uint32_t slot = 0;
-            if (k < n)
-            {
-                slot = wf.regen[k];
-                const uint32_t j = __float_as_uint(wf.slotT[slot].w) >> 16;
-                JobView& J = ev.jobs[j];
-                const uint32_t sample = wf.slotSample[slot];
-                const uint32_t pixel = sample / J.spp;
-                const uint32_t pass = sample - pixel * J.spp;
-                const uint32_t r = pass % J.ring;
-                const float4 L = wf.slotL[slot];
-                float* dst = J.sampleRadiance + (static_cast<size_t>(r) * J.pixels + pixel) * 3;
-                dst[0] = L.x;
-                dst[1] = L.y;
-                dst[2] = L.z;
-                agg_increment_keyed(&J.passDone[r], (j << 8) | r);
-            }
-            if (k < launch)
-            {
-                if (k >= n) slot = ev.freeList[freeCount - 1u - (k - n)];
-                uint32_t lo = 0, hi = segmentCount - 1u;
-                while (lo < hi)
-                {
-                    const uint32_t mid = (lo + hi + 1u) >> 1;
-                    if (ev.segments[mid].start <= k) lo = mid;
-                    else hi = mid - 1u;
-                }
-                const LaunchSegment sg = ev.segments[lo];
-                const JobView& J = ev.jobs[sg.job];
-                const uint64_t g = sg.first + (k - sg.start);
-                const uint32_t pass = static_cast<uint32_t>(g / J.pixels);
-                const uint32_t pixel = static_cast<uint32_t>(g - static_cast<uint64_t>(pass) * J.pixels);
-                start_path(J, sg.job, wf, slot, pixel * J.spp + pass, nxt, base + k);
-            }
-            else if (k < n)
-                ev.freeList[freeCount + (k - launch)] = slot;
-        }
-        phase_end(ctr, 3);
-    }
-
     // Folds every job's complete passes, in pass order, into its Kahan accumulator; the job's
     // last fold also writes its tone-mapped RGBA8 image.
     __global__ void fold_kernel(EngineView ev)
@@ -2189,10 +2132,7 @@ namespace pt
         }
         plan_kernel<<<1, 1, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (L.wf.regenBits != nullptr)
-            engine_regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
-        else
-            engine_regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
+        engine_regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         fold_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

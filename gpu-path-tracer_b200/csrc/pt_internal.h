@@ -224,7 +224,7 @@ namespace pt
         float4* shD;
         float4* shL;
         uint32_t* regen;
-        uint32_t* regenBits;      // frame renderer: bit per slot set when its path finished (nullptr: regen queue)
+        uint32_t* regenBits;      // bit per slot set when its path finished (nullptr: the regen queue, frame renderer only)
         float4* slotT;            // throughput xyz, w = bits(depth | delta << 8)
         float4* slotL;            // radiance xyz, w = bits(rng stream position)
         uint32_t* slotSample;
