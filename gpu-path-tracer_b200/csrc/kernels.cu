@@ -1129,9 +1129,12 @@ namespace pt
         return out;
     }
 
-    // One kernel per shading model; grid-stride over the model's queue. A path's job (its depth
-    // limit, NEE switch and Philox offset) comes from its slot metadata, its scene (lights) from
-    // the ray tag; NEE is off in scenes without emitters.
+    // One kernel per shading model; blocks stride over the model's queue, one entry per thread. A
+    // path's job (its depth limit, NEE switch and Philox offset) comes from its slot metadata, its
+    // scene (lights) from the ray tag; NEE is off in scenes without emitters. Each block pushes its
+    // extension rays and its shadow rays with one atomic each, grouped by direction octant: a
+    // traversal warp then takes runs of rays leaving neighbouring surfaces (a block's entries come
+    // from neighbouring hits) in the same octant. Queue order changes no result.
     template <uint32_t MODEL>
     __global__ void __launch_bounds__(128) shade_kernel(SceneView sc, Wavefront wf, const JobView* jobs, const SceneEntry* scenes)
     {
@@ -1141,168 +1144,220 @@ namespace pt
         const uint32_t cur = ctr->cur;
         const uint32_t nxt = cur ^ 1u;
         const uint32_t* queue = wf.matQ[MODEL];
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+        __shared__ uint32_t octCount[16], octBase[16], blockBase[2];
+        for (uint32_t kb = blockIdx.x * blockDim.x; kb < n; kb += gridDim.x * blockDim.x)
         {
-            const uint32_t r = queue[k];
-            const float4 o4 = wf.rayO[cur][r];
-            const float4 d4 = wf.rayD[cur][r];
-            const float4 h4 = wf.hit[r];
-            const uint32_t tag = __float_as_uint(o4.w);
-            const uint32_t slot = tag & kSlotMask;
-            const float3 o = f3(o4), d = f3(d4);
-            const float tHit = h4.w;
-            const uint32_t tri = __float_as_uint(h4.x);
-            const float4 T4 = wf.slotT[slot];
-            float4 L4 = wf.slotL[slot];
-            const uint32_t meta = __float_as_uint(T4.w);
-            const uint32_t depth = meta & 0xFFu;
-            const bool delta = (meta & 0x100u) != 0;
-            const uint32_t jobIndex = meta >> 16;
-            const JobView& job = jobs[jobIndex];
-            const uint32_t limit = __ldg(&job.depthLimit);
-            const uint4 se = __ldg(reinterpret_cast<const uint4*>(scenes) + (tag >> kSlotBits));
-            const LightSet ls{se.y, se.z};
-            const bool nee = __ldg(&job.nee) != 0 && ls.count > 0;
-            const float3 T = f3(T4);
-            uint32_t rngPos = __float_as_uint(L4.w);
-            bool terminated = true;
-            float3 nextDir = f3(0.0f);
-            float3 nextGn = f3(0.0f);
-            Continuation cont{true, 0, f3(0.0f)};
-            bool nextDelta = false;
-            ShadowOut sh;
-            sh.valid = false;
-            float3 hitPos = f3(0.0f);
-
-            if (MODEL == 5)  // Emissive (:882-912)
+            const uint32_t k = kb + threadIdx.x;
+            bool pushRay = false, pushShadow = false;
+            float4 rayOut0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), rayOut1 = rayOut0;
+            float4 shOut0 = rayOut0, shOut1 = rayOut0, shOut2 = rayOut0;
+            if (k < n)
             {
-                if (!(nee && !delta))
+                const uint32_t r = queue[k];
+                const float4 o4 = wf.rayO[cur][r];
+                const float4 d4 = wf.rayD[cur][r];
+                const float4 h4 = wf.hit[r];
+                const uint32_t tag = __float_as_uint(o4.w);
+                const uint32_t slot = tag & kSlotMask;
+                const float3 o = f3(o4), d = f3(d4);
+                const float tHit = h4.w;
+                const uint32_t tri = __float_as_uint(h4.x);
+                const float4 T4 = wf.slotT[slot];
+                float4 L4 = wf.slotL[slot];
+                const uint32_t meta = __float_as_uint(T4.w);
+                const uint32_t depth = meta & 0xFFu;
+                const bool delta = (meta & 0x100u) != 0;
+                const uint32_t jobIndex = meta >> 16;
+                const JobView& job = jobs[jobIndex];
+                const uint32_t limit = __ldg(&job.depthLimit);
+                const uint4 se = __ldg(reinterpret_cast<const uint4*>(scenes) + (tag >> kSlotBits));
+                const LightSet ls{se.y, se.z};
+                const bool nee = __ldg(&job.nee) != 0 && ls.count > 0;
+                const float3 T = f3(T4);
+                uint32_t rngPos = __float_as_uint(L4.w);
+                bool terminated = true;
+                float3 nextDir = f3(0.0f);
+                float3 nextGn = f3(0.0f);
+                Continuation cont{true, 0, f3(0.0f)};
+                bool nextDelta = false;
+                ShadowOut sh;
+                sh.valid = false;
+                float3 hitPos = f3(0.0f);
+
+                if (MODEL == 5)  // Emissive (:882-912)
                 {
-                    // LoadPartiallyResolvedHit (MaterialEval.cu:32-52): material and interpolated uv
-                    const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
-                    const uint32_t mat = __float_as_uint(__ldg(&rec[6].w));
-                    const float b0 = 1.0f - h4.y - h4.z;
-                    float2 uv = make_float2(0.0f, 0.0f);
-                    if (sc.textures != nullptr)
+                    if (!(nee && !delta))
                     {
-                        const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
-                        uv = b0 * make_float2(u01.x, u01.y) + h4.y * make_float2(u01.z, u01.w) + h4.z * make_float2(u2.x, u2.y);
+                        // LoadPartiallyResolvedHit (MaterialEval.cu:32-52): material and interpolated uv
+                        const float4* rec = sc.shading + static_cast<size_t>(tri) * 9;
+                        const uint32_t mat = __float_as_uint(__ldg(&rec[6].w));
+                        const float b0 = 1.0f - h4.y - h4.z;
+                        float2 uv = make_float2(0.0f, 0.0f);
+                        if (sc.textures != nullptr)
+                        {
+                            const float4 u01 = ldg4(rec + 7), u2 = ldg4(rec + 8);
+                            uv = b0 * make_float2(u01.x, u01.y) + h4.y * make_float2(u01.z, u01.w) + h4.z * make_float2(u2.x, u2.y);
+                        }
+                        const float3 em = slot_rgb(sc, mat, 4, uv, sc.materials[mat].emission);
+                        const float3 c = T * em;
+                        L4.x = L4.x + c.x;
+                        L4.y = L4.y + c.y;
+                        L4.z = L4.z + c.z;
                     }
-                    const float3 em = slot_rgb(sc, mat, 4, uv, sc.materials[mat].emission);
-                    const float3 c = T * em;
+                }
+                else if (MODEL == 0)  // Normal (:194-220)
+                {
+                    const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
+                    const float3 c = T * s.normal * 0.5f + 0.5f;
                     L4.x = L4.x + c.x;
                     L4.y = L4.y + c.y;
                     L4.z = L4.z + c.z;
                 }
-            }
-            else if (MODEL == 0)  // Normal (:194-220)
-            {
-                const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
-                const float3 c = T * s.normal * 0.5f + 0.5f;
-                L4.x = L4.x + c.x;
-                L4.y = L4.y + c.y;
-                L4.z = L4.z + c.z;
-            }
-            else
-            {
-                const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
-                hitPos = s.position;
-                nextGn = s.gN;
-                const MaterialDev& m = sc.materials[s.material];
-                const Frame f = shading_frame(sc, s, m);
-                curandStatePhilox4_32_10_t rng;
-                curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + __ldg(&job.rngOffset),
-                            static_cast<unsigned long long>(rngPos), &rng);
-                if (MODEL == 1)  // Diffuse (:311-350, :270-309)
+                else
                 {
-                    const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
-                    const float4 ind = curand_uniform4(&rng);
-                    rngPos += 4;
-                    if (nee)
+                    const Surface s = resolve_hit(sc, o, d, tHit, tri, h4.y, h4.z);
+                    hitPos = s.position;
+                    nextGn = s.gN;
+                    const MaterialDev& m = sc.materials[s.material];
+                    const Frame f = shading_frame(sc, s, m);
+                    curandStatePhilox4_32_10_t rng;
+                    curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + __ldg(&job.rngOffset),
+                                static_cast<unsigned long long>(rngPos), &rng);
+                    if (MODEL == 1)  // Diffuse (:311-350, :270-309)
                     {
-                        const float4 dir4 = curand_uniform4(&rng);
+                        const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
+                        const float4 ind = curand_uniform4(&rng);
                         rngPos += 4;
-                        sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
+                        if (nee)
+                        {
+                            const float4 dir4 = curand_uniform4(&rng);
+                            rngPos += 4;
+                            sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
+                        }
+                        const float3 wi = f.from_local(cosine_hemisphere(make_float2(ind.x, ind.y)));
+                        const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
+                        const float gCos = fmaxf(dot(s.gN, wi), 0.0f);
+                        if (!(cosThetaI <= 0.0f || gCos <= 0.0f))
+                        {
+                            cont = continue_path(depth, T, limit, albedo, ind.z);
+                            terminated = cont.terminated;
+                            nextDir = wi;
+                            nextDelta = false;
+                        }
                     }
-                    const float3 wi = f.from_local(cosine_hemisphere(make_float2(ind.x, ind.y)));
-                    const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
-                    const float gCos = fmaxf(dot(s.gN, wi), 0.0f);
-                    if (!(cosThetaI <= 0.0f || gCos <= 0.0f))
+                    else if (MODEL == 2)  // Mirror (:352-392)
                     {
-                        cont = continue_path(depth, T, limit, albedo, ind.z);
+                        const float3 reflectance = slot_rgb(sc, s.material, 1, s.uv, m.specular);
+                        const float rr = curand_uniform(&rng);
+                        rngPos += 1;
+                        const float3 wi = reflect(d, f.normal);
+                        cont = continue_path(depth, T, limit, reflectance, rr);
                         terminated = cont.terminated;
                         nextDir = wi;
+                        nextDelta = true;
+                    }
+                    else if (MODEL == 3)  // Phong (:544-585)
+                    {
+                        const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
+                        const float3 specular = slot_rgb(sc, s.material, 1, s.uv, m.specular);
+                        const float shininess = slot_scalar(sc, s.material, 2, s.uv, &m.shininess) * (1000.0f - 1.0f) + 1.0f;
+                        const float4 ind = curand_uniform4(&rng);
+                        rngPos += 4;
+                        if (nee) sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(ind), albedo, true, specular, shininess);
+                        const Scatter sc2 = indirect_phong(depth, T, limit, d, s, f, ind, albedo, specular, shininess);
+                        terminated = sc2.terminated;
+                        cont = sc2.c;
+                        nextDir = sc2.direction;
+                        nextDelta = false;
+                    }
+                    else if (MODEL == 4)  // GGX (:838-880)
+                    {
+                        const float3 base = slot_rgb(sc, s.material, 0, s.uv, m.color);
+                        const float3 rma = slot_rgb(sc, s.material, 3, s.uv, m.rma);
+                        const float alpha = fmaxf(rma.x * rma.x, 0.001f);
+                        const float metallic = rma.y;
+                        const float ior = __ldg(&m.ior);
+                        const float4 ind = curand_uniform4(&rng);
+                        rngPos += 4;
+                        if (nee)
+                        {
+                            const float4 dir4 = curand_uniform4(&rng);
+                            rngPos += 4;
+                            sh = direct_ggx(sc, ls, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
+                        }
+                        const Scatter sc2 = indirect_ggx(depth, T, limit, d, s, f, ind, base, alpha, metallic, ior);
+                        terminated = sc2.terminated;
+                        cont = sc2.c;
+                        nextDir = sc2.direction;
                         nextDelta = false;
                     }
                 }
-                else if (MODEL == 2)  // Mirror (:352-392)
+                L4.w = __uint_as_float(rngPos);
+                wf.slotL[slot] = L4;
+                if (sh.valid)
                 {
-                    const float3 reflectance = slot_rgb(sc, s.material, 1, s.uv, m.specular);
-                    const float rr = curand_uniform(&rng);
-                    rngPos += 1;
-                    const float3 wi = reflect(d, f.normal);
-                    cont = continue_path(depth, T, limit, reflectance, rr);
-                    terminated = cont.terminated;
-                    nextDir = wi;
-                    nextDelta = true;
+                    pushShadow = true;
+                    shOut0 = make_float4(sh.origin.x, sh.origin.y, sh.origin.z, __uint_as_float(tag));
+                    shOut1 = make_float4(sh.direction.x, sh.direction.y, sh.direction.z, sh.tMax);
+                    shOut2 = make_float4(sh.radiance.x, sh.radiance.y, sh.radiance.z, 0.0f);
                 }
-                else if (MODEL == 3)  // Phong (:544-585)
+                if (terminated) path_finished(wf, ctr, slot);
+                else
                 {
-                    const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
-                    const float3 specular = slot_rgb(sc, s.material, 1, s.uv, m.specular);
-                    const float shininess = slot_scalar(sc, s.material, 2, s.uv, &m.shininess) * (1000.0f - 1.0f) + 1.0f;
-                    const float4 ind = curand_uniform4(&rng);
-                    rngPos += 4;
-                    if (nee) sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(ind), albedo, true, specular, shininess);
-                    const Scatter sc2 = indirect_phong(depth, T, limit, d, s, f, ind, albedo, specular, shininess);
-                    terminated = sc2.terminated;
-                    cont = sc2.c;
-                    nextDir = sc2.direction;
-                    nextDelta = false;
+                    // SpawnScatteredRay (:148-156)
+                    const float3 origin = o + d * tHit + nextGn * 1e-4f;
+                    wf.slotT[slot] = make_float4(cont.throughput.x, cont.throughput.y, cont.throughput.z,
+                                                 __uint_as_float(pack_meta(cont.depth, nextDelta, jobIndex)));
+                    pushRay = true;
+                    rayOut0 = make_float4(origin.x, origin.y, origin.z, __uint_as_float(tag));
+                    rayOut1 = make_float4(nextDir.x, nextDir.y, nextDir.z, kMaxT);
                 }
-                else if (MODEL == 4)  // GGX (:838-880)
-                {
-                    const float3 base = slot_rgb(sc, s.material, 0, s.uv, m.color);
-                    const float3 rma = slot_rgb(sc, s.material, 3, s.uv, m.rma);
-                    const float alpha = fmaxf(rma.x * rma.x, 0.001f);
-                    const float metallic = rma.y;
-                    const float ior = __ldg(&m.ior);
-                    const float4 ind = curand_uniform4(&rng);
-                    rngPos += 4;
-                    if (nee)
-                    {
-                        const float4 dir4 = curand_uniform4(&rng);
-                        rngPos += 4;
-                        sh = direct_ggx(sc, ls, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
-                    }
-                    const Scatter sc2 = indirect_ggx(depth, T, limit, d, s, f, ind, base, alpha, metallic, ior);
-                    terminated = sc2.terminated;
-                    cont = sc2.c;
-                    nextDir = sc2.direction;
-                    nextDelta = false;
-                }
+                (void)hitPos;
             }
-            L4.w = __uint_as_float(rngPos);
-            wf.slotL[slot] = L4;
-            if (sh.valid)
+            // the block's extension rays and shadow rays, each grouped by direction octant, take one
+            // range of their queue each
+            if (threadIdx.x < 16) octCount[threadIdx.x] = 0;
+            __syncthreads();
+            uint32_t oct = 0, rank = 0, soct = 0, srank = 0;
+            if (pushRay)
             {
-                const uint32_t pos = agg_push(&ctr->shadowCount);
-                wf.shO[pos] = make_float4(sh.origin.x, sh.origin.y, sh.origin.z, __uint_as_float(tag));
-                wf.shD[pos] = make_float4(sh.direction.x, sh.direction.y, sh.direction.z, sh.tMax);
-                wf.shL[pos] = make_float4(sh.radiance.x, sh.radiance.y, sh.radiance.z, 0.0f);
+                oct = (rayOut1.x < 0.0f ? 1u : 0u) | (rayOut1.y < 0.0f ? 2u : 0u) | (rayOut1.z < 0.0f ? 4u : 0u);
+                rank = atomicAdd(&octCount[oct], 1u);
             }
-            if (terminated) path_finished(wf, ctr, slot);
-            else
+            if (pushShadow)
             {
-                // SpawnScatteredRay (:148-156)
-                const float3 origin = o + d * tHit + nextGn * 1e-4f;
-                wf.slotT[slot] = make_float4(cont.throughput.x, cont.throughput.y, cont.throughput.z,
-                                             __uint_as_float(pack_meta(cont.depth, nextDelta, jobIndex)));
-                const uint32_t pos = agg_push(&ctr->rayCount[nxt]);
-                wf.rayO[nxt][pos] = make_float4(origin.x, origin.y, origin.z, __uint_as_float(tag));
-                wf.rayD[nxt][pos] = make_float4(nextDir.x, nextDir.y, nextDir.z, kMaxT);
+                soct = 8u | (shOut1.x < 0.0f ? 1u : 0u) | (shOut1.y < 0.0f ? 2u : 0u) | (shOut1.z < 0.0f ? 4u : 0u);
+                srank = atomicAdd(&octCount[soct], 1u);
             }
-            (void)hitPos;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                uint32_t total = 0, stotal = 0;
+                for (int q = 0; q < 8; q++)
+                {
+                    octBase[q] = total;
+                    total += octCount[q];
+                    octBase[8 + q] = stotal;
+                    stotal += octCount[8 + q];
+                }
+                blockBase[0] = total ? atomicAdd(&ctr->rayCount[nxt], total) : 0u;
+                blockBase[1] = stotal ? atomicAdd(&ctr->shadowCount, stotal) : 0u;
+            }
+            __syncthreads();
+            if (pushRay)
+            {
+                const uint32_t pos = blockBase[0] + octBase[oct] + rank;
+                wf.rayO[nxt][pos] = rayOut0;
+                wf.rayD[nxt][pos] = rayOut1;
+            }
+            if (pushShadow)
+            {
+                const uint32_t pos = blockBase[1] + octBase[soct] + srank;
+                wf.shO[pos] = shOut0;
+                wf.shD[pos] = shOut1;
+                wf.shL[pos] = shOut2;
+            }
+            __syncthreads();
         }
         phase_end(ctr, 1);
     }
