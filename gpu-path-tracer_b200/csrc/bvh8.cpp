@@ -527,7 +527,7 @@ namespace pt
             result.depth2 = f.maxDepth;
         }
         result.order = b.idx;
-        result.tris.resize(static_cast<size_t>(n) * 3);
+        result.tris.assign(static_cast<size_t>(n) * kTriangleVec4, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
         for (uint32_t j = 0; j < n; j++)
         {
             const uint32_t t = b.idx[j];
@@ -538,9 +538,9 @@ namespace pt
             float of, mf;
             std::memcpy(&of, &ob, 4);
             std::memcpy(&mf, &mb, 4);
-            result.tris[static_cast<size_t>(j) * 3 + 0] = make_float4(p0[0], p0[1], p0[2], of);
-            result.tris[static_cast<size_t>(j) * 3 + 1] = make_float4(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2], mf);
-            result.tris[static_cast<size_t>(j) * 3 + 2] = make_float4(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2], 0.0f);
+            result.tris[static_cast<size_t>(j) * kTriangleVec4 + 0] = make_float4(p0[0], p0[1], p0[2], of);
+            result.tris[static_cast<size_t>(j) * kTriangleVec4 + 1] = make_float4(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2], mf);
+            result.tris[static_cast<size_t>(j) * kTriangleVec4 + 2] = make_float4(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2], 0.0f);
         }
         return result;
     }

@@ -10,7 +10,7 @@ namespace pt
     struct Bvh8
     {
         std::vector<Node8> nodes;
-        std::vector<float4> tris;      // 3 per triangle, leaf order: (v0, orig), (e1, model), (e2, 0)
+        std::vector<float4> tris;      // kTriangleVec4 per triangle, leaf order: (v0, orig), (e1, model), (e2, 0), 0
         std::vector<uint32_t> order;   // leaf position -> input triangle index
         uint32_t depth = 0;            // levels of the wide tree
         std::vector<Node2> nodes2;     // the binary tree the BVH8 is collapsed from, FP32 boxes (same leaf order)

@@ -140,14 +140,14 @@ namespace pt
                 return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^24 triangles");
             DeviceBuffer nn, nt, ns, nm, nl, nb, ntex, ne;
             PT_TRY(Grow(nn, p.nodes, size_t(p.nodeCount) * sizeof(Node8), s.nodes, size_t(s.nodeCount) * sizeof(Node8), st));
-            PT_TRY(Grow(nt, p.tris, size_t(p.triangleCount) * 48, s.tris, size_t(s.triangleCount) * 48, st));
+            PT_TRY(Grow(nt, p.tris, size_t(p.triangleCount) * kTriangleVec4 * 16, s.tris, size_t(s.triangleCount) * kTriangleVec4 * 16, st));
             PT_TRY(Grow(ns, p.shading, size_t(p.triangleCount) * 144, s.shading, size_t(s.triangleCount) * 144, st));
             PT_TRY(Grow(nm, p.materials, size_t(p.materialCount) * sizeof(MaterialDev), s.materials, size_t(s.materialCount) * sizeof(MaterialDev), st));
             PT_TRY(Grow(nl, p.lights, size_t(p.lightCount) * 112, s.lights, size_t(s.lightCount) * 112, st));
             PT_TRY(Grow(nb, p.bins, size_t(p.lightCount) * 16, s.bins, size_t(s.lightCount) * 16, st));
             PT_CUDA("rebase nodes", launch_rebase_nodes(nn.get<Node8>() + p.nodeCount, s.nodeCount, p.nodeCount, p.triangleCount, st));
-            uint32_t* triWords = reinterpret_cast<uint32_t*>(nt.get<float4>() + size_t(p.triangleCount) * 3);
-            PT_CUDA("rebase triangles", launch_rebase_field(triWords + 3, s.triangleCount, 12, p.triangleCount, false, st));
+            uint32_t* triWords = reinterpret_cast<uint32_t*>(nt.get<float4>() + size_t(p.triangleCount) * kTriangleVec4);
+            PT_CUDA("rebase triangles", launch_rebase_field(triWords + 3, s.triangleCount, kTriangleVec4 * 4, p.triangleCount, false, st));
             uint32_t* shadeWords = reinterpret_cast<uint32_t*>(ns.get<float4>() + size_t(p.triangleCount) * 9);
             PT_CUDA("rebase shading", launch_rebase_field(shadeWords + 27, s.triangleCount, 36, p.materialCount, false, st));
             uint32_t* lightWords = reinterpret_cast<uint32_t*>(nl.get<float4>() + size_t(p.lightCount) * 7);

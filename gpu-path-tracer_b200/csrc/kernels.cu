@@ -71,6 +71,14 @@ namespace pt
 
     __device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
     __device__ __forceinline__ uint4 ldg4(const uint4* p) { return __ldg(p); }
+    // 32 read-only bytes in one 256-bit load (sm_100); p must be 32-byte aligned. Halves the load
+    // instructions of a node visit and of a triangle test against 16-byte loads.
+    __device__ __forceinline__ void ldg8(const uint4* p, uint4& a, uint4& b)
+    {
+        asm("ld.global.nc.v8.u32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+            : "l"(p));
+    }
 
     // ------------------------------------------------------------------ traversal
     // Registers of a ray in flight. Values a traversal step reads rarely live in the thread's slot
@@ -112,8 +120,12 @@ namespace pt
         const float3 d = cold.direction();
         for (uint32_t k = 0; k < count; k++)
         {
-            const float4* tp = sc.tris + static_cast<size_t>(first + k) * 3;
-            const float4 a = ldg4(tp), b = ldg4(tp + 1), c = ldg4(tp + 2);
+            const uint4* tp = reinterpret_cast<const uint4*>(sc.tris) + static_cast<size_t>(first + k) * kTriangleVec4;
+            uint4 ua, ub;
+            ldg8(tp, ua, ub);
+            const float4 a = make_float4(__uint_as_float(ua.x), __uint_as_float(ua.y), __uint_as_float(ua.z), __uint_as_float(ua.w));
+            const float4 b = make_float4(__uint_as_float(ub.x), __uint_as_float(ub.y), __uint_as_float(ub.z), __uint_as_float(ub.w));
+            const float4 c = ldg4(reinterpret_cast<const float4*>(tp + 2));
             float t, u, v;
             if (!intersect_triangle(a, b, c, st.ray.o, d, t, u, v)) continue;
             if (ANY)
@@ -257,7 +269,9 @@ namespace pt
         }
         const uint4* nw = sc.nodes[node].w;
         work += kVisit;
-        const uint4 w0 = ldg4(nw + 0), w1 = ldg4(nw + 1), w2 = ldg4(nw + 2), w3 = ldg4(nw + 3);
+        uint4 w0, w1, w2, w3;
+        ldg8(nw, w0, w1);
+        ldg8(nw + 2, w2, w3);
         const uint32_t hitSlots = intersect_children(w0, w1, w2, w3, st.ray, FIXED ? kMinT : st.ray.tmin, st.hitT);
         const uint32_t innerSlots = hitSlots & (w0.w >> 24);
         uint32_t leafOrder = permute_mask(hitSlots & ~(w0.w >> 24), st.ray.oct);

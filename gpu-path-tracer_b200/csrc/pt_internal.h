@@ -2,7 +2,8 @@
 //
 // HBM layout (all structure-of-arrays, 16-byte vector records, one CUDA allocation each):
 //   BVH8 node        128 B  (Node8 below)           scene-resident
-//   triangle (MT)     48 B  v0|orig, e1|model, e2     leaf order, scene-resident
+//   triangle (MT)     64 B  v0|orig, e1|model, e2, 0  leaf order, scene-resident (32-byte aligned:
+//                           v0 and e1 in one 256-bit load, e2 in a 128-bit one)
 //   triangle shading 144 B  3 normals, 3 tangents, gN|material, uvs (Triangle.hpp:24-38 layout), input order
 //   light           112 B   v0|index, e1|area, e2, gN, emission, uv0|uvE1, uvE2|material
 //   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14)
@@ -34,6 +35,7 @@ namespace pt
     constexpr uint32_t kMaxPool = 1u << kSlotBits;
     constexpr uint32_t kMaxScenes = 256;
     constexpr uint32_t kMaxTriangles = 1u << 24;  // leaf references hold 24-bit triangle positions
+    constexpr uint32_t kTriangleVec4 = 4;         // 16-byte words per traversal triangle record (64 B)
     constexpr uint32_t kMaxJobs = 65536;
     constexpr uint32_t kMaxRing = 256;
 
@@ -101,7 +103,7 @@ namespace pt
     struct SceneView
     {
         const Node8* nodes;
-        const float4* tris;       // 3 per triangle, leaf order
+        const float4* tris;       // kTriangleVec4 per triangle, leaf order
         const float4* shading;    // 9 per triangle, input order
         const MaterialDev* materials;
         const MaterialTextures* textures;  // per material, nullptr when the scene has no image textures
