@@ -2,7 +2,10 @@
 //
 // Replaces the reference's median-split binary BVH (Core/Source/Graphics/Cuda/Bvh/HostBvh.cpp:22-100)
 // and its DFS flattening to 40-byte nodes (Core/Source/Graphics/Cuda/Bvh/DeviceBvh.cpp:7-52).
-//  1. Binary BVH by binned SAH (16 bins, all three axes), leaves of at most 4 triangles.
+//  1. Binary BVH by binned SAH (32 bins, all three axes), one triangle per leaf: the 8-wide node's
+//     quantised box test then culls single triangles, which costs less than their triangle tests
+//     (on a 1.3M-triangle frame, leaves of up to 4 triangles took 3.46 triangle tests and 7.84 node
+//     visits per closest-hit ray; single-triangle leaves take 2.70 and 8.23, and the frame is 2% faster).
 //  2. Collapse to 8-wide: a wide node takes the two binary children of its binary node and keeps
 //     opening the child of largest surface area until it has 8 children.
 //  3. Child slots are assigned by octant (greedy on dot(child centre - node centre, octant
@@ -62,8 +65,8 @@ namespace pt
             bool leaf() const { return left == kInvalid; }
         };
 
-        constexpr int kBins = 16;
-        constexpr uint32_t kMaxLeaf = 4;
+        constexpr int kBins = 32;
+        constexpr uint32_t kMaxLeaf = 1;
         constexpr float kTraversalCost = 1.2f;
 
         struct BinaryBuilder

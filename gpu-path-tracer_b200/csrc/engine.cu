@@ -554,6 +554,7 @@ namespace pt
             L.refill = refill_;
             L.refillShadow = refillShadow_;
             L.shadeBlocks = sms * 8;
+            L.sms = sms;
             L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             const cudaError_t le = launch_engine_iteration(L, stream_);

@@ -2107,17 +2107,32 @@ namespace pt
         return sms * perSm;
     }
 
-    static cudaError_t launch_shade(uint32_t m, int blocks, const SceneView& sc, const Wavefront& wf, const JobView* jobs,
+    // Resident 128-thread blocks per SM of shade_kernel<M> (its registers decide: 32 to 96 per thread),
+    // at most 8. The shading loop strides over its queue by the grid, so a grid larger than what is
+    // resident at once leaves the blocks that start late with a full share of the work.
+    template <uint32_t M>
+    static int shade_blocks_per_sm()
+    {
+        static const int perSm = []
+        {
+            int b = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, shade_kernel<M>, 128, 0) != cudaSuccess) b = 8;
+            return b < 1 ? 1 : (b > 8 ? 8 : b);
+        }();
+        return perSm;
+    }
+
+    static cudaError_t launch_shade(uint32_t m, int sms, const SceneView& sc, const Wavefront& wf, const JobView* jobs,
                                     const SceneEntry* scenes, cudaStream_t s)
     {
         switch (m)
         {
-            case 0: shade_kernel<0><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
-            case 1: shade_kernel<1><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
-            case 2: shade_kernel<2><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
-            case 3: shade_kernel<3><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
-            case 4: shade_kernel<4><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
-            default: shade_kernel<5><<<blocks, 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 0: shade_kernel<0><<<sms * shade_blocks_per_sm<0>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 1: shade_kernel<1><<<sms * shade_blocks_per_sm<1>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 2: shade_kernel<2><<<sms * shade_blocks_per_sm<2>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 3: shade_kernel<3><<<sms * shade_blocks_per_sm<3>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            case 4: shade_kernel<4><<<sms * shade_blocks_per_sm<4>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
+            default: shade_kernel<5><<<sms * shade_blocks_per_sm<5>(), 128, 0, s>>>(sc, wf, jobs, scenes); break;
         }
         return cudaGetLastError();
     }
@@ -2144,7 +2159,7 @@ namespace pt
             {
                 if (!L.modelPresent[m]) continue;
                 if ((e = cudaStreamWaitEvent(L.shadeStreams[m], L.shadeFork, 0)) != cudaSuccess) return e;
-                if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, L.shadeStreams[m])) != cudaSuccess) return e;
+                if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.job, L.scenes, L.shadeStreams[m])) != cudaSuccess) return e;
                 if ((e = cudaEventRecord(L.shadeJoin[m], L.shadeStreams[m])) != cudaSuccess) return e;
                 if ((e = cudaStreamWaitEvent(s, L.shadeJoin[m], 0)) != cudaSuccess) return e;
             }
@@ -2154,7 +2169,7 @@ namespace pt
             for (uint32_t m = 0; m < kModelCount; m++)
             {
                 if (!L.modelPresent[m]) continue;
-                if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
+                if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
             }
         }
         if (L.nee && L.scene.lightCount > 0)
@@ -2191,7 +2206,7 @@ namespace pt
         for (uint32_t m = 0; m < kModelCount; m++)
         {
             if (!L.modelPresent[m]) continue;
-            if ((e = launch_shade(m, L.shadeBlocks, L.scene, L.wf, L.ev.jobs, L.ev.scenes, s)) != cudaSuccess) return e;
+            if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.ev.jobs, L.ev.scenes, s)) != cudaSuccess) return e;
         }
         if (L.anyLights)
         {

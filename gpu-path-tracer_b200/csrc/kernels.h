@@ -20,7 +20,8 @@ namespace pt
         uint32_t refill;
         uint32_t refillShadow;     // the same threshold for the shadow-ray (any-hit) traversal
         int occupancy;             // traversal kernel variant: 1, 10 or 12 resident blocks per SM targeted
-        int shadeBlocks;
+        int shadeBlocks;           // grid of the 256-thread bookkeeping kernels (regeneration, folding)
+        int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
         uint32_t bvhFormat;        // kBvh8Quantised or kBvh2Fp32 (scene.nodes2 must be present)
         cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
@@ -46,7 +47,8 @@ namespace pt
         uint32_t refill;
         uint32_t refillShadow;
         int occupancy;
-        int shadeBlocks;
+        int shadeBlocks;           // grid of the 256-thread bookkeeping kernels (regeneration, folding)
+        int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;
     };
 

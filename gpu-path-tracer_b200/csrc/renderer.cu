@@ -495,6 +495,7 @@ namespace pt
                 L.shadeStreams[m] = shadeStreams_[m];
             }
             L.shadeBlocks = sms * 8;
+            L.sms = sms;
             L.graphLoop = true;
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             le = launch_iteration(L, stream_);
@@ -543,6 +544,7 @@ namespace pt
                 L.shadeStreams[m] = shadeStreams_[m];
             }
             L.shadeBlocks = sms * 8;
+            L.sms = sms;
             L.graphLoop = false;
             L.traceStart = traceStart_;
             L.traceStop = traceStop_;
