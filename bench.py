@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--no-reference-build", action="store_true",
                     help="skip timing the reference's own kernels (oracle/_ref) on the same frame")
     ap.add_argument("--serve-rates", default="20,50,100", help="Poisson arrival rates (jobs/s) of the serving section")
+    ap.add_argument("--serve-pool", type=int, default=1 << 23,
+                    help="most path slots of the serving section's servers (latency of small jobs grows with the pool)")
     return ap.parse_args()
 
 
@@ -364,8 +366,10 @@ def batched_section(knobs):
     return out
 
 
-def serving_section(knobs, rates, n_jobs):
-    """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time."""
+def serving_section(knobs, rates, n_jobs, max_pool):
+    """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time.
+    Both servers hold at most max_pool path slots: an iteration's time grows with the slots in flight,
+    and a small job needs a fixed number of iterations, so its latency grows with the pool."""
     import pathtracer
     import scenes
     import workloads
@@ -376,8 +380,10 @@ def serving_section(knobs, rates, n_jobs):
                      "seeded orbit cameras; admission: 64 B per in-flight path + framebuffers within the budget",
            "latency": "server done_s - submit_s per job (submission at the scheduled arrival time)"}
     warm = [workloads.Job(n, 64, 64, 4, 8, scenes.scene_camera(s, 64, 64)) for n, s in resident.items()]
+    pool = min(knobs["pool_size"], max_pool)
+    out["pool_size"] = pool
     for mode, active in (("served", 0), ("plain", 1)):
-        srv = pathtracer.Server(0, pool_size=knobs["pool_size"], max_active_jobs=active, hbm_budget_bytes=16 << 30,
+        srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30,
                                 **_server_knobs(knobs))
         res = {}
         try:
@@ -638,7 +644,7 @@ def b200_arm(args):
         line["batched"] = run_section("batched", lambda: batched_section(knobs))
     if "serving" in sections:
         rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
-        line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs))
+        line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs, args.serve_pool))
     if "precision" in sections:
         pr = run_section("precision", lambda: precision_section(knobs))
         line["precision"] = pr

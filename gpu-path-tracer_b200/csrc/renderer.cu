@@ -654,81 +654,92 @@ namespace pt
             return Status::Ok();
         }
 
-        // Measured choice of the frame's tuning knobs for a workload: every candidate renders the
-        // same reduced frame (the whole image at min(spp, 4) samples per pixel, so all of the scene
-        // is represented) twice, and the fastest device time wins. Results do not depend on the
-        // knobs; only speed does.
+        // Measured choice of the frame's tuning knobs for a workload: every candidate renders a reduced
+        // frame (the whole image, so all of the scene is represented) twice, and the lowest device time
+        // per sample wins. A pool candidate's trial frame has the smallest square sample count per pixel
+        // (at least 4, at most the frame's own) that gives two pool-fulls of samples, so the pool stays
+        // full for most of the trial as it does in the real frame. Results do not depend on the knobs;
+        // only speed does.
         Status Autotune(const gpt_device_camera& cam, const gpt_render_settings& base, gpt_render_settings& best, float& bestMs,
                         uint32_t& tried)
         {
             if (!scene_) return Status::Err(GPT_ERR_NO_SCENE, "No scene has been uploaded");
             gpt_render_settings trial = base;
-            trial.samples_per_pixel = std::min<uint32_t>(std::max(base.samples_per_pixel, 1u), 4u);
             trial.max_samples = 0;
             trial.loop_mode = GPT_LOOP_GRAPH;
             const uint64_t pixels = static_cast<uint64_t>(std::max(base.width, 1u)) * std::max(base.height, 1u);
-            const uint32_t pools[] = {1u << 20, 2u << 20, 4u << 20, 8u << 20};
+            const uint32_t spp = std::max(base.samples_per_pixel, 1u);
+            const uint32_t pools[] = {1u << 20, 2u << 20, 4u << 20, 8u << 20, 16u << 20};
             const uint32_t occupancies[] = {1u, 10u, 12u};
             const uint32_t refills[] = {8u, 16u};
             const uint32_t blocks[] = {64u, 128u};
+            const auto trialSpp = [&](uint32_t pool)
+            {
+                uint32_t side = 2;
+                while (side * side < spp && static_cast<uint64_t>(side) * side * pixels < 2ull * pool) side++;
+                return std::min(side * side, spp);
+            };
+            const auto perSample = [&](const gpt_render_settings& t, float& score) -> Status
+            {
+                score = 1e30f;
+                for (int rep = 0; rep < 2; rep++)
+                {
+                    gpt_frame_stats st{};
+                    PT_TRY(RenderFrame(cam, t, &st, false));
+                    if (rep && st.samples) score = static_cast<float>(static_cast<double>(st.device_ms) / static_cast<double>(st.samples));
+                }
+                return Status::Ok();
+            };
             best = base;
-            bestMs = 1e30f;
+            bestMs = 1e30f;  // device ms per sample of the best trial until the end, then per frame of the base settings
             tried = 0;
             // the frame's own sample count bounds the useful pool size
-            const uint64_t frameSamples = pixels * std::max(base.samples_per_pixel, 1u);
+            const uint64_t frameSamples = pixels * spp;
             for (uint32_t pool : pools)
             {
                 if (pool > 2 * frameSamples && pool != pools[0]) continue;
+                trial.samples_per_pixel = trialSpp(pool);
                 for (uint32_t occ : occupancies)
                     for (uint32_t refill : refills)
                         for (uint32_t tb : blocks)
+                        {
+                            trial.pool_size = pool;
+                            trial.trace_occupancy = occ;
+                            trial.trace_refill = refill;
+                            trial.trace_block = tb;
+                            float score = 1e30f;
+                            PT_TRY(perSample(trial, score));
+                            tried++;
+                            if (score < bestMs)
                             {
-                                trial.pool_size = pool;
-                                trial.trace_occupancy = occ;
-                                trial.trace_refill = refill;
-                                trial.trace_block = tb;
-                                float ms = 1e30f;
-                                for (int rep = 0; rep < 2; rep++)
-                                {
-                                    gpt_frame_stats st{};
-                                    PT_TRY(RenderFrame(cam, trial, &st, false));
-                                    if (rep) ms = st.device_ms;
-                                }
-                                tried++;
-                                if (ms < bestMs)
-                                {
-                                    bestMs = ms;
-                                    best = base;
-                                    best.pool_size = pool;
-                                    best.trace_occupancy = occ;
-                                    best.trace_refill = refill;
-                                    best.trace_block = tb;
-                                }
+                                bestMs = score;
+                                best = base;
+                                best.pool_size = pool;
+                                best.trace_occupancy = occ;
+                                best.trace_refill = refill;
+                                best.trace_block = tb;
                             }
+                        }
             }
             // shadow rays tune their own refill threshold with the other knobs fixed
             const uint32_t closestRefill = best.trace_refill & 0xFFu;
             for (uint32_t shadowRefill : {2u, 4u, 8u, 16u})
             {
                 trial = best;
-                trial.samples_per_pixel = std::min<uint32_t>(std::max(base.samples_per_pixel, 1u), 4u);
+                trial.samples_per_pixel = trialSpp(best.pool_size);
                 trial.max_samples = 0;
                 trial.loop_mode = GPT_LOOP_GRAPH;
                 trial.trace_refill = closestRefill | (shadowRefill << 8);
-                float ms = 1e30f;
-                for (int rep = 0; rep < 2; rep++)
-                {
-                    gpt_frame_stats st{};
-                    PT_TRY(RenderFrame(cam, trial, &st, false));
-                    if (rep) ms = st.device_ms;
-                }
+                float score = 1e30f;
+                PT_TRY(perSample(trial, score));
                 tried++;
-                if (ms < bestMs)
+                if (score < bestMs)
                 {
-                    bestMs = ms;
+                    bestMs = score;
                     best.trace_refill = trial.trace_refill;
                 }
             }
+            bestMs = static_cast<float>(static_cast<double>(bestMs) * static_cast<double>(frameSamples));
             return Status::Ok();
         }
 

@@ -218,9 +218,11 @@ int gpt_render_frame(gpt_renderer* renderer, const gpt_device_camera* camera,
                      const gpt_render_settings* settings, gpt_frame_stats* stats);
 /*
  * Autotuner: measures the frame's tuning knobs (pool_size = path slots and queue capacities,
- * trace_occupancy, trace_refill, trace_block) on a reduced frame of the same workload (whole
- * image, min(spp, 4) samples per pixel) and writes the fastest combination into *best (the other
- * fields copied from *base). Results of a frame do not depend on these knobs, only its speed.
+ * trace_occupancy, trace_refill, trace_block) on reduced frames of the same workload (whole
+ * image; per pool candidate, the smallest square spp of at least 4, and at most the frame's spp,
+ * that holds two pool-fulls of samples) and writes the combination with the lowest device time
+ * per sample into *best (the other fields copied from *base); *best_ms is that time scaled to the
+ * full frame. Results of a frame do not depend on these knobs, only its speed.
  * No counterpart in the reference, whose launch shapes are compile-time constants
  * (Kernels/LaunchUtils.cuh:7-17, PathTracerDefaults.hpp:9).
  */

@@ -267,7 +267,7 @@ def test_autotune_returns_valid_knobs_and_results_do_not_change(gpu_renderer, sc
     cam = scenes.scene_camera(s, 128, 96)
     knobs = gpu_renderer.autotune(cam, 128, 96, 16, 12, True)
     assert knobs["candidates"] >= 12 and knobs["trial_ms"] > 0
-    assert knobs["pool_size"] in (1 << 20, 2 << 20, 4 << 20, 8 << 20)
+    assert knobs["pool_size"] in (1 << 20, 2 << 20, 4 << 20, 8 << 20, 16 << 20)
     assert knobs["trace_occupancy"] in (1, 10, 12) and knobs["trace_block"] in (64, 128)
     assert knobs["trace_refill"] & 0xFF in (8, 16) and knobs["trace_refill"] >> 8 in (0, 2, 4, 8, 16)
     gpu_renderer.render_frame(cam, 128, 96, 16, 12, True)
