@@ -6,8 +6,15 @@
 //     quantised box test then culls single triangles, which costs less than their triangle tests
 //     (on a 1.3M-triangle frame, leaves of up to 4 triangles took 3.46 triangle tests and 7.84 node
 //     visits per closest-hit ray; single-triangle leaves take 2.70 and 8.23, and the frame is 2% faster).
-//  2. Collapse to 8-wide: a wide node takes the two binary children of its binary node and keeps
-//     opening the child of largest surface area until it has 8 children.
+//  2. Collapse to 8-wide by the surface-area-optimal distribution of binary subtrees over child slots
+//     (the dynamic programme of Ylitie, Karras and Laine, "Efficient Incoherent Ray Traversal on
+//     GPUs Through Compressed Wide BVHs", HPG 2017): for every binary node and every slot budget
+//     i = 1..8, the least expected cost of its subtree in at most i slots of the parent wide node,
+//     where a wide node costs its area x kNodeCost and a leaf its area x its triangle count. On the
+//     1.3M-triangle frame this gives 256K instead of 422K nodes (6.1 instead of 4.1 children per node)
+//     and 7.91 instead of 8.23 node visits per closest-hit ray against greedily opening the child of
+//     largest area, and a 2.7% faster frame. Leaves stay single triangles: letting the programme
+//     choose leaves of 2 or 3 triangles gave fewer nodes but more triangle tests and slower frames.
 //  3. Child slots are assigned by octant (greedy on dot(child centre - node centre, octant
 //     direction)) so a ray visiting slot i ^ octant(ray) goes roughly front to back.
 //  4. Child boxes are padded (1e-5 of their largest extent, plus a relative 1e-7 of their
@@ -205,9 +212,96 @@ namespace pt
             }
         };
 
+        constexpr float kNodeCost = 2.0f;     // wide-node visit against one triangle test
+        constexpr uint32_t kWideLeafMax = 1;   // most triangles in one leaf slot of a wide node
+
+        // Surface-area-optimal distribution of binary subtrees over the 8 child slots of wide nodes.
+        struct CollapsePlan
+        {
+            const BinaryBuilder& bin;
+            std::vector<float> cost;     // [node * 8 + i - 1]: least cost of the subtree in at most i slots
+            std::vector<uint8_t> how;    // i == 1: 0 leaf, 1 wide node; i > 1: 0 = as in i - 1 slots, k = k slots to the left child
+            std::vector<uint8_t> split;  // slots of the left child in the node's own wide node
+
+            void plan(uint32_t n)
+            {
+                const BNode& b = bin.nodes[n];
+                const float A = b.box.area();
+                float* C = &cost[static_cast<size_t>(n) * 8];
+                uint8_t* H = &how[static_cast<size_t>(n) * 8];
+                if (b.leaf())
+                {
+                    for (int i = 0; i < 8; i++)
+                    {
+                        C[i] = A * static_cast<float>(b.count);
+                        H[i] = 0;
+                    }
+                    return;
+                }
+                plan(b.left);
+                plan(b.right);
+                const float* L = &cost[static_cast<size_t>(b.left) * 8];
+                const float* R = &cost[static_cast<size_t>(b.right) * 8];
+                float D[9];
+                uint8_t Dk[9] = {};
+                for (int j = 2; j <= 8; j++)
+                {
+                    D[j] = FLT_MAX;
+                    for (int k = 1; k < j; k++)
+                    {
+                        const float v = L[k - 1] + R[j - k - 1];
+                        if (v < D[j])
+                        {
+                            D[j] = v;
+                            Dk[j] = static_cast<uint8_t>(k);
+                        }
+                    }
+                }
+                split[n] = Dk[8];
+                const float nodeCost = A * kNodeCost + D[8];
+                const float leafCost = b.count <= kWideLeafMax ? A * static_cast<float>(b.count) : FLT_MAX;
+                C[0] = std::min(leafCost, nodeCost);
+                H[0] = leafCost <= nodeCost ? 0 : 1;
+                for (int i = 2; i <= 8; i++)
+                {
+                    if (D[i] < C[i - 2])
+                    {
+                        C[i - 1] = D[i];
+                        H[i - 1] = Dk[i];
+                    }
+                    else
+                    {
+                        C[i - 1] = C[i - 2];
+                        H[i - 1] = 0;
+                    }
+                }
+            }
+
+            // The children that node n contributes with i slots: binary nodes, each a leaf slot or a wide node.
+            void collect(uint32_t n, int i, std::vector<uint32_t>& kids, std::vector<uint8_t>& leaf) const
+            {
+                const uint8_t h = how[static_cast<size_t>(n) * 8 + i - 1];
+                if (i == 1)
+                {
+                    kids.push_back(n);
+                    leaf.push_back(h == 0 ? 1 : 0);
+                    return;
+                }
+                if (h == 0)
+                {
+                    collect(n, i - 1, kids, leaf);
+                    return;
+                }
+                const BNode& b = bin.nodes[n];
+                collect(b.left, h, kids, leaf);
+                collect(b.right, i - h, kids, leaf);
+            }
+        };
+
         struct WideBuilder
         {
             const BinaryBuilder& bin;
+            const CollapsePlan& plan;
             std::vector<Node8> out;
             uint32_t maxDepth = 0;
 
@@ -234,33 +328,18 @@ namespace pt
                 out.push_back(Node8{});
                 // children list
                 std::vector<uint32_t> kids;
+                std::vector<uint8_t> kidLeaf;
                 const BNode& root = bin.nodes[bnode];
                 if (root.leaf())
+                {
                     kids.push_back(bnode);
+                    kidLeaf.push_back(1);
+                }
                 else
                 {
-                    kids.push_back(root.left);
-                    kids.push_back(root.right);
-                    while (kids.size() < 8)
-                    {
-                        int best = -1;
-                        float bestArea = -1.0f;
-                        for (size_t i = 0; i < kids.size(); i++)
-                        {
-                            const BNode& c = bin.nodes[kids[i]];
-                            if (c.leaf()) continue;
-                            float a = c.box.area();
-                            if (a > bestArea)
-                            {
-                                bestArea = a;
-                                best = static_cast<int>(i);
-                            }
-                        }
-                        if (best < 0) break;
-                        const BNode& c = bin.nodes[kids[best]];
-                        kids[best] = c.left;
-                        kids.push_back(c.right);
-                    }
+                    const int k = plan.split[bnode];
+                    plan.collect(root.left, k, kids, kidLeaf);
+                    plan.collect(root.right, 8 - k, kids, kidLeaf);
                 }
                 // slot assignment by octant
                 Box nodeBox;
@@ -304,7 +383,7 @@ namespace pt
                 {
                     const BNode& c = bin.nodes[kids[i]];
                     const int s = slotOf[i];
-                    if (c.leaf())
+                    if (kidLeaf[i])
                     {
                         if (c.count > 255) throw std::runtime_error("BVH leaf larger than 255 triangles");
                         childRef[s] = c.first | (c.count << 24);  // first triangle (24 bits), count (8 bits)
@@ -514,9 +593,15 @@ namespace pt
         std::iota(b.idx.begin(), b.idx.end(), 0u);
         b.nodes.resize(static_cast<size_t>(n) * 2);
         const uint32_t root = b.build(0, n, 0);
-        WideBuilder w{b, {}, 0};
-        w.out.reserve(static_cast<size_t>(n) / 3 + 8);
         if (root != 0) throw std::runtime_error("BVH root index");
+        CollapsePlan plan{b, {}, {}, {}};
+        const size_t binaryNodes = b.nodeCount.load();
+        plan.cost.assign(binaryNodes * 8, 0.0f);
+        plan.how.assign(binaryNodes * 8, 0);
+        plan.split.assign(binaryNodes, 1);
+        plan.plan(root);
+        WideBuilder w{b, plan, {}, 0};
+        w.out.reserve(static_cast<size_t>(n) / 4 + 8);
         w.emit(root, 0);
         Bvh8 result;
         result.nodes = std::move(w.out);
