@@ -257,6 +257,12 @@ namespace pt
             if (staging_) cudaFreeHost(staging_);
             if (hostMapped_) cudaFreeHost(hostMapped_);
             if (copyStream_) cudaStreamDestroy(copyStream_);
+            if (shadeFork_) cudaEventDestroy(shadeFork_);
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                if (shadeJoin_[m]) cudaEventDestroy(shadeJoin_[m]);
+                if (shadeStreams_[m]) cudaStreamDestroy(shadeStreams_[m]);
+            }
             if (stream_) cudaStreamDestroy(stream_);
         }
 
@@ -266,6 +272,12 @@ namespace pt
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking));
+            PT_CUDA("cudaEventCreateWithFlags", cudaEventCreateWithFlags(&shadeFork_, cudaEventDisableTiming));
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&shadeStreams_[m], cudaStreamNonBlocking));
+                PT_CUDA("cudaEventCreateWithFlags", cudaEventCreateWithFlags(&shadeJoin_[m], cudaEventDisableTiming));
+            }
             PT_CUDA("cudaHostAlloc", cudaHostAlloc(&staging_, kStagingBytes, cudaHostAllocDefault));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&startEvent_));
             PT_CUDA("cudaEventCreate", cudaEventCreate(&stopEvent_));
@@ -556,6 +568,12 @@ namespace pt
             L.shadeBlocks = sms * 8;
             L.sms = sms;
             L.graphLoop = true;
+            L.shadeFork = shadeFork_;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                L.shadeJoin[m] = shadeJoin_[m];
+                L.shadeStreams[m] = shadeStreams_[m];
+            }
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             const cudaError_t le = launch_engine_iteration(L, stream_);
             const cudaError_t ce = cudaStreamEndCapture(stream_, &body);
@@ -828,6 +846,9 @@ namespace pt
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;
         cudaStream_t copyStream_ = nullptr;  // images of finished jobs to host memory, beside the running slice
+        cudaEvent_t shadeFork_ = nullptr;     // the shading kernels run as parallel branches of the slice graph
+        cudaEvent_t shadeJoin_[kModelCount] = {};
+        cudaStream_t shadeStreams_[kModelCount] = {};
         void* staging_ = nullptr;            // pinned staging of those copies, kStagingBytes
         std::vector<uint64_t> toCopy_;       // finished jobs whose images are not on the host yet
         cudaEvent_t startEvent_ = nullptr, stopEvent_ = nullptr;

@@ -2137,6 +2137,37 @@ namespace pt
         return cudaGetLastError();
     }
 
+    // The shading kernels of the models present: with a fork event they run on their own streams side
+    // by side (parallel branches when captured into a graph; they touch disjoint queue entries and push
+    // with atomics) and join the launching stream again; without one, in order on it.
+    static cudaError_t launch_shading(const bool* modelPresent, cudaEvent_t fork, const cudaEvent_t* join, const cudaStream_t* streams,
+                                      int sms, const SceneView& sc, const Wavefront& wf, const JobView* jobs, const SceneEntry* scenes,
+                                      cudaStream_t s)
+    {
+        cudaError_t e;
+        uint32_t models = 0;
+        for (uint32_t m = 0; m < kModelCount; m++) models += modelPresent[m] ? 1u : 0u;
+        if (fork && models > 1)
+        {
+            if ((e = cudaEventRecord(fork, s)) != cudaSuccess) return e;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                if (!modelPresent[m]) continue;
+                if ((e = cudaStreamWaitEvent(streams[m], fork, 0)) != cudaSuccess) return e;
+                if ((e = launch_shade(m, sms, sc, wf, jobs, scenes, streams[m])) != cudaSuccess) return e;
+                if ((e = cudaEventRecord(join[m], streams[m])) != cudaSuccess) return e;
+                if ((e = cudaStreamWaitEvent(s, join[m], 0)) != cudaSuccess) return e;
+            }
+            return cudaSuccess;
+        }
+        for (uint32_t m = 0; m < kModelCount; m++)
+        {
+            if (!modelPresent[m]) continue;
+            if ((e = launch_shade(m, sms, sc, wf, jobs, scenes, s)) != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+
     cudaError_t launch_iteration(const IterationLaunch& L, cudaStream_t s)
     {
         cudaError_t e;
@@ -2149,29 +2180,8 @@ namespace pt
             e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
         if (L.traceStop && (e = cudaEventRecord(L.traceStop, s)) != cudaSuccess) return e;
-        uint32_t models = 0;
-        for (uint32_t m = 0; m < kModelCount; m++) models += L.modelPresent[m] ? 1u : 0u;
-        if (L.shadeFork && models > 1)
-        {
-            // the per-model shading kernels touch disjoint queue entries and push with atomics: run them side by side
-            if ((e = cudaEventRecord(L.shadeFork, s)) != cudaSuccess) return e;
-            for (uint32_t m = 0; m < kModelCount; m++)
-            {
-                if (!L.modelPresent[m]) continue;
-                if ((e = cudaStreamWaitEvent(L.shadeStreams[m], L.shadeFork, 0)) != cudaSuccess) return e;
-                if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.job, L.scenes, L.shadeStreams[m])) != cudaSuccess) return e;
-                if ((e = cudaEventRecord(L.shadeJoin[m], L.shadeStreams[m])) != cudaSuccess) return e;
-                if ((e = cudaStreamWaitEvent(s, L.shadeJoin[m], 0)) != cudaSuccess) return e;
-            }
-        }
-        else
-        {
-            for (uint32_t m = 0; m < kModelCount; m++)
-            {
-                if (!L.modelPresent[m]) continue;
-                if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess) return e;
-            }
-        }
+        if ((e = launch_shading(L.modelPresent, L.shadeFork, L.shadeJoin, L.shadeStreams, L.sms, L.scene, L.wf, L.job, L.scenes, s)) != cudaSuccess)
+            return e;
         if (L.nee && L.scene.lightCount > 0)
         {
             WavefrontShadow ws{L.scene, L.wf, nullptr};
@@ -2203,11 +2213,9 @@ namespace pt
         WavefrontClosest wc{L.scene, L.wf, L.ev.scenes};
         e = launch_trace<false>(wc, L.scene.depth, L.occupancy, L.traceBlocks, L.traceThreads, L.refill, &L.wf.ctr->errorFlags, s);
         if (e != cudaSuccess) return e;
-        for (uint32_t m = 0; m < kModelCount; m++)
-        {
-            if (!L.modelPresent[m]) continue;
-            if ((e = launch_shade(m, L.sms, L.scene, L.wf, L.ev.jobs, L.ev.scenes, s)) != cudaSuccess) return e;
-        }
+        if ((e = launch_shading(L.modelPresent, L.shadeFork, L.shadeJoin, L.shadeStreams, L.sms, L.scene, L.wf, L.ev.jobs, L.ev.scenes, s)) !=
+            cudaSuccess)
+            return e;
         if (L.anyLights)
         {
             WavefrontShadow ws{L.scene, L.wf, L.ev.scenes};

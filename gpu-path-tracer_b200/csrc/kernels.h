@@ -50,6 +50,10 @@ namespace pt
         int shadeBlocks;           // grid of the 256-thread bookkeeping kernels (regeneration, folding)
         int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;
+        // Optional fork/join of the shading kernels, as in IterationLaunch. nullptr = in order.
+        cudaEvent_t shadeFork;
+        cudaEvent_t shadeJoin[kModelCount];
+        cudaStream_t shadeStreams[kModelCount];
     };
 
     int trace_grid_blocks(int device, int threads, uint32_t depth, int occupancy, uint32_t bvhFormat = kBvh8Quantised);
