@@ -46,7 +46,7 @@ import numpy as np  # noqa: E402
 
 WORKLOAD = dict(workload="spheres-1m", scene="spheres-1m", triangles=1310978, width=1920, height=1080, spp=64,
                 depth=12, nee=True, lights=256, pool=1 << 20)
-TRACE_ALGO_BYTES_PER_RAY = 32 + 16 + 4   # ray record read, hit record write, queue index write
+TRACE_ALGO_BYTES_PER_RAY = 32 + 48   # ray record read, material-queue entry (ray and hit) written; a miss writes none
 NODE_BYTES = 64 + 4   # a BVH8 node visit reads the 64-byte header (boxes, origin, scales, masks) and its 4-byte reference
 TRIANGLE_BYTES = 48
 
@@ -589,7 +589,7 @@ def b200_arm(args):
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": per_launch_bytes,
-                     "bytes_model": f"{TRACE_ALGO_BYTES_PER_RAY} B/ray (ray in, hit out, queue index) + {NODE_BYTES} B/node visited + {TRIANGLE_BYTES} B/triangle tested",
+                     "bytes_model": f"{TRACE_ALGO_BYTES_PER_RAY} B/ray (ray in, material-queue entry out, every ray counted as a hit) + {NODE_BYTES} B/node visited + {TRIANGLE_BYTES} B/triangle tested",
                      "traffic_source": "ncu DRAM bytes per ray of a full-pool launch (profiles/trace_closest_spheres1m.json) x this run's rays per launch",
                      "node_visits_per_ray": visits / max(rays, 1), "triangle_tests_per_ray": tests / max(rays, 1),
                      "avg_launch_ms": per_launch_s * 1000.0,

@@ -290,8 +290,7 @@ namespace pt
                 PT_TRY(rayO_[q].allocate(P * 16));
                 PT_TRY(rayD_[q].allocate(P * 16));
             }
-            PT_TRY(hit_.allocate(P * 16));
-            PT_TRY(matQ_.allocate(P * 4 * kModelCount));
+            PT_TRY(matQ_.allocate(P * 48 * kModelCount));
             PT_TRY(shO_.allocate(P * 16));
             PT_TRY(shD_.allocate(P * 16));
             PT_TRY(shL_.allocate(P * 16));
@@ -498,8 +497,7 @@ namespace pt
                 w.rayO[q] = rayO_[q].get<float4>();
                 w.rayD[q] = rayD_[q].get<float4>();
             }
-            w.hit = hit_.get<float4>();
-            for (uint32_t m = 0; m < kModelCount; m++) w.matQ[m] = matQ_.get<uint32_t>() + size_t(m) * cfg_.pool_size;
+            for (uint32_t m = 0; m < kModelCount; m++) w.matQ[m] = matQ_.get<float4>() + size_t(m) * cfg_.pool_size * 3;
             w.shO = shO_.get<float4>();
             w.shD = shD_.get<float4>();
             w.shL = shL_.get<float4>();
@@ -861,7 +859,7 @@ namespace pt
         JobView* mirror_ = nullptr;
         uint32_t* orderHost_ = nullptr;
         uint32_t* sliceWords_ = nullptr;
-        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regenBits_, slotT_, slotL_, slotSample_, freeList_;
+        DeviceBuffer rayO_[2], rayD_[2], matQ_, shO_, shD_, shL_, regenBits_, slotT_, slotL_, slotSample_, freeList_;
         DeviceBuffer counters_, ctl_, jobs_, order_, segments_;
         ScenePack pack_;
         Arena arena_;

@@ -334,17 +334,21 @@ namespace pt
             tmax = b.w;
             tag = __float_as_uint(a.w);
         }
-        __device__ void finish(uint32_t i, uint32_t slot, const HitRecord& h, bool) const
+        // A hit enters its shading model's queue with the ray (origin, tag, direction) beside it, so
+        // the shading kernel reads one contiguous entry instead of gathering the ray and the hit.
+        __device__ void finish(uint32_t, uint32_t tag, const HitRecord& h, bool, float3 o, float3 d) const
         {
-            wf.hit[i] = make_float4(__uint_as_float(h.tri), h.u, h.v, h.t);
             if (h.tri != kInvalid)
             {
                 const uint32_t pos = agg_push_keyed(wf.ctr->matCount, h.model);
-                wf.matQ[h.model][pos] = i;
+                float4* e = wf.matQ[h.model] + static_cast<size_t>(pos) * 3;
+                e[0] = make_float4(o.x, o.y, o.z, __uint_as_float(tag));
+                e[1] = make_float4(d.x, d.y, d.z, kMaxT);
+                e[2] = make_float4(__uint_as_float(h.tri), h.u, h.v, h.t);
             }
             else
             {
-                path_finished(wf, wf.ctr, slot & kSlotMask);
+                path_finished(wf, wf.ctr, tag & kSlotMask);
             }
         }
     };
@@ -378,7 +382,7 @@ namespace pt
             tmax = b.w;
             tag = __float_as_uint(a.w);
         }
-        __device__ void finish(uint32_t i, uint32_t tag, const HitRecord&, bool occluded) const
+        __device__ void finish(uint32_t i, uint32_t tag, const HitRecord&, bool occluded, float3, float3) const
         {
             if (occluded) return;
             const uint32_t slot = tag & kSlotMask;
@@ -417,7 +421,7 @@ namespace pt
             tmax = r[7];
             tag = i;
         }
-        __device__ void finish(uint32_t i, uint32_t, const HitRecord& h, bool occluded) const
+        __device__ void finish(uint32_t i, uint32_t, const HitRecord& h, bool occluded, float3, float3) const
         {
             if (occOut)
             {
@@ -529,7 +533,7 @@ namespace pt
                     h.u = c1.x;
                     h.v = c1.y;
                     h.model = best == kInvalid ? 0u : (best >> 24);
-                    work.finish(__float_as_uint(c1.w), __float_as_uint(c0.w), h, occluded);
+                    work.finish(__float_as_uint(c1.w), __float_as_uint(c0.w), h, occluded, st.ray.o, make_float3(c0.x, c0.y, c0.z));
                     active = false;
                 }
                 // a step adds at most 8 x 255 tests: flush the packed counters well before a field overflows
@@ -1157,7 +1161,7 @@ namespace pt
         const uint32_t n = ctr->matCount[MODEL];
         const uint32_t cur = ctr->cur;
         const uint32_t nxt = cur ^ 1u;
-        const uint32_t* queue = wf.matQ[MODEL];
+        const float4* queue = wf.matQ[MODEL];
         __shared__ uint32_t octCount[16], octBase[16], blockBase[2];
         for (uint32_t kb = blockIdx.x * blockDim.x; kb < n; kb += gridDim.x * blockDim.x)
         {
@@ -1167,10 +1171,10 @@ namespace pt
             float4 shOut0 = rayOut0, shOut1 = rayOut0, shOut2 = rayOut0;
             if (k < n)
             {
-                const uint32_t r = queue[k];
-                const float4 o4 = wf.rayO[cur][r];
-                const float4 d4 = wf.rayD[cur][r];
-                const float4 h4 = wf.hit[r];
+                const float4* entry = queue + static_cast<size_t>(k) * 3;
+                const float4 o4 = entry[0];
+                const float4 d4 = entry[1];
+                const float4 h4 = entry[2];
                 const uint32_t tag = __float_as_uint(o4.w);
                 const uint32_t slot = tag & kSlotMask;
                 const float3 o = f3(o4), d = f3(d4);

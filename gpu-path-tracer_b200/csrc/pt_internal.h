@@ -9,8 +9,8 @@
 //   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14)
 //   path slot         36 B  throughput|depth/flags/job, radiance|rng position, sample index
 //   ray queue entry   32 B  origin|tag, direction|tMax   (x2, ping-pong; tag = slot | scene << 24)
-//   hit record        16 B  triangle, u, v, t             (aligned with the current ray queue)
-//   material queue     4 B  ray-queue index               (x6, one per shading model)
+//   material queue    48 B  origin|tag, direction|tMax, triangle|u|v|t   (x6, one per shading model: the
+//                           closest-hit kernel writes the ray and its hit, so shading reads one entry)
 //   shadow queue      48 B  origin|slot, direction|tMax, radiance
 //   regen queue        4 B  slot
 #pragma once
@@ -220,8 +220,7 @@ namespace pt
     {
         float4* rayO[2];
         float4* rayD[2];
-        float4* hit;
-        uint32_t* matQ[kModelCount];
+        float4* matQ[kModelCount];   // per model: entries of 3 float4 = origin|tag, direction|tMax, triangle|u|v|t
         float4* shO;
         float4* shD;
         float4* shL;

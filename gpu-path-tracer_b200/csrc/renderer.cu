@@ -334,8 +334,7 @@ namespace pt
                 PT_TRY(rayO_[q].allocate(P * 16));
                 PT_TRY(rayD_[q].allocate(P * 16));
             }
-            PT_TRY(hit_.allocate(P * 16));
-            PT_TRY(matQ_.allocate(P * 4 * kModelCount));
+            PT_TRY(matQ_.allocate(P * 48 * kModelCount));
             PT_TRY(shO_.allocate(P * 16));
             PT_TRY(shD_.allocate(P * 16));
             PT_TRY(shL_.allocate(P * 16));
@@ -358,8 +357,7 @@ namespace pt
                 w.rayO[q] = rayO_[q].get<float4>();
                 w.rayD[q] = rayD_[q].get<float4>();
             }
-            w.hit = hit_.get<float4>();
-            for (uint32_t m = 0; m < kModelCount; m++) w.matQ[m] = matQ_.get<uint32_t>() + static_cast<size_t>(m) * pool_;
+            for (uint32_t m = 0; m < kModelCount; m++) w.matQ[m] = matQ_.get<float4>() + static_cast<size_t>(m) * pool_ * 3;
             w.shO = shO_.get<float4>();
             w.shD = shD_.get<float4>();
             w.shL = shL_.get<float4>();
@@ -920,7 +918,7 @@ namespace pt
         static constexpr uint32_t kDefaultPool = 1u << 20;
         static constexpr uint32_t kLogCapacity = 1u << 16;
         uint32_t pool_ = 0;
-        DeviceBuffer rayO_[2], rayD_[2], hit_, matQ_, shO_, shD_, shL_, regen_, regenBits_, slotT_, slotL_, slotSample_, queueLog_;
+        DeviceBuffer rayO_[2], rayD_[2], matQ_, shO_, shD_, shL_, regen_, regenBits_, slotT_, slotL_, slotSample_, queueLog_;
         DeviceBuffer counters_, job_, cursor_, accumulation_, framebuffer_, sampleRadiance_;
         JobView hostJob_{};
         Counters hostCounters_{};
