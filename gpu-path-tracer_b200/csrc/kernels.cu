@@ -1,10 +1,10 @@
 // sm_100a kernels of the wavefront path tracer.
 //
 // Per wavefront iteration (one CUDA-graph body, no host round trip):
-//   trace_kernel<closest>  BVH8 closest hit for the current ray queue -> hit records, per-model queues
+//   trace_kernel<closest>  BVH8 closest hit for the current ray queue -> per-model queues of (ray, hit) entries
 //   shade_kernel<model>    one launch per shading model present (MaterialEval.cu:194-912)
 //   trace_kernel<any>      NEE shadow rays, any hit; unoccluded radiance added to the path slot
-//   regen_kernel           finished paths -> per-sample radiance; new samples -> next ray queue
+//   regen_bits_kernel      finished paths -> per-sample radiance; new samples -> next ray queue
 //   advance_kernel         one thread: queue bookkeeping, log, loop condition (Renderer.cpp:573-619)
 // All arithmetic that reaches a result uses IEEE operators in the reference's order; the
 // library is compiled with -fmad=false.
