@@ -658,6 +658,8 @@ namespace pt
     // (the queue holds them in the order paths finished, i.e. scattered). The set of new samples, their
     // ray-queue positions and every sample's result are those of the queue-driven regeneration; only
     // which slot a new sample lands in differs.
+    constexpr uint32_t kRegenGroup = 4;  // bitmap words whose finished slots are loaded together
+
     __global__ void regen_bits_kernel(Wavefront wf, const JobView* jobPtr)
     {
         Counters* ctr = wf.ctr;
@@ -691,20 +693,37 @@ namespace pt
             if (lane == 0) first = atomicAdd(&ctr->regenCursor, tileTotal);
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
             const uint32_t excl = incl - count;
-            for (uint32_t j = 0; j < 32; j++)
+            // words in groups of kRegenGroup: the finished slots' loads of a group are in flight together
+            for (uint32_t jb = 0; jb < 32; jb += kRegenGroup)
             {
-                const uint32_t w = __shfl_sync(0xFFFFFFFFu, bits, j);
-                const uint32_t offset = __shfl_sync(0xFFFFFFFFu, excl, j);
-                if (!((w >> lane) & 1u)) continue;
-                const uint32_t slot = (tile * 32u + j) * 32u + lane;
-                const float4 L = wf.slotL[slot];
-                const uint32_t sample = wf.slotSample[slot];
-                float* dst = out + static_cast<size_t>(sample) * 3;
-                dst[0] = L.x;
-                dst[1] = L.y;
-                dst[2] = L.z;
-                const uint32_t k = first + offset + static_cast<uint32_t>(__popc(w & lanesBelow));
-                if (k < regenerate) start_path(*jobPtr, 0, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
+                uint32_t w[kRegenGroup], offset[kRegenGroup], sample[kRegenGroup];
+                float4 L[kRegenGroup];
+#pragma unroll
+                for (uint32_t q = 0; q < kRegenGroup; q++)
+                {
+                    w[q] = __shfl_sync(0xFFFFFFFFu, bits, jb + q);
+                    offset[q] = __shfl_sync(0xFFFFFFFFu, excl, jb + q);
+                    L[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    sample[q] = 0;
+                    if ((w[q] >> lane) & 1u)
+                    {
+                        const uint32_t slot = (tile * 32u + jb + q) * 32u + lane;
+                        L[q] = wf.slotL[slot];
+                        sample[q] = wf.slotSample[slot];
+                    }
+                }
+#pragma unroll
+                for (uint32_t q = 0; q < kRegenGroup; q++)
+                {
+                    if (!((w[q] >> lane) & 1u)) continue;
+                    const uint32_t slot = (tile * 32u + jb + q) * 32u + lane;
+                    float* dst = out + static_cast<size_t>(sample[q]) * 3;
+                    dst[0] = L[q].x;
+                    dst[1] = L[q].y;
+                    dst[2] = L[q].z;
+                    const uint32_t k = first + offset[q] + static_cast<uint32_t>(__popc(w[q] & lanesBelow));
+                    if (k < regenerate) start_path(*jobPtr, 0, wf, slot, static_cast<uint32_t>(launched + k), nxt, base + k);
+                }
             }
         }
         phase_end(ctr, 3);
@@ -1607,15 +1626,14 @@ namespace pt
     }
 
     // A finished path writes its radiance into its job's pass ring and counts towards the pass.
-    __device__ __forceinline__ void engine_retire_path(const Wavefront& wf, const EngineView& ev, uint32_t slot)
+    // meta: the slot's path metadata (job in bits 16-31), sample and L: its sample index and radiance.
+    __device__ __forceinline__ void engine_retire_path(const EngineView& ev, uint32_t meta, uint32_t sample, float4 L)
     {
-        const uint32_t j = __float_as_uint(wf.slotT[slot].w) >> 16;
+        const uint32_t j = meta >> 16;
         JobView& J = ev.jobs[j];
-        const uint32_t sample = wf.slotSample[slot];
         const uint32_t pixel = sample / J.spp;
         const uint32_t pass = sample - pixel * J.spp;
         const uint32_t r = pass % J.ring;
-        const float4 L = wf.slotL[slot];
         float* dst = J.sampleRadiance + (static_cast<size_t>(r) * J.pixels + pixel) * 3;
         dst[0] = L.x;
         dst[1] = L.y;
@@ -1624,17 +1642,18 @@ namespace pt
     }
 
     // Planned launch k of the iteration starts in `slot` (the plan's segments map k to a job and launch index).
-    __device__ __forceinline__ void engine_start_launch(const Wavefront& wf, const EngineView& ev, uint32_t k, uint32_t slot,
-                                                        uint32_t segmentCount, uint32_t nxt, uint32_t base)
+    // segments: the plan's segments (a shared-memory copy when they fit, else ev.segments).
+    __device__ __forceinline__ void engine_start_launch(const Wavefront& wf, const EngineView& ev, const LaunchSegment* segments, uint32_t k,
+                                                        uint32_t slot, uint32_t segmentCount, uint32_t nxt, uint32_t base)
     {
         uint32_t lo = 0, hi = segmentCount - 1u;
         while (lo < hi)
         {
             const uint32_t mid = (lo + hi + 1u) >> 1;
-            if (ev.segments[mid].start <= k) lo = mid;
+            if (segments[mid].start <= k) lo = mid;
             else hi = mid - 1u;
         }
-        const LaunchSegment sg = ev.segments[lo];
+        const LaunchSegment sg = segments[lo];
         const JobView& J = ev.jobs[sg.job];
         const uint64_t g = sg.first + (k - sg.start);
         const uint32_t pass = static_cast<uint32_t>(g / J.pixels);
@@ -1645,6 +1664,8 @@ namespace pt
     // Job-engine regeneration from the finished-slot bitmap (same tiling as regen_bits_kernel): the
     // finished slot of rank k takes planned launch k, or goes onto the free list when k >= the plan;
     // launches beyond the finished slots take slots from the free list.
+    constexpr uint32_t kSharedSegments = 512;  // plan segments held in shared memory by the engine's regeneration
+
     __global__ void engine_regen_bits_kernel(Wavefront wf, EngineView ev)
     {
         Counters* ctr = wf.ctr;
@@ -1661,6 +1682,13 @@ namespace pt
         const uint32_t lane = lane_id();
         const uint32_t lanesBelow = (1u << lane) - 1u;
         const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+        // the plan's segments, searched once per launch, from shared memory when they fit
+        __shared__ LaunchSegment localSegments[kSharedSegments];
+        const bool shared = segmentCount <= kSharedSegments;
+        if (shared)
+            for (uint32_t i = threadIdx.x; i < segmentCount; i += blockDim.x) localSegments[i] = ev.segments[i];
+        __syncthreads();
+        const LaunchSegment* segments = shared ? localSegments : ev.segments;
         for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps)
         {
             const uint32_t wi = tile * 32u + lane;
@@ -1679,20 +1707,41 @@ namespace pt
             if (lane == 0) first = atomicAdd(&ctr->regenCursor, tileTotal);
             first = __shfl_sync(0xFFFFFFFFu, first, 0);
             const uint32_t excl = incl - count;
-            for (uint32_t j = 0; j < 32; j++)
+            // words in groups of kRegenGroup: the finished slots' loads of a group are in flight together
+            for (uint32_t jb = 0; jb < 32; jb += kRegenGroup)
             {
-                const uint32_t w = __shfl_sync(0xFFFFFFFFu, bits, j);
-                const uint32_t offset = __shfl_sync(0xFFFFFFFFu, excl, j);
-                if (!((w >> lane) & 1u)) continue;
-                const uint32_t slot = (tile * 32u + j) * 32u + lane;
-                engine_retire_path(wf, ev, slot);
-                const uint32_t k = first + offset + static_cast<uint32_t>(__popc(w & lanesBelow));
-                if (k < launch) engine_start_launch(wf, ev, k, slot, segmentCount, nxt, base);
-                else ev.freeList[freeCount + (k - launch)] = slot;
+                uint32_t w[kRegenGroup], offset[kRegenGroup], meta[kRegenGroup], sample[kRegenGroup];
+                float4 L[kRegenGroup];
+#pragma unroll
+                for (uint32_t q = 0; q < kRegenGroup; q++)
+                {
+                    w[q] = __shfl_sync(0xFFFFFFFFu, bits, jb + q);
+                    offset[q] = __shfl_sync(0xFFFFFFFFu, excl, jb + q);
+                    L[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    meta[q] = 0;
+                    sample[q] = 0;
+                    if ((w[q] >> lane) & 1u)
+                    {
+                        const uint32_t slot = (tile * 32u + jb + q) * 32u + lane;
+                        meta[q] = __float_as_uint(wf.slotT[slot].w);
+                        sample[q] = wf.slotSample[slot];
+                        L[q] = wf.slotL[slot];
+                    }
+                }
+#pragma unroll
+                for (uint32_t q = 0; q < kRegenGroup; q++)
+                {
+                    if (!((w[q] >> lane) & 1u)) continue;
+                    const uint32_t slot = (tile * 32u + jb + q) * 32u + lane;
+                    engine_retire_path(ev, meta[q], sample[q], L[q]);
+                    const uint32_t k = first + offset[q] + static_cast<uint32_t>(__popc(w[q] & lanesBelow));
+                    if (k < launch) engine_start_launch(wf, ev, segments, k, slot, segmentCount, nxt, base);
+                    else ev.freeList[freeCount + (k - launch)] = slot;
+                }
             }
         }
         for (uint32_t k = n + blockIdx.x * blockDim.x + threadIdx.x; k < launch; k += gridDim.x * blockDim.x)
-            engine_start_launch(wf, ev, k, ev.freeList[freeCount - 1u - (k - n)], segmentCount, nxt, base);
+            engine_start_launch(wf, ev, segments, k, ev.freeList[freeCount - 1u - (k - n)], segmentCount, nxt, base);
         phase_end(ctr, 3);
     }
 
@@ -2126,6 +2175,26 @@ namespace pt
         return perSm;
     }
 
+    // Resident 256-thread blocks per SM of a regeneration kernel, at most 8 (its tiles are handed out
+    // by a grid stride, so a grid larger than what is resident leaves late blocks a full share).
+    template <class K>
+    static int resident_blocks_256(K kernel)
+    {
+        int b = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, 256, 0) != cudaSuccess) b = 8;
+        return b < 1 ? 1 : (b > 8 ? 8 : b);
+    }
+    static int regen_blocks_per_sm()
+    {
+        static const int perSm = resident_blocks_256(regen_bits_kernel);
+        return perSm;
+    }
+    static int engine_regen_blocks_per_sm()
+    {
+        static const int perSm = resident_blocks_256(engine_regen_bits_kernel);
+        return perSm;
+    }
+
     static cudaError_t launch_shade(uint32_t m, int sms, const SceneView& sc, const Wavefront& wf, const JobView* jobs,
                                     const SceneEntry* scenes, cudaStream_t s)
     {
@@ -2196,7 +2265,7 @@ namespace pt
             if (e != cudaSuccess) return e;
         }
         if (L.wf.regenBits != nullptr)
-            regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
+            regen_bits_kernel<<<L.sms * regen_blocks_per_sm(), 256, 0, s>>>(L.wf, L.job);
         else
             regen_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.job);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -2228,7 +2297,7 @@ namespace pt
         }
         plan_kernel<<<1, 1, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        engine_regen_bits_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.wf, L.ev);
+        engine_regen_bits_kernel<<<L.sms * engine_regen_blocks_per_sm(), 256, 0, s>>>(L.wf, L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         fold_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
