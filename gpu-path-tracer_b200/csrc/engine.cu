@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <memory>
 #include <cstddef>
 #include <cstring>
 #include <deque>
@@ -215,8 +216,9 @@ namespace pt
         uint64_t admittedBytes = 0;
         double tSubmit = -1.0, tAdmit = -1.0, tDone = -1.0;
         bool cancelRequested = false, cancelApplied = false;
-        std::vector<uint32_t> rgba;
-        std::vector<float> accumulation;
+        // Shared so that a read copies the image outside the server's lock while a release may drop the record.
+        std::shared_ptr<std::vector<uint32_t>> rgba;
+        std::shared_ptr<std::vector<float>> accumulation;
     };
 
     class Server
@@ -414,19 +416,25 @@ namespace pt
             return Status::Ok();
         }
 
+        // The copy runs outside the lock: the worker thread, which takes the lock between slices, is
+        // not held up by a large image on its way to the caller.
         Status Read(uint64_t id, uint32_t* rgba, float* accumulation)
         {
-            std::scoped_lock lock(mu_);
-            auto it = records_.find(id);
-            if (it == records_.end()) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown job id");
-            const JobRecord& J = it->second;
-            if (J.state != GPT_JOB_DONE) return Status::Err(GPT_ERR_STATE, "Job has no result (not done, cancelled or failed)");
-            if (rgba) std::memcpy(rgba, J.rgba.data(), J.rgba.size() * 4);
-            if (accumulation)
+            std::shared_ptr<std::vector<uint32_t>> image;
+            std::shared_ptr<std::vector<float>> accum;
             {
-                if (J.accumulation.empty()) return Status::Err(GPT_ERR_STATE, "Job was submitted without keep_accumulation");
-                std::memcpy(accumulation, J.accumulation.data(), J.accumulation.size() * 4);
+                std::scoped_lock lock(mu_);
+                auto it = records_.find(id);
+                if (it == records_.end()) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown job id");
+                const JobRecord& J = it->second;
+                if (J.state != GPT_JOB_DONE) return Status::Err(GPT_ERR_STATE, "Job has no result (not done, cancelled or failed)");
+                if (accumulation && (!J.accumulation || J.accumulation->empty()))
+                    return Status::Err(GPT_ERR_STATE, "Job was submitted without keep_accumulation");
+                image = J.rgba;
+                accum = J.accumulation;
             }
+            if (rgba && image) std::memcpy(rgba, image->data(), image->size() * 4);
+            if (accumulation) std::memcpy(accumulation, accum->data(), accum->size() * 4);
             return Status::Ok();
         }
 
@@ -713,8 +721,6 @@ namespace pt
                     finish(J, GPT_JOB_CANCELLED);
                 else
                 {
-                    J.rgba.resize(J.pixels);
-                    if (J.desc.keep_accumulation) J.accumulation.resize(size_t(J.pixels) * 4);
                     toCopy_.push_back(J.id);
                 }
                 active_.erase(active_.begin() + static_cast<std::ptrdiff_t>(i));
@@ -723,15 +729,19 @@ namespace pt
         }
 
         // Without mu_: images (and accumulations) of finished jobs to host memory through pinned
-        // staging on the copy stream, while the next slice runs on the render stream.
+        // staging on the copy stream, while the next slice runs on the render stream. Their host
+        // buffers are allocated here too, not under the lock between slices (no other thread reads a
+        // record's image before finish() marks it done).
         Status copyImages(const std::vector<JobRecord*>& jobs)
         {
             char* st = static_cast<char*>(staging_);
             for (JobRecord* J : jobs)
             {
+                J->rgba = std::make_shared<std::vector<uint32_t>>(J->pixels);
+                if (J->desc.keep_accumulation) J->accumulation = std::make_shared<std::vector<float>>(size_t(J->pixels) * 4);
                 // RGBA8 image in chunks of the fixed staging buffer
                 const char* src = reinterpret_cast<const char*>(J->view.framebuffer);
-                char* dst = reinterpret_cast<char*>(J->rgba.data());
+                char* dst = reinterpret_cast<char*>(J->rgba->data());
                 for (size_t done = 0, total = size_t(J->pixels) * 4; done < total;)
                 {
                     const size_t n = std::min(kStagingBytes, total - done);
@@ -748,7 +758,7 @@ namespace pt
                     const size_t n = std::min(rows, size_t(J->pixels) - px);
                     PT_CUDA("cudaMemcpy2DAsync", cudaMemcpy2DAsync(st, 16, J->view.accum + 2 * px, 32, 16, n, cudaMemcpyDeviceToHost, copyStream_));
                     PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(copyStream_));
-                    std::memcpy(J->accumulation.data() + 4 * px, st, n * 16);
+                    std::memcpy(J->accumulation->data() + 4 * px, st, n * 16);
                     px += n;
                 }
             }
