@@ -43,14 +43,6 @@ namespace pt
         return base + static_cast<uint32_t>(__popc(peers & ((1u << lane) - 1u)));
     }
 
-    // Warp-aggregated atomicAdd(ptr, 1) where lanes with equal key share ptr: one atomic per key.
-    __device__ __forceinline__ void agg_increment_keyed(uint32_t* ptr, uint32_t key)
-    {
-        const unsigned active = __activemask();
-        const unsigned peers = __match_any_sync(active, key);
-        if (static_cast<int>(lane_id()) == __ffs(peers) - 1) atomicAdd(ptr, static_cast<uint32_t>(__popc(peers)));
-    }
-
     __device__ __forceinline__ unsigned long long global_ns()
     {
         unsigned long long t;
@@ -1626,8 +1618,34 @@ namespace pt
     }
 
     // A finished path writes its radiance into its job's pass ring and counts towards the pass.
+    // Finished samples per (job, ring buffer) are counted per block in shared memory first: every path
+    // of a job's pass increments the same counter, and a global atomic per warp and key piles up on a
+    // few addresses (worst with one job). A block flushes its table once, at the end of the kernel.
+    constexpr uint32_t kPassTable = 256;
+
+    __device__ __forceinline__ void count_finished(uint32_t* tableKey, uint32_t* tableCount, uint32_t* globalCounter, uint32_t key)
+    {
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, key);
+        if (static_cast<int>(lane_id()) != __ffs(peers) - 1) return;
+        const uint32_t n = static_cast<uint32_t>(__popc(peers));
+        const uint32_t h = (key * 2654435761u) >> 24;
+        for (uint32_t probe = 0; probe < 8; probe++)
+        {
+            const uint32_t s = (h + probe) & (kPassTable - 1u);
+            const uint32_t prev = atomicCAS(&tableKey[s], kInvalid, key);
+            if (prev == kInvalid || prev == key)
+            {
+                atomicAdd(&tableCount[s], n);
+                return;
+            }
+        }
+        atomicAdd(globalCounter, n);  // table crowded: count directly
+    }
+
     // meta: the slot's path metadata (job in bits 16-31), sample and L: its sample index and radiance.
-    __device__ __forceinline__ void engine_retire_path(const EngineView& ev, uint32_t meta, uint32_t sample, float4 L)
+    __device__ __forceinline__ void engine_retire_path(const EngineView& ev, uint32_t meta, uint32_t sample, float4 L, uint32_t* tableKey,
+                                                       uint32_t* tableCount)
     {
         const uint32_t j = meta >> 16;
         JobView& J = ev.jobs[j];
@@ -1638,7 +1656,7 @@ namespace pt
         dst[0] = L.x;
         dst[1] = L.y;
         dst[2] = L.z;
-        agg_increment_keyed(&J.passDone[r], (j << 8) | r);
+        count_finished(tableKey, tableCount, &J.passDone[r], (j << 8) | r);
     }
 
     // Planned launch k of the iteration starts in `slot` (the plan's segments map k to a job and launch index).
@@ -1684,9 +1702,15 @@ namespace pt
         const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
         // the plan's segments, searched once per launch, from shared memory when they fit
         __shared__ LaunchSegment localSegments[kSharedSegments];
+        __shared__ uint32_t passKey[kPassTable], passCount[kPassTable];
         const bool shared = segmentCount <= kSharedSegments;
         if (shared)
             for (uint32_t i = threadIdx.x; i < segmentCount; i += blockDim.x) localSegments[i] = ev.segments[i];
+        for (uint32_t i = threadIdx.x; i < kPassTable; i += blockDim.x)
+        {
+            passKey[i] = kInvalid;
+            passCount[i] = 0;
+        }
         __syncthreads();
         const LaunchSegment* segments = shared ? localSegments : ev.segments;
         for (uint32_t tile = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tile < tiles; tile += warps)
@@ -1733,7 +1757,7 @@ namespace pt
                 {
                     if (!((w[q] >> lane) & 1u)) continue;
                     const uint32_t slot = (tile * 32u + jb + q) * 32u + lane;
-                    engine_retire_path(ev, meta[q], sample[q], L[q]);
+                    engine_retire_path(ev, meta[q], sample[q], L[q], passKey, passCount);
                     const uint32_t k = first + offset[q] + static_cast<uint32_t>(__popc(w[q] & lanesBelow));
                     if (k < launch) engine_start_launch(wf, ev, segments, k, slot, segmentCount, nxt, base);
                     else ev.freeList[freeCount + (k - launch)] = slot;
@@ -1742,6 +1766,12 @@ namespace pt
         }
         for (uint32_t k = n + blockIdx.x * blockDim.x + threadIdx.x; k < launch; k += gridDim.x * blockDim.x)
             engine_start_launch(wf, ev, segments, k, ev.freeList[freeCount - 1u - (k - n)], segmentCount, nxt, base);
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kPassTable; i += blockDim.x)
+        {
+            const uint32_t key = passKey[i];
+            if (key != kInvalid) atomicAdd(&ev.jobs[key >> 8].passDone[key & 0xFFu], passCount[i]);
+        }
         phase_end(ctr, 3);
     }
 
