@@ -2417,7 +2417,7 @@ namespace pt
         return cudaGetLastError();
     }
 
-    cudaError_t launch_light_build(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+    cudaError_t launch_light_build(const float4* shading, const MaterialDev* materials, uint32_t n,
                                    uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCountDev, cudaStream_t s)
     {
         const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;

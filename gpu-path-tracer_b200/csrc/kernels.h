@@ -71,7 +71,7 @@ namespace pt
                                    uint32_t bvhFormat = kBvh8Quantised);
     cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
                                        const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t stream);
-    cudaError_t launch_light_build(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
+    cudaError_t launch_light_build(const float4* shading, const MaterialDev* materials, uint32_t n,
                                    uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCount, cudaStream_t stream);
     cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
                                      const uint32_t* flags, const uint32_t* index, float4* lights, double* weights, cudaStream_t stream);

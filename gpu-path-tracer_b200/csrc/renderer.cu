@@ -226,7 +226,7 @@ namespace pt
         PT_TRY(index.allocate(static_cast<size_t>(n) * 4));
         PT_TRY(scanScratch.allocate(scan_scratch_elements(n) * 8));
         PT_TRY(lightCountDev.allocate(16));
-        PT_CUDA("light build", launch_light_build(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
+        PT_CUDA("light build", launch_light_build(scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
                                                   flags.get<uint32_t>(), index.get<uint32_t>(), scanScratch.get<uint32_t>(), lightCountDev.get<uint32_t>(), stream));
         uint32_t lightCount = 0;
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&lightCount, lightCountDev.get<void>(), 4, cudaMemcpyDeviceToHost, stream));

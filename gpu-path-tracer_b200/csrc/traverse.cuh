@@ -86,7 +86,9 @@ namespace pt
         const uint32_t nzl = nz ? w3.z : w2.x, nzh = nz ? w3.w : w2.y;
         const uint32_t fzl = nz ? w2.x : w3.z, fzh = nz ? w2.y : w3.w;
         uint32_t hit = 0;
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
         for (int s = 0; s < 8; s++)
         {
             const float tnx = fma_hd(byte_to_float(nxl, nxh, s), ax, bnx);
