@@ -1617,7 +1617,6 @@ namespace pt
         e->segmentCount = segments;
     }
 
-    // A finished path writes its radiance into its job's pass ring and counts towards the pass.
     // Finished samples per (job, ring buffer) are counted per block in shared memory first: every path
     // of a job's pass increments the same counter, and a global atomic per warp and key piles up on a
     // few addresses (worst with one job). A block flushes its table once, at the end of the kernel.
@@ -1643,6 +1642,7 @@ namespace pt
         atomicAdd(globalCounter, n);  // table crowded: count directly
     }
 
+    // A finished path writes its radiance into its job's pass ring and counts towards the pass.
     // meta: the slot's path metadata (job in bits 16-31), sample and L: its sample index and radiance.
     __device__ __forceinline__ void engine_retire_path(const EngineView& ev, uint32_t meta, uint32_t sample, float4 L, uint32_t* tableKey,
                                                        uint32_t* tableCount)
@@ -1779,41 +1779,86 @@ namespace pt
     // last fold also writes its tone-mapped RGBA8 image.
     __global__ void fold_kernel(EngineView ev)
     {
+        // jobs in blocks of blockDim.x: their foldable pass counts are found side by side first
+        __shared__ uint32_t jobOf[256], countOf[256];
         const uint32_t orderCount = ev.ctl->orderCount;
-        for (uint32_t i = 0; i < orderCount; i++)
+        for (uint32_t base = 0; base < orderCount; base += blockDim.x)
         {
-            const uint32_t j = ev.order[i];
-            const JobView& J = ev.jobs[j];
-            if (J.state != kJobActive) continue;
-            const uint32_t count = foldable_passes(J);
-            if (count == 0) continue;
-            const bool last = J.folded + count == job_passes(J);
-            const float invSpp = 1.0f / static_cast<float>(J.spp);
-            for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < J.pixels; px += gridDim.x * blockDim.x)
+            const uint32_t i = base + threadIdx.x;
+            uint32_t count = 0, j = 0;
+            if (i < orderCount)
             {
-                const float4 s4 = J.accum[2 * static_cast<size_t>(px)];
-                const float4 c4 = J.accum[2 * static_cast<size_t>(px) + 1];
-                float sum[3] = {s4.x, s4.y, s4.z}, comp[3] = {c4.x, c4.y, c4.z};
-                for (uint32_t q = 0; q < count; q++)
-                {
-                    const uint64_t p = static_cast<uint64_t>(J.folded) + q;
-                    if (p * J.pixels + px >= J.totalSamples) break;
-                    const float* x = J.sampleRadiance + (static_cast<size_t>(p % J.ring) * J.pixels + px) * 3;
-                    for (int ch = 0; ch < 3; ch++) kahan_add(sum[ch], comp[ch], x[ch]);
-                }
-                J.accum[2 * static_cast<size_t>(px)] = make_float4(sum[0], sum[1], sum[2], 0.0f);
-                J.accum[2 * static_cast<size_t>(px) + 1] = make_float4(comp[0], comp[1], comp[2], 0.0f);
-                if (last) J.framebuffer[px] = tonemap_rgba8(sum, invSpp);
+                j = ev.order[i];
+                const JobView& J = ev.jobs[j];
+                if (J.state == kJobActive) count = foldable_passes(J);
             }
+            jobOf[threadIdx.x] = j;
+            countOf[threadIdx.x] = count;
+            __syncthreads();
+            const uint32_t chunk = orderCount - base < blockDim.x ? orderCount - base : blockDim.x;
+            for (uint32_t t = 0; t < chunk; t++)
+            {
+                const uint32_t count_t = countOf[t];
+                if (count_t == 0) continue;
+                const JobView& J = ev.jobs[jobOf[t]];
+                const bool last = J.folded + count_t == job_passes(J);
+                const float invSpp = 1.0f / static_cast<float>(J.spp);
+                for (uint32_t px = blockIdx.x * blockDim.x + threadIdx.x; px < J.pixels; px += gridDim.x * blockDim.x)
+                {
+                    const float4 s4 = J.accum[2 * static_cast<size_t>(px)];
+                    const float4 c4 = J.accum[2 * static_cast<size_t>(px) + 1];
+                    float sum[3] = {s4.x, s4.y, s4.z}, comp[3] = {c4.x, c4.y, c4.z};
+                    for (uint32_t q = 0; q < count_t; q++)
+                    {
+                        const uint64_t p = static_cast<uint64_t>(J.folded) + q;
+                        if (p * J.pixels + px >= J.totalSamples) break;
+                        const float* x = J.sampleRadiance + (static_cast<size_t>(p % J.ring) * J.pixels + px) * 3;
+                        for (int ch = 0; ch < 3; ch++) kahan_add(sum[ch], comp[ch], x[ch]);
+                    }
+                    J.accum[2 * static_cast<size_t>(px)] = make_float4(sum[0], sum[1], sum[2], 0.0f);
+                    J.accum[2 * static_cast<size_t>(px) + 1] = make_float4(comp[0], comp[1], comp[2], 0.0f);
+                    if (last) J.framebuffer[px] = tonemap_rgba8(sum, invSpp);
+                }
+            }
+            __syncthreads();
         }
     }
 
-    // One thread: queue bookkeeping, fold accounting, job completion and the slice's loop
-    // condition. The slice ends when a job completes (so the host can hand out its result and
-    // admit waiting jobs), when the host rings the doorbell (a job arrived), when there is nothing
-    // left to do, or after maxSliceIterations iterations.
+    // One block: fold accounting and job completion, one thread per job, then (thread 0) queue
+    // bookkeeping and the slice's loop condition. The slice ends when a job completes (so the host can
+    // hand out its result and admit waiting jobs), when the host rings the doorbell (a job arrived),
+    // when there is nothing left to do, or after maxSliceIterations iterations.
     __global__ void engine_advance_kernel(Wavefront wf, EngineView ev, cudaGraphConditionalHandle handle, bool graphLoop)
     {
+        __shared__ uint32_t completedJobs, unfinishedJobs, launchableJobs;
+        if (threadIdx.x == 0)
+        {
+            completedJobs = 0;
+            unfinishedJobs = 0;
+            launchableJobs = 0;
+        }
+        __syncthreads();
+        {
+            const uint32_t orderCount = ev.ctl->orderCount;
+            for (uint32_t i = threadIdx.x; i < orderCount; i += blockDim.x)
+            {
+                JobView& J = ev.jobs[ev.order[i]];
+                if (J.state != kJobActive) continue;
+                const uint32_t count = foldable_passes(J);
+                for (uint32_t q = 0; q < count; q++) J.passDone[(static_cast<uint64_t>(J.folded) + q) % J.ring] = 0;
+                J.folded += count;
+                if (J.folded == job_passes(J))
+                {
+                    J.state = kJobDone;
+                    atomicAdd(&completedJobs, 1u);
+                    continue;
+                }
+                atomicOr(&unfinishedJobs, 1u);
+                if (job_window_end(J) > J.launched) atomicOr(&launchableJobs, 1u);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x != 0) return;
         Counters* c = wf.ctr;
         EngineCtl* e = ev.ctl;
         const uint32_t cur = c->cur;
@@ -1842,24 +1887,8 @@ namespace pt
         c->iteration += 1;
         e->launchCount = 0;
         e->segmentCount = 0;
-        uint32_t completed = 0;
-        bool launchable = false, unfinished = false;
-        for (uint32_t i = 0; i < e->orderCount; i++)
-        {
-            JobView& J = ev.jobs[ev.order[i]];
-            if (J.state != kJobActive) continue;
-            const uint32_t count = foldable_passes(J);
-            for (uint32_t q = 0; q < count; q++) J.passDone[(static_cast<uint64_t>(J.folded) + q) % J.ring] = 0;
-            J.folded += count;
-            if (J.folded == job_passes(J))
-            {
-                J.state = kJobDone;
-                completed++;
-                continue;
-            }
-            unfinished = true;
-            if (job_window_end(J) > J.launched) launchable = true;
-        }
+        const uint32_t completed = completedJobs;
+        const bool launchable = launchableJobs != 0, unfinished = unfinishedJobs != 0;
         e->completed += completed;
         e->sliceIterations += 1;
         const bool idle = next == 0 && !launchable;
@@ -2331,7 +2360,7 @@ namespace pt
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         fold_kernel<<<L.shadeBlocks, 256, 0, s>>>(L.ev);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        engine_advance_kernel<<<1, 1, 0, s>>>(L.wf, L.ev, L.handle, L.graphLoop);
+        engine_advance_kernel<<<1, 256, 0, s>>>(L.wf, L.ev, L.handle, L.graphLoop);
         return cudaGetLastError();
     }
 
