@@ -139,6 +139,21 @@ def test_tiny_pool_and_single_pass_ring(resident, frame_renderers):
         srv.close()
 
 
+def test_many_single_pixel_jobs(resident, frame_renderers):
+    """1,200 jobs of one pixel in flight together: a regeneration block retires paths of more jobs and
+    passes than its shared-memory pass table and plan-segment copy hold, so both fall back to
+    global memory. Every image still equals the frame renderer's."""
+    srv, ids = make_server(resident, pool_size=1 << 14, max_jobs=2048)
+    try:
+        jobs = [("cornell-all", 1 + (k % 2), 1, (1, 4)[k % 2], 3 + k % 3, True, 7 * k) for k in range(1200)]
+        jids = [submit(srv, ids, resident, job) for job in jobs]
+        for jid, job in zip(jids, jobs):
+            check_job(srv, jid, frame_renderers, resident, job)
+        assert srv.stats()["completed_jobs"] == len(jobs)
+    finally:
+        srv.close()
+
+
 def test_one_job_at_a_time(resident, frame_renderers):
     srv, ids = make_server(resident, pool_size=1 << 16, max_active_jobs=1)
     try:
