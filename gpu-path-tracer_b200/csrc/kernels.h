@@ -20,7 +20,7 @@ namespace pt
         uint32_t refill;
         uint32_t refillShadow;     // the same threshold for the shadow-ray (any-hit) traversal
         int occupancy;             // traversal kernel variant: 1, 10 or 12 resident blocks per SM targeted
-        int shadeBlocks;           // grid of the 256-thread bookkeeping kernels (regeneration, folding)
+        int shadeBlocks;           // grid of the 256-thread regeneration-queue kernel (the reference-structure layout)
         int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
         uint32_t bvhFormat;        // kBvh8Quantised or kBvh2Fp32 (scene.nodes2 must be present)
@@ -47,7 +47,7 @@ namespace pt
         uint32_t refill;
         uint32_t refillShadow;
         int occupancy;
-        int shadeBlocks;           // grid of the 256-thread bookkeeping kernels (regeneration, folding)
+        int shadeBlocks;           // grid of the 256-thread folding kernel
         int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;
         // Optional fork/join of the shading kernels, as in IterationLaunch. nullptr = in order.
