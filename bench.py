@@ -466,6 +466,31 @@ def precision_section(knobs):
     return out
 
 
+def summary(line):
+    """The line's comparisons in a few numbers: headline, plain form, the reference's own kernels on the
+    same GPU, the batched mix, and serving latency per arrival rate."""
+    def get(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+    out = {"value": line["value"], "e2e": line["e2e"]["value"], "roofline_frac": line["roofline"]["frac"],
+           "dram_frac": line["roofline"].get("dram_frac"),
+           "plain_form_speedup_of_value": get(line, "plain_form", "speedup_of_value"),
+           "reference_build_b200_value": get(line, "reference_build_b200", "value"),
+           "reference_build_b200_speedup_of_value": get(line, "reference_build_b200", "speedup_of_value"),
+           "batched_speedup_vs_plain_form": get(line, "batched", "speedup_vs_plain_form"),
+           "cpu_baseline_value": get(line, "cpu_baseline", "value")}
+    serving = line.get("serving")
+    if isinstance(serving, dict) and isinstance(serving.get("served"), dict):
+        out["serving_latency_s"] = {
+            rate: {"served_p50": v.get("p50_latency_s"), "served_p99": v.get("p99_latency_s"),
+                   "plain_p50": get(serving, "plain", rate, "p50_latency_s"), "plain_p99": get(serving, "plain", rate, "p99_latency_s")}
+            for rate, v in serving["served"].items() if isinstance(v, dict)}
+    return out
+
+
 def b200_arm(args):
     import torch
     import pathtracer
@@ -585,8 +610,11 @@ def b200_arm(args):
         "iterations_per_step": iters / args.steps,
         "phase_ms_per_step": {k: sum(s["phase_ms"][k] for s in stats) / args.steps for k in ("trace", "shade", "shadow", "regen")},
         "scene_upload_s": upload_s,
-        "roofline": {"kernel": "trace_kernel<closest> (BVH8 closest hit)", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": "trace_kernel<closest> (BVH8 closest hit)", "bound": "latency", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "dram_frac": (traffic / per_launch_s / 1e9 / peak) if traffic else None,
+                     "bound_note": "load latency and lane divergence: the algorithmic node/triangle bytes (frac) are served mostly "
+                                   "by L1/L2; dram_frac is the DRAM traffic of a launch over its duration against the same peak",
                      "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": per_launch_bytes,
                      "bytes_model": f"{TRACE_ALGO_BYTES_PER_RAY} B/ray (ray in, material-queue entry out, every ray counted as a hit) + {NODE_BYTES} B/node visited + {TRIANGLE_BYTES} B/triangle tested",
@@ -663,6 +691,7 @@ def b200_arm(args):
         total, times, sample = run_cpu(WORKLOAD["scene"], args.cpu_seconds, threads, steps=1)
         line["cpu_baseline"] = {"value": total / times[0], "unit": "paths/s", "cores": threads, "kind": "port",
                                 "sample": sample}
+    line["summary"] = summary(line)  # last key: a truncated tail of the line still carries it
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

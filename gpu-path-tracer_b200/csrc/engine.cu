@@ -98,7 +98,7 @@ namespace pt
         // pointers; a ray only needs its scene's root node (SceneEntry).
         struct ScenePack
         {
-            DeviceBuffer nodes, tris, shading, materials, textures, lights, bins, entries;
+            DeviceBuffer nodes, tris, shading, materials, textures, lights, bins, binsPower, entries;
             std::vector<SceneEntry> entry;
             std::vector<std::unique_ptr<TextureObject>> textureObjects;
             uint32_t nodeCount = 0, triangleCount = 0, materialCount = 0, lightCount = 0, depth = 0;
@@ -115,6 +115,7 @@ namespace pt
                 v.textures = anyTextures ? textures.get<MaterialTextures>() : nullptr;
                 v.lights = lights.get<float4>();
                 v.bins = bins.get<uint4>();
+                v.binsPower = binsPower.get<uint4>();
                 v.lightCount = lightCount;
                 v.nodeCount = nodeCount;
                 v.triangleCount = triangleCount;
@@ -139,13 +140,14 @@ namespace pt
                 return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^24 BVH8 nodes");
             if (static_cast<uint64_t>(p.triangleCount) + s.triangleCount > kMaxTriangles)
                 return Status::Err(GPT_ERR_CAPACITY, "Resident scenes exceed 2^24 triangles");
-            DeviceBuffer nn, nt, ns, nm, nl, nb, ntex, ne;
+            DeviceBuffer nn, nt, ns, nm, nl, nb, nbp, ntex, ne;
             PT_TRY(Grow(nn, p.nodes, size_t(p.nodeCount) * sizeof(Node8), s.nodes, size_t(s.nodeCount) * sizeof(Node8), st));
             PT_TRY(Grow(nt, p.tris, size_t(p.triangleCount) * kTriangleVec4 * 16, s.tris, size_t(s.triangleCount) * kTriangleVec4 * 16, st));
             PT_TRY(Grow(ns, p.shading, size_t(p.triangleCount) * 144, s.shading, size_t(s.triangleCount) * 144, st));
             PT_TRY(Grow(nm, p.materials, size_t(p.materialCount) * sizeof(MaterialDev), s.materials, size_t(s.materialCount) * sizeof(MaterialDev), st));
             PT_TRY(Grow(nl, p.lights, size_t(p.lightCount) * 112, s.lights, size_t(s.lightCount) * 112, st));
             PT_TRY(Grow(nb, p.bins, size_t(p.lightCount) * 16, s.bins, size_t(s.lightCount) * 16, st));
+            PT_TRY(Grow(nbp, p.binsPower, size_t(p.lightCount) * 16, s.binsPower, size_t(s.lightCount) * 16, st));
             PT_CUDA("rebase nodes", launch_rebase_nodes(nn.get<Node8>() + p.nodeCount, s.nodeCount, p.nodeCount, p.triangleCount, st));
             uint32_t* triWords = reinterpret_cast<uint32_t*>(nt.get<float4>() + size_t(p.triangleCount) * kTriangleVec4);
             PT_CUDA("rebase triangles", launch_rebase_field(triWords + 3, s.triangleCount, kTriangleVec4 * 4, p.triangleCount, false, st));
@@ -156,6 +158,8 @@ namespace pt
             PT_CUDA("rebase lights", launch_rebase_field(lightWords + 26, s.lightCount, 28, p.materialCount, false, st));
             uint32_t* binWords = reinterpret_cast<uint32_t*>(nb.get<uint4>() + p.lightCount);
             PT_CUDA("rebase alias table", launch_rebase_field(binWords + 2, s.lightCount, 4, p.lightCount, true, st));
+            uint32_t* powerWords = reinterpret_cast<uint32_t*>(nbp.get<uint4>() + p.lightCount);
+            PT_CUDA("rebase alias table", launch_rebase_field(powerWords + 2, s.lightCount, 4, p.lightCount, true, st));
             const bool sceneTextures = !s.textures.empty();
             const bool anyTextures = p.anyTextures || sceneTextures;
             if (anyTextures)
@@ -183,6 +187,7 @@ namespace pt
             p.materials.swap(nm);
             p.lights.swap(nl);
             p.bins.swap(nb);
+            p.binsPower.swap(nbp);
             if (anyTextures) p.textures.swap(ntex);
             p.entries.swap(ne);
             p.entry = std::move(entries);
@@ -345,6 +350,9 @@ namespace pt
         {
             std::scoped_lock lock(mu_);
             if (d.scene >= pack_.entry.size()) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown scene id");
+            if (d.rng_policy != GPT_RNG_PHILOX && d.rng_policy != GPT_RNG_PCG32) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown rng_policy");
+            if (d.light_sampling != GPT_LIGHTS_AREA && d.light_sampling != GPT_LIGHTS_POWER)
+                return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown light_sampling");
             JobRecord J;
             J.desc = d;
             // clamps of StartSimulation (Renderer.cpp:340-344, 366-367)
@@ -630,6 +638,8 @@ namespace pt
                 v.totalSamples = uint64_t(J.spp) * J.pixels;
                 v.sampleRadiance = reinterpret_cast<float*>(base);
                 v.rngOffset = J.desc.rng_offset;
+                v.rngPolicy = J.desc.rng_policy;
+                v.lightMode = J.desc.light_sampling;
                 v.pixels = J.pixels;
                 v.ring = J.ring;
                 v.state = kJobActive;

@@ -6,8 +6,10 @@
 //   trace_kernel<any>      NEE shadow rays, any hit; unoccluded radiance added to the path slot
 //   regen_bits_kernel      finished paths -> per-sample radiance; new samples -> next ray queue
 //   advance_kernel         one thread: queue bookkeeping, log, loop condition (Renderer.cpp:573-619)
-// All arithmetic that reaches a result uses IEEE operators in the reference's order; the
-// library is compiled with -fmad=false.
+// Every expression that reaches a result is written in the reference's operator order. The
+// product library compiles this file as the reference's kernels are compiled (multiply-add
+// contraction, CUDA's sinf/cosf/powf/rsqrtf); the deterministic library compiles it with
+// -fmad=false and the IEEE definitions of pt_math.cuh (PT_CUDA_MATH).
 #include <curand_kernel.h>
 
 #include "kernels.h"
@@ -350,7 +352,7 @@ namespace pt
     {
         const float lengthSquared = dot(radiance, radiance);
         const float maxLengthSquared = maxLength * maxLength;
-        if (lengthSquared > maxLengthSquared) radiance = radiance * (maxLength * rsqrt_ieee(lengthSquared));
+        if (lengthSquared > maxLengthSquared) radiance = radiance * (maxLength * rsqrt_f(lengthSquared));
         return radiance;
     }
 
@@ -554,6 +556,100 @@ namespace pt
         phase_end(ctr, Work::kPhase);
     }
 
+    // ------------------------------------------------------------------ random numbers
+    // A path's stream, positioned at the number of 32-bit words it has drawn (kept in the path slot).
+    //   Philox (the reference's): cuRAND's device API, seed 1234, subsequence = sample index; the
+    //     position is curand_init's offset, which continues the stream bit for bit.
+    //   PCG32: PCG-XSH-RR with 64-bit state (O'Neill, "PCG: A Family of Simple Fast Space-Efficient
+    //     Statistically Good Algorithms for Random Number Generation", 2014), one stream per sample,
+    //     seeded by a hash of (seed, key) where key = pixel * spp + sample within the pixel (+ the
+    //     shard offset) names (pixel, sample) uniquely, and positioned by the LCG's jump-ahead (Brown,
+    //     "Random Number Generation with Arbitrary Strides", 1994). Uniforms are (w >> 8) 2^-24 +
+    //     2^-25, in (0, 1]. Stateless per draw position, so a slot needs no stored generator state.
+    __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z)  // splitmix64's finaliser (Steele, Lea, Flood, OOPSLA 2014)
+    {
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+
+    constexpr uint64_t kPcgMultiplier = 6364136223846793005ull;
+
+    struct Pcg32
+    {
+        uint64_t state, inc;
+        __device__ __forceinline__ uint32_t next()
+        {
+            const uint64_t old = state;
+            state = old * kPcgMultiplier + inc;
+            const uint32_t xorshifted = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+            const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+            return (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+        }
+        __device__ __forceinline__ float uniform() { return static_cast<float>(next() >> 8) * 0x1p-24f + 0x1p-25f; }
+        // state after `delta` more steps: the LCG's affine map raised to the delta-th power by squaring
+        __device__ __forceinline__ void advance(uint64_t delta)
+        {
+            uint64_t accMult = 1, accPlus = 0, curMult = kPcgMultiplier, curPlus = inc;
+            while (delta > 0)
+            {
+                if (delta & 1u)
+                {
+                    accMult *= curMult;
+                    accPlus = accPlus * curMult + curPlus;
+                }
+                curPlus = (curMult + 1) * curPlus;
+                curMult *= curMult;
+                delta >>= 1;
+            }
+            state = accMult * state + accPlus;
+        }
+        // the generator's seeding: stream (increment) from initseq, then initstate mixed in over two steps
+        __device__ __forceinline__ static Pcg32 seeded(uint64_t key)
+        {
+            Pcg32 g;
+            const uint64_t initstate = mix64(kRandomSeed ^ mix64(key));
+            const uint64_t initseq = mix64(key ^ 0x9E3779B97F4A7C15ull);
+            g.state = 0;
+            g.inc = (initseq << 1u) | 1u;
+            g.next();
+            g.state += initstate;
+            g.next();
+            return g;
+        }
+    };
+
+    struct PathRng
+    {
+        curandStatePhilox4_32_10_t philox;
+        Pcg32 pcg;
+        bool usePcg;
+        __device__ __forceinline__ void init(uint32_t policy, uint64_t key, uint32_t position)
+        {
+            usePcg = policy == kRngPcg32;
+            if (usePcg)
+            {
+                pcg = Pcg32::seeded(key);
+                pcg.advance(position);
+            }
+            else
+                curand_init(kRandomSeed, static_cast<unsigned long long>(key), static_cast<unsigned long long>(position), &philox);
+        }
+        __device__ __forceinline__ float4 uniform4()
+        {
+            if (usePcg)
+            {
+                const float x = pcg.uniform();
+                const float y = pcg.uniform();
+                const float z = pcg.uniform();
+                const float w = pcg.uniform();
+                return make_float4(x, y, z, w);
+            }
+            return curand_uniform4(&philox);
+        }
+        __device__ __forceinline__ float uniform() { return usePcg ? pcg.uniform() : curand_uniform(&philox); }
+    };
+
     // ------------------------------------------------------------------ paths
     __device__ __forceinline__ uint32_t pack_meta(uint32_t depth, bool delta, uint32_t job)
     {
@@ -588,9 +684,9 @@ namespace pt
     __device__ __forceinline__ void start_path(const JobView& job, uint32_t jobIndex, const Wavefront& wf, uint32_t slot, uint32_t sample,
                                                uint32_t queue, uint32_t position)
     {
-        curandStatePhilox4_32_10_t rng;
-        curand_init(kRandomSeed, static_cast<unsigned long long>(sample) + job.rngOffset, 0ull, &rng);
-        const float4 r = curand_uniform4(&rng);
+        PathRng rng;
+        rng.init(job.rngPolicy, static_cast<uint64_t>(sample) + job.rngOffset, 0u);
+        const float4 r = rng.uniform4();
         float3 o, d;
         camera_ray(job, sample, make_float2(r.x, r.y), o, d);
         wf.slotT[slot] = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(pack_meta(0, true, jobIndex)));
@@ -732,7 +828,7 @@ namespace pt
     __device__ __forceinline__ float3 safe_normalize(float3 v, float3 fallback)
     {
         const float l2 = dot(v, v);
-        if (l2 > 1e-16f) return v * rsqrt_ieee(l2);
+        if (l2 > 1e-16f) return v * rsqrt_f(l2);
         return fallback;
     }
 
@@ -749,7 +845,7 @@ namespace pt
         n = safe_normalize(n, make_float3(0.0f, 0.0f, 1.0f));
         t = t - n * dot(n, t);
         const float l2 = dot(t, t);
-        if (l2 > 1e-16f) t = t * rsqrt_ieee(l2);
+        if (l2 > 1e-16f) t = t * rsqrt_f(l2);
         else t = frame_from_normal(n).tangent;
         return Frame{t, cross(n, t) * sign, n};
     }
@@ -858,7 +954,7 @@ namespace pt
         const float cosTheta = sqrtf(u.y);
         const float sinTheta = sqrtf(1.0f - u.y);
         float s, c;
-        sincos_det(phi, &s, &c);
+        sincos_f(phi, &s, &c);
         return make_float3(sinTheta * c, sinTheta * s, cosTheta);
     }
 
@@ -872,6 +968,7 @@ namespace pt
     struct LightSet
     {
         uint32_t base, count;
+        const uint4* bins;  // the job's alias table (area or power weights)
     };
 
     // SampleLightTriangle (MaterialEval.cu:171-192) with the alias table (AliasTableView.hpp:32-60).
@@ -884,13 +981,13 @@ namespace pt
         bin = bin < n - 1u ? bin : n - 1u;
         const float up = fminf(scaledU - static_cast<float>(bin), kOneMinusEpsilon);
         bin += ls.base;
-        const uint4 b = ldg4(sc.bins + bin);
+        const uint4 b = ldg4(ls.bins + bin);
         uint32_t index = bin;
         float pmf = __uint_as_float(b.y);
         if (!(up < __uint_as_float(b.x)))
         {
             index = b.z;
-            pmf = __uint_as_float(__ldg(&sc.bins[index].y));
+            pmf = __uint_as_float(__ldg(&ls.bins[index].y));
         }
         const float4* L = sc.lights + static_cast<size_t>(index) * 7;
         const float4 l0 = ldg4(L), l1 = ldg4(L + 1), l2 = ldg4(L + 2), l3 = ldg4(L + 3), l4 = ldg4(L + 4);
@@ -962,7 +1059,7 @@ namespace pt
             const float3 refl = normalize(reflect(dir, f.normal));
             const float cosThetaR = fmaxf(dot(refl, lh.wi), 0.0f);
             const float3 diffuseBrdf = albedo / kPi;
-            const float3 specularBrdf = specular * (shininess + 2.0f) * kInvTwoPi * pow_det(cosThetaR, shininess);
+            const float3 specularBrdf = specular * (shininess + 2.0f) * kInvTwoPi * pow_f(cosThetaR, shininess);
             brdf = diffuseBrdf + specularBrdf;
         }
         else
@@ -1009,7 +1106,7 @@ namespace pt
     {
         return ggx_g1(w, alpha) / fabsf(w.z) * ggx_d(wm, alpha) * fabsf(dot(w, wm));
     }
-    __device__ __forceinline__ float3 fresnel_schlick(float3 f0, float c) { return f0 + (1.0f - f0) * pow5_det(1.0f - c); }
+    __device__ __forceinline__ float3 fresnel_schlick(float3 f0, float c) { return f0 + (1.0f - f0) * pow5_f(1.0f - c); }
 
     __device__ __forceinline__ float3 trowbridge_sample(float3 w, float alpha, float2 u)
     {
@@ -1020,7 +1117,7 @@ namespace pt
         const float r = sqrtf(u.x);
         const float theta = 2.0f * kPi * u.y;
         float sn, cs;
-        sincos_det(theta, &sn, &cs);
+        sincos_f(theta, &sn, &cs);
         float2 disk = make_float2(r * cs, r * sn);
         const float h = sqrtf(1.0f - disk.x * disk.x);
         disk.y = lerpf(h, disk.y, (1 + wh.z) * 0.5f);
@@ -1134,17 +1231,17 @@ namespace pt
         else
         {
             const float phi = 2.0f * kPi * rs.x;
-            const float cosTheta = pow_det(rs.y, 1.0f / (shininess + 1.0f));
+            const float cosTheta = pow_f(rs.y, 1.0f / (shininess + 1.0f));
             const float sinTheta = sqrtf(1.0f - cosTheta * cosTheta);
             float sn, cs;
-            sincos_det(phi, &sn, &cs);
+            sincos_f(phi, &sn, &cs);
             wi = frame_from_normal(refl).from_local(make_float3(sinTheta * cs, sinTheta * sn, cosTheta));
         }
         const float cosThetaI = fmaxf(dot(f.normal, wi), 0.0f);
         const float gCos = fmaxf(dot(s.gN, wi), 0.0f);
         if (cosThetaI <= 0.0f || gCos <= 0.0f) return scatter_terminated();
         const float cosThetaR = fmaxf(dot(refl, wi), 0.0f);
-        const float lobe = kInvTwoPi * pow_det(cosThetaR, shininess);
+        const float lobe = kInvTwoPi * pow_f(cosThetaR, shininess);
         const float diffusePdf = cosThetaI * kInvPi;
         const float specularPdf = (shininess + 1.0f) * lobe;
         const float pdf = dsp * diffusePdf + ssp * specularPdf;
@@ -1200,7 +1297,7 @@ namespace pt
                 const JobView& job = jobs[jobIndex];
                 const uint32_t limit = __ldg(&job.depthLimit);
                 const uint4 se = __ldg(reinterpret_cast<const uint4*>(scenes) + (tag >> kSlotBits));
-                const LightSet ls{se.y, se.z};
+                const LightSet ls{se.y, se.z, __ldg(&job.lightMode) == kLightsPower ? sc.binsPower : sc.bins};
                 const bool nee = __ldg(&job.nee) != 0 && ls.count > 0;
                 const float3 T = f3(T4);
                 uint32_t rngPos = __float_as_uint(L4.w);
@@ -1249,17 +1346,16 @@ namespace pt
                     nextGn = s.gN;
                     const MaterialDev& m = sc.materials[s.material];
                     const Frame f = shading_frame(sc, s, m);
-                    curandStatePhilox4_32_10_t rng;
-                    curand_init(kRandomSeed, static_cast<unsigned long long>(wf.slotSample[slot]) + __ldg(&job.rngOffset),
-                                static_cast<unsigned long long>(rngPos), &rng);
+                    PathRng rng;
+                    rng.init(__ldg(&job.rngPolicy), static_cast<uint64_t>(wf.slotSample[slot]) + __ldg(&job.rngOffset), rngPos);
                     if (MODEL == 1)  // Diffuse (:311-350, :270-309)
                     {
                         const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
-                        const float4 ind = curand_uniform4(&rng);
+                        const float4 ind = rng.uniform4();
                         rngPos += 4;
                         if (nee)
                         {
-                            const float4 dir4 = curand_uniform4(&rng);
+                            const float4 dir4 = rng.uniform4();
                             rngPos += 4;
                             sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(dir4), albedo, false, f3(0.0f), 0.0f);
                         }
@@ -1277,7 +1373,7 @@ namespace pt
                     else if (MODEL == 2)  // Mirror (:352-392)
                     {
                         const float3 reflectance = slot_rgb(sc, s.material, 1, s.uv, m.specular);
-                        const float rr = curand_uniform(&rng);
+                        const float rr = rng.uniform();
                         rngPos += 1;
                         const float3 wi = reflect(d, f.normal);
                         cont = continue_path(depth, T, limit, reflectance, rr);
@@ -1290,7 +1386,7 @@ namespace pt
                         const float3 albedo = slot_rgb(sc, s.material, 0, s.uv, m.color);
                         const float3 specular = slot_rgb(sc, s.material, 1, s.uv, m.specular);
                         const float shininess = slot_scalar(sc, s.material, 2, s.uv, &m.shininess) * (1000.0f - 1.0f) + 1.0f;
-                        const float4 ind = curand_uniform4(&rng);
+                        const float4 ind = rng.uniform4();
                         rngPos += 4;
                         if (nee) sh = direct_lambert_phong(sc, ls, T, d, s, f, f3(ind), albedo, true, specular, shininess);
                         const Scatter sc2 = indirect_phong(depth, T, limit, d, s, f, ind, albedo, specular, shininess);
@@ -1306,11 +1402,11 @@ namespace pt
                         const float alpha = fmaxf(rma.x * rma.x, 0.001f);
                         const float metallic = rma.y;
                         const float ior = __ldg(&m.ior);
-                        const float4 ind = curand_uniform4(&rng);
+                        const float4 ind = rng.uniform4();
                         rngPos += 4;
                         if (nee)
                         {
-                            const float4 dir4 = curand_uniform4(&rng);
+                            const float4 dir4 = rng.uniform4();
                             rngPos += 4;
                             sh = direct_ggx(sc, ls, T, d, s, f, f3(dir4), base, alpha, metallic, ior);
                         }
@@ -1479,7 +1575,7 @@ namespace pt
         {
             const float hdr = acc[ch] * invSpp;
             const float ldr = hdr / (hdr + 1.0f);
-            const float g = pow_det(ldr, 1.0f / 2.2f);
+            const float g = pow_f(ldr, 1.0f / 2.2f);
             rgb[ch] = static_cast<uint32_t>(static_cast<unsigned char>(clampf(g * 255.0f, 0.0f, 255.0f)));
         }
         return rgb[0] | (rgb[1] << 8) | (rgb[2] << 16) | (255u << 24);
@@ -1959,186 +2055,6 @@ namespace pt
         for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) framebuffer[i] = value;
     }
 
-    // ------------------------------------------------------------------ scene: lights and alias table on the device
-    // LightSampler::BuildSync (LightSampler.cpp:5-40): emissive triangles in input order.
-    __global__ void light_flag_kernel(const float4* shading, const MaterialDev* materials, uint32_t n, uint32_t* flags)
-    {
-        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        {
-            const uint32_t mat = __float_as_uint(shading[static_cast<size_t>(t) * 9 + 6].w);
-            flags[t] = materials[mat].model == kModelEmissive ? 1u : 0u;
-        }
-    }
-
-    __global__ void light_record_kernel(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
-                                        const uint32_t* flags, const uint32_t* index, float4* lights, double* weights)
-    {
-        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        {
-            if (!flags[t]) continue;
-            const float* p = positions + static_cast<size_t>(t) * 9;
-            const float3 p0 = make_float3(p[0], p[1], p[2]);
-            const float3 e1 = make_float3(p[3], p[4], p[5]) - p0;
-            const float3 e2 = make_float3(p[6], p[7], p[8]) - p0;
-            const float area = 0.5f * length(cross(e1, e2));
-            const float4 g = shading[static_cast<size_t>(t) * 9 + 6];
-            const uint32_t mat = __float_as_uint(g.w);
-            const uint32_t li = index[t];
-            float4* L = lights + static_cast<size_t>(li) * 7;
-            L[0] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(t));
-            L[1] = make_float4(e1.x, e1.y, e1.z, area);
-            L[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
-            L[3] = make_float4(g.x, g.y, g.z, 0.0f);
-            L[4] = make_float4(materials[mat].emission[0], materials[mat].emission[1], materials[mat].emission[2], 0.0f);
-            // uv0, uv1 - uv0, uv2 - uv0 (LightSampler.cpp:28-30) and the material for its emission texture
-            const float4 u01 = shading[static_cast<size_t>(t) * 9 + 7], u2 = shading[static_cast<size_t>(t) * 9 + 8];
-            L[5] = make_float4(u01.x, u01.y, u01.z - u01.x, u01.w - u01.y);
-            L[6] = make_float4(u2.x - u01.x, u2.y - u01.y, __uint_as_float(mat), 0.0f);
-            weights[li] = static_cast<double>(area);
-        }
-    }
-
-    // Triangle records of the shading pass (Renderer.cpp:159-213): normals, tangents, geometric
-    // normal normalize(cross(e1, e2)), material, uvs; 144 bytes per triangle.
-    __global__ void shading_record_kernel(const float* positions, const float* normals, const float* tangents, const float* uvs,
-                                          const uint32_t* materialIds, uint32_t n, float4* shading)
-    {
-        for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
-        {
-            const float* p = positions + static_cast<size_t>(t) * 9;
-            const float* nn = normals + static_cast<size_t>(t) * 9;
-            const float* tt = tangents + static_cast<size_t>(t) * 12;
-            const float* uu = uvs + static_cast<size_t>(t) * 6;
-            const float3 p0 = make_float3(p[0], p[1], p[2]);
-            const float3 e1 = make_float3(p[3], p[4], p[5]) - p0;
-            const float3 e2 = make_float3(p[6], p[7], p[8]) - p0;
-            const float3 gn = normalize(cross(e1, e2));
-            float4* S = shading + static_cast<size_t>(t) * 9;
-            S[0] = make_float4(nn[0], nn[1], nn[2], 0.0f);
-            S[1] = make_float4(nn[3], nn[4], nn[5], 0.0f);
-            S[2] = make_float4(nn[6], nn[7], nn[8], 0.0f);
-            S[3] = make_float4(tt[0], tt[1], tt[2], tt[3]);
-            S[4] = make_float4(tt[4], tt[5], tt[6], tt[7]);
-            S[5] = make_float4(tt[8], tt[9], tt[10], tt[11]);
-            S[6] = make_float4(gn.x, gn.y, gn.z, __uint_as_float(materialIds[t]));
-            S[7] = make_float4(uu[0], uu[1], uu[2], uu[3]);
-            S[8] = make_float4(uu[4], uu[5], 0.0f, 0.0f);
-        }
-    }
-
-    // Exclusive scan, one block of 1024 threads per 1024 elements; block totals out.
-    template <typename T>
-    __global__ void scan_block_kernel(const T* in, T* out, T* blockSums, uint32_t n)
-    {
-        __shared__ T warpSums[32];
-        const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
-        const T x = i < n ? in[i] : T(0);
-        T v = x;
-        const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-            const T y = __shfl_up_sync(0xFFFFFFFFu, v, o);
-            if (lane >= static_cast<uint32_t>(o)) v = v + y;
-        }
-        if (lane == 31) warpSums[warp] = v;
-        __syncthreads();
-        if (warp == 0)
-        {
-            T w = warpSums[lane];
-            for (int o = 1; o < 32; o <<= 1)
-            {
-                const T y = __shfl_up_sync(0xFFFFFFFFu, w, o);
-                if (lane >= static_cast<uint32_t>(o)) w = w + y;
-            }
-            warpSums[lane] = w;
-        }
-        __syncthreads();
-        const T warpOffset = warp > 0 ? warpSums[warp - 1] : T(0);
-        const T inclusive = v + warpOffset;
-        if (i < n) out[i] = inclusive - x;
-        if (threadIdx.x == 1023u && blockSums) blockSums[blockIdx.x] = inclusive;
-    }
-
-    template <typename T>
-    __global__ void scan_add_kernel(T* data, const T* blockOffsets, uint32_t n)
-    {
-        const uint32_t i = blockIdx.x * 1024u + threadIdx.x;
-        if (i < n && blockIdx.x > 0) data[i] = data[i] + blockOffsets[blockIdx.x];
-    }
-
-    __global__ void scan_total_kernel(const uint32_t* flags, const uint32_t* excl, uint32_t n, uint32_t* total)
-    {
-        *total = n ? excl[n - 1] + flags[n - 1] : 0u;
-    }
-
-    // AliasTable<uint32_t>::BuildSync (AliasTable.hpp:22-84): p_i = w_i / sum (sum accumulated in
-    // FP64 by the device prefix sum, rounded to float), pHat = p * n, then the reference's
-    // sequential pairing of the last light (under) and last heavy (over) outcome. The pairing is
-    // inherently ordered, so one thread runs it; under/over stacks live in the scratch arrays.
-    __global__ void alias_build_kernel(const double* weights, const double* prefix, uint32_t n, uint4* bins,
-                                       uint32_t* stackIndex, float* stackValue)
-    {
-        if (blockIdx.x != 0 || threadIdx.x != 0 || n == 0) return;
-        const float sum = static_cast<float>(prefix[n - 1] + weights[n - 1]);
-        uint32_t* underIdx = stackIndex;
-        uint32_t* overIdx = stackIndex + n;
-        float* underVal = stackValue;
-        float* overVal = stackValue + n;
-        uint32_t nu = 0, no = 0;
-        for (uint32_t i = 0; i < n; i++)
-        {
-            const float p = static_cast<float>(weights[i]) / sum;
-            bins[i] = make_uint4(__float_as_uint(0.0f), __float_as_uint(p), 0u, i);
-            const float pHat = p * static_cast<float>(n);
-            if (pHat < 1)
-            {
-                underIdx[nu] = i;
-                underVal[nu] = pHat;
-                nu++;
-            }
-            else
-            {
-                overIdx[no] = i;
-                overVal[no] = pHat;
-                no++;
-            }
-        }
-        while (nu > 0 && no > 0)
-        {
-            nu--;
-            no--;
-            const uint32_t ui = underIdx[nu], oi = overIdx[no];
-            const float uv = underVal[nu], ov = overVal[no];
-            bins[ui].x = __float_as_uint(uv);
-            bins[ui].z = oi;
-            const float excess = uv + ov - 1;
-            if (excess < 1)
-            {
-                underIdx[nu] = oi;
-                underVal[nu] = excess;
-                nu++;
-            }
-            else
-            {
-                overIdx[no] = oi;
-                overVal[no] = excess;
-                no++;
-            }
-        }
-        while (no > 0)
-        {
-            no--;
-            bins[overIdx[no]].x = __float_as_uint(1.0f);
-            bins[overIdx[no]].z = kInvalid;
-        }
-        while (nu > 0)
-        {
-            nu--;
-            bins[underIdx[nu]].x = __float_as_uint(1.0f);
-            bins[underIdx[nu]].z = kInvalid;
-        }
-    }
-
     // ------------------------------------------------------------------ host launchers
     namespace
     {
@@ -2421,71 +2337,5 @@ namespace pt
         if (occOut) return launch_trace<true>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
         return launch_trace<false>(b, sc.depth, 1, blocks, threads, 32, errorFlags, s);
     }
-
-    cudaError_t launch_shading_records(const float* positions, const float* normals, const float* tangents, const float* uvs,
-                                       const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t s)
-    {
-        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
-        shading_record_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(positions, normals, tangents, uvs, materialIds, n, shading);
-        return cudaGetLastError();
-    }
-
-    template <typename T>
-    static cudaError_t exclusive_scan(const T* in, T* out, uint32_t n, T* scratch, cudaStream_t s)
-    {
-        // scratch: >= ceil(n/1024) + ceil(n/1024^2) + ... + 3 elements
-        if (n == 0) return cudaSuccess;
-        const uint32_t blocks = (n + 1023) / 1024;
-        T* sums = scratch;
-        scan_block_kernel<T><<<blocks, 1024, 0, s>>>(in, out, blocks > 1 ? sums : nullptr, n);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess || blocks == 1) return e;
-        e = exclusive_scan<T>(sums, sums, blocks, scratch + blocks, s);
-        if (e != cudaSuccess) return e;
-        scan_add_kernel<T><<<blocks, 1024, 0, s>>>(out, sums, n);
-        return cudaGetLastError();
-    }
-
-    cudaError_t launch_light_build(const float4* shading, const MaterialDev* materials, uint32_t n,
-                                   uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCountDev, cudaStream_t s)
-    {
-        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
-        light_flag_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(shading, materials, n, flags);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-        e = exclusive_scan<uint32_t>(flags, index, n, scanScratch, s);
-        if (e != cudaSuccess) return e;
-        scan_total_kernel<<<1, 1, 0, s>>>(flags, index, n, lightCountDev);
-        return cudaGetLastError();
-    }
-
-    cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
-                                     const uint32_t* flags, const uint32_t* index, float4* lights, double* weights, cudaStream_t s)
-    {
-        const uint32_t blocks = (n + 255) / 256 < 16384 ? (n + 255) / 256 : 16384;
-        light_record_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(positions, shading, materials, n, flags, index, lights, weights);
-        return cudaGetLastError();
-    }
-
-    cudaError_t launch_alias_build(const double* weights, uint32_t n, double* prefix, double* scanScratch, uint4* bins,
-                                   uint32_t* stackIndex, float* stackValue, cudaStream_t s)
-    {
-        if (n == 0) return cudaSuccess;
-        cudaError_t e = exclusive_scan<double>(weights, prefix, n, scanScratch, s);
-        if (e != cudaSuccess) return e;
-        alias_build_kernel<<<1, 32, 0, s>>>(weights, prefix, n, bins, stackIndex, stackValue);
-        return cudaGetLastError();
-    }
-
-    size_t scan_scratch_elements(uint32_t n)
-    {
-        size_t total = 3;
-        uint32_t m = n;
-        while (m > 1)
-        {
-            m = (m + 1023) / 1024;
-            total += m;
-        }
-        return total;
-    }
 }
+

@@ -73,9 +73,13 @@ namespace pt
                                        const uint32_t* materialIds, uint32_t n, float4* shading, cudaStream_t stream);
     cudaError_t launch_light_build(const float4* shading, const MaterialDev* materials, uint32_t n,
                                    uint32_t* flags, uint32_t* index, uint32_t* scanScratch, uint32_t* lightCount, cudaStream_t stream);
-    cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials, uint32_t n,
-                                     const uint32_t* flags, const uint32_t* index, float4* lights, double* weights, cudaStream_t stream);
+    cudaError_t launch_light_records(const float* positions, const float4* shading, const MaterialDev* materials,
+                                     const MaterialTextures* textures, uint32_t n, const uint32_t* flags, const uint32_t* index,
+                                     float4* lights, double* weights, double* powerWeights, cudaStream_t stream);
     cudaError_t launch_alias_build(const double* weights, uint32_t n, double* prefix, double* scanScratch, uint4* bins,
                                    uint32_t* stackIndex, float* stackValue, cudaStream_t stream);
     size_t scan_scratch_elements(uint32_t n);
+    size_t alias_power_scratch_bytes(uint32_t n);
+    cudaError_t launch_alias_build_power(const double* weights, const double* areaWeights, uint32_t n, void* scratch, uint4* bins,
+                                         cudaStream_t stream);
 }

@@ -18,6 +18,15 @@
 // Nothing here reads a value before this call has written it, so no clearing is needed. Two
 // calls whose work overlaps on the GPU (different streams, or different host threads on the
 // same device without ordering) race on the array and corrupt each other's tables: order them.
+//
+// The cached address belongs to the device's current primary context. A device reset
+// (cudaDeviceReset) after the first call tears that context down and is not supported: the
+// library would keep using the old address.
+//
+// The weights must be finite and non-negative with a positive sum, as the scene upload's
+// emitter areas are (the reference asserts the sum, AliasTable.hpp:24). Other weights give a
+// table of NaN or infinite probabilities; the entry point does not read them back to check.
+#include <cstdint>
 #include <mutex>
 
 #include "../../include/gpt_b200.h"
@@ -73,6 +82,8 @@ extern "C" int gpt_build_alias_table_noalloc(const float* weights, uint32_t ligh
     static_assert(kScanElements >= 3 + (kMaxLights + 1023) / 1024 + 2, "scan scratch too small");
     if (light_count == 0) return GPT_OK;
     if (!weights || !bins) return GPT_ERR_INVALID_ARGUMENT;
+    // the kernels read 4-byte weights and store whole 16-byte bins
+    if (reinterpret_cast<uintptr_t>(bins) % 16 != 0 || reinterpret_cast<uintptr_t>(weights) % 4 != 0) return GPT_ERR_INVALID_ARGUMENT;
     if (light_count > kMaxLights) return GPT_ERR_CAPACITY;
     if (pt::scan_scratch_elements(light_count) > kScanElements) return GPT_ERR_CAPACITY;
     void* base = nullptr;

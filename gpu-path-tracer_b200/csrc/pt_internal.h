@@ -6,7 +6,7 @@
 //                           v0 and e1 in one 256-bit load, e2 in a 128-bit one)
 //   triangle shading 144 B  3 normals, 3 tangents, gN|material, uvs (Triangle.hpp:24-38 layout), input order
 //   light           112 B   v0|index, e1|area, e2, gN, emission, uv0|uvE1, uvE2|material
-//   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14)
+//   alias bin         16 B  q, p, alias, value (AliasTableView.hpp:8-14); two tables, area and power weights
 //   path slot         36 B  throughput|depth/flags/job, radiance|rng position, sample index
 //   ray queue entry   32 B  origin|tag, direction|tMax   (x2, ping-pong; tag = slot | scene << 24)
 //   material queue    48 B  origin|tag, direction|tMax, triangle|u|v|t   (x6, one per shading model: the
@@ -38,6 +38,23 @@ namespace pt
     constexpr uint32_t kTriangleVec4 = 4;         // 16-byte words per traversal triangle record (64 B)
     constexpr uint32_t kMaxJobs = 65536;
     constexpr uint32_t kMaxRing = 256;
+
+    // Random-number policy of a job. Philox: cuRAND Philox4_32_10, seed 1234, subsequence = sample
+    // index (the reference's streams, PathData.hpp:37-73). PCG32: a per-sample PCG32 stream seeded by
+    // a hash of (seed, pixel, sample), O'Neill's PCG-XSH-RR 64/32.
+    enum RngPolicy : uint32_t
+    {
+        kRngPhilox = 0,
+        kRngPcg32 = 1,
+    };
+
+    // Light selection of NEE. Area: probability proportional to the emitter's area, the reference's
+    // LightSampler (LightSampler.cpp:16-19). Power: proportional to area x luminance of the emission.
+    enum LightMode : uint32_t
+    {
+        kLightsArea = 0,
+        kLightsPower = 1,
+    };
 
     // BVH8 node, 128 bytes = 8 x uint4, loaded as one L1 line.
     //  w[0] = px, py, pz (float bits), ex | ey<<8 | ez<<16 | innerMask<<24   (biased float exponents of the scales)
@@ -108,7 +125,8 @@ namespace pt
         const MaterialDev* materials;
         const MaterialTextures* textures;  // per material, nullptr when the scene has no image textures
         const float4* lights;     // 7 per light
-        const uint4* bins;        // alias table
+        const uint4* bins;        // alias table, area weights (the reference's light sampler)
+        const uint4* binsPower;   // alias table, power weights (area x emission luminance)
         uint32_t lightCount;
         uint32_t nodeCount;
         uint32_t triangleCount;
@@ -143,7 +161,8 @@ namespace pt
         float4* accum;            // [pixels][2]: Kahan sum (xyz), compensation (xyz)
         uint32_t* framebuffer;    // RGBA8, written when the last pass is folded
         uint32_t* passDone;       // [ring] finished samples of the pass held by each ring buffer
-        uint64_t pad2;
+        uint32_t rngPolicy;       // RngPolicy
+        uint32_t lightMode;       // LightMode
     };
 
     enum JobState : uint32_t

@@ -1,26 +1,35 @@
-// Vector algebra and the deterministic transcendental functions of the path tracer.
+// Vector algebra and the transcendental functions of the path tracer.
 //
-// The whole library is compiled with -fmad=false (no multiply-add contraction) and
-// IEEE division / square root, so each float expression below rounds once per
-// operator, in source order. The scalar operator order of the vector helpers is the
-// one of cuda-samples' helper_math.h that the reference kernels use
-// (External/cuda-samples/Common/helper_math.h: dot :1264, cross :1436, reflect :1427,
-// lerp :1154, clamp :1168), so expressions written like the reference's give the
-// same bits.
+// The scalar operator order of the vector helpers is the one of cuda-samples' helper_math.h that
+// the reference kernels use (External/cuda-samples/Common/helper_math.h: dot :1264, cross :1436,
+// reflect :1427, lerp :1154, clamp :1168, normalize :1325), so expressions written like the
+// reference's compile to the same operations.
 //
-// Transcendentals: the reference calls CUDA's sinf/cosf/powf/rsqrtf
-// (MaterialEval.cu:224-228, 397, 589-591, 649; Image.cu:31; helper_math normalize).
-// Here each is defined from the mathematics and evaluated in IEEE double, rounded
-// once to float: sin/cos by reduction modulo pi/2 and Taylor series to r^15/r^16;
-// pow(x, y) = exp(y ln x) with ln from the atanh series and exp by reduction modulo
-// ln 2 and a Taylor series; x^5 by repeated double multiplication; rsqrt(x) =
-// 1/sqrt(x). The results are reproducible bit for bit on any IEEE machine.
+// Two arithmetic modes, chosen per translation unit by PT_CUDA_MATH:
+//   1  the product build (libgpt_b200.so). Compiled as the reference's kernels are (nvcc's
+//      default multiply-add contraction), and the transcendentals are CUDA's own, called where
+//      the reference calls them (MaterialEval.cu:224-228, 397, 442, 511, 589-591, 649;
+//      Intersect.cu:131; Image.cu:31; rsqrtf in helper_math's normalize). Its results are the
+//      reference build's on the same GPU.
+//   0  the deterministic build (libgpt_b200_det.so, and the scene-upload kernels of every build,
+//      which restate host code). Compiled with -fmad=false, so every float operator rounds once
+//      in source order, and the transcendentals are defined below from the mathematics,
+//      evaluated in IEEE double and rounded once to float: sin/cos by reduction modulo pi/2 and
+//      Taylor series to r^15/r^16; pow(x, y) = exp(y ln x) with ln from the atanh series and exp
+//      by reduction modulo ln 2 (the two-constant split of ln 2 published with fdlibm's e_exp.c,
+//      Sun Microsystems 1993, used here only as the reduction's constants) and a Taylor series;
+//      x^5 by repeated double multiplication; rsqrt(x) = 1/sqrt(x). These results are
+//      reproducible bit for bit on any IEEE machine, which is what the CPU oracle relies on.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <math.h>
 
 #define PT_HD __host__ __device__ __forceinline__
+
+#ifndef PT_CUDA_MATH
+#define PT_CUDA_MATH 0
+#endif
 
 namespace pt
 {
@@ -52,11 +61,6 @@ namespace pt
     }
     PT_HD float rsqrt_ieee(float x) { return 1.0f / sqrtf(x); }
     PT_HD float length(float3 v) { return sqrtf(dot(v, v)); }
-    PT_HD float3 normalize(float3 v)
-    {
-        float invLen = rsqrt_ieee(dot(v, v));
-        return v * invLen;
-    }
     PT_HD float3 reflect(float3 i, float3 n) { return i - 2.0f * n * dot(n, i); }
     PT_HD float clampf(float f, float a, float b) { return fmaxf(a, fminf(f, b)); }
     PT_HD float lerpf(float a, float b, float t) { return a + t * (b - a); }
@@ -241,5 +245,42 @@ namespace pt
         const double d2 = d * d;
         const double d4 = d2 * d2;
         return static_cast<float>(d4 * d);
+    }
+
+    // ---------------------------------------------------------------- the build's arithmetic
+    // The two modes live in differently named inline namespaces, so translation units of both
+    // modes link into one library without two definitions of one function.
+#if PT_CUDA_MATH
+    inline namespace cuda_math
+    {
+        // helper_math.h:78 and its device rsqrtf: CUDA's reciprocal square root on the GPU
+        PT_HD float rsqrt_f(float x)
+        {
+#ifdef __CUDA_ARCH__
+            return rsqrtf(x);
+#else
+            return 1.0f / sqrtf(x);
+#endif
+        }
+        PT_HD void sincos_f(float x, float* s, float* c)
+        {
+            *c = cosf(x);
+            *s = sinf(x);
+        }
+        PT_HD float pow_f(float x, float y) { return powf(x, y); }
+        PT_HD float pow5_f(float x) { return powf(x, 5.0f); }
+#else
+    inline namespace ieee_math
+    {
+        PT_HD float rsqrt_f(float x) { return rsqrt_ieee(x); }
+        PT_HD void sincos_f(float x, float* s, float* c) { sincos_det(x, s, c); }
+        PT_HD float pow_f(float x, float y) { return pow_det(x, y); }
+        PT_HD float pow5_f(float x) { return pow5_det(x); }
+#endif
+        PT_HD float3 normalize(float3 v)
+        {
+            float invLen = rsqrt_f(dot(v, v));
+            return v * invLen;
+        }
     }
 }

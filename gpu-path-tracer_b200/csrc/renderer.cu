@@ -234,17 +234,24 @@ namespace pt
         scene->lightCount = lightCount;
         if (lightCount > 0)
         {
-            DeviceBuffer weights, prefix, stackIndex, stackValue;
+            DeviceBuffer weights, powerWeights, powerScratch, prefix, stackIndex, stackValue;
             PT_TRY(scene->lights.allocate(static_cast<size_t>(lightCount) * 7 * sizeof(float4)));
             PT_TRY(scene->bins.allocate(static_cast<size_t>(lightCount) * sizeof(uint4)));
+            PT_TRY(scene->binsPower.allocate(static_cast<size_t>(lightCount) * sizeof(uint4)));
             PT_TRY(weights.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_TRY(powerWeights.allocate(static_cast<size_t>(lightCount) * 8));
+            PT_TRY(powerScratch.allocate(alias_power_scratch_bytes(lightCount)));
             PT_TRY(prefix.allocate(static_cast<size_t>(lightCount) * 8));
             PT_TRY(stackIndex.allocate(static_cast<size_t>(lightCount) * 8));
             PT_TRY(stackValue.allocate(static_cast<size_t>(lightCount) * 8));
-            PT_CUDA("light records", launch_light_records(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), n,
-                                                          flags.get<uint32_t>(), index.get<uint32_t>(), scene->lights.get<float4>(), weights.get<double>(), stream));
+            const MaterialTextures* tex = scene->textures.empty() ? nullptr : scene->materialTextures.get<MaterialTextures>();
+            PT_CUDA("light records", launch_light_records(pos.get<float>(), scene->shading.get<float4>(), scene->materials.get<MaterialDev>(), tex,
+                                                          n, flags.get<uint32_t>(), index.get<uint32_t>(), scene->lights.get<float4>(),
+                                                          weights.get<double>(), powerWeights.get<double>(), stream));
             PT_CUDA("alias table", launch_alias_build(weights.get<double>(), lightCount, prefix.get<double>(), scanScratch.get<double>(),
                                                       scene->bins.get<uint4>(), stackIndex.get<uint32_t>(), stackValue.get<float>(), stream));
+            PT_CUDA("power alias table", launch_alias_build_power(powerWeights.get<double>(), weights.get<double>(), lightCount,
+                                                                  powerScratch.get<void>(), scene->binsPower.get<uint4>(), stream));
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream));
         }
         const SceneEntry entry{0u, 0u, lightCount, 0u};
@@ -415,6 +422,10 @@ namespace pt
             if (s.max_samples && s.max_samples < c.totalSamples) c.totalSamples = s.max_samples;
             if (c.totalSamples >= 0xFFFFFFFFull)
                 return Status::Err(GPT_ERR_CAPACITY, "A frame is limited to 2^32-1 samples (per-sample radiance capture)");
+            if (s.rng_policy != GPT_RNG_PHILOX && s.rng_policy != GPT_RNG_PCG32)
+                return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown rng_policy");
+            if (s.light_sampling != GPT_LIGHTS_AREA && s.light_sampling != GPT_LIGHTS_POWER)
+                return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown light_sampling");
             c.traceThreads = s.trace_block ? static_cast<int>(s.trace_block) : 128;
             if (c.traceThreads != 64 && c.traceThreads != 128) c.traceThreads = 128;
             // bits 0-7: closest-hit traversal (0 = 16); bits 8-15: shadow rays (0 = half the closest-hit value)
@@ -604,6 +615,8 @@ namespace pt
             jv.totalSamples = c.totalSamples;
             jv.sampleRadiance = sampleRadiance_.get<float>();
             jv.rngOffset = s.rng_offset;
+            jv.rngPolicy = s.rng_policy;
+            jv.lightMode = s.light_sampling;
             const uint64_t rounds = (c.totalSamples + c.pool - 1) / c.pool;
             jv.maxIterations = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(c.depth) * (rounds + 2) + 64));
             hostJob_ = jv;
@@ -1215,6 +1228,16 @@ extern "C"
         if (count > r->impl->scene_->lightCount) return GPT_ERR_CAPACITY;
         cudaSetDevice(r->impl->device_);
         cudaError_t e = cudaMemcpy(bins, r->impl->scene_->bins.get<void>(), static_cast<size_t>(count) * 16, cudaMemcpyDeviceToHost);
+        return Report(r, pt::CudaStatus("cudaMemcpy", e));
+    }
+
+    int gpt_read_alias_table_power(gpt_renderer* r, uint32_t* bins, uint32_t count)
+    {
+        if (!r || !bins) return GPT_ERR_INVALID_ARGUMENT;
+        if (!r->impl->scene_) return GPT_ERR_NO_SCENE;
+        if (count > r->impl->scene_->lightCount) return GPT_ERR_CAPACITY;
+        cudaSetDevice(r->impl->device_);
+        cudaError_t e = cudaMemcpy(bins, r->impl->scene_->binsPower.get<void>(), static_cast<size_t>(count) * 16, cudaMemcpyDeviceToHost);
         return Report(r, pt::CudaStatus("cudaMemcpy", e));
     }
 

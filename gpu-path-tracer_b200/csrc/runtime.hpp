@@ -93,7 +93,7 @@ namespace pt
 
     struct SceneGpu
     {
-        DeviceBuffer nodes, tris, shading, materials, lights, bins, materialTextures, entry, nodes2;
+        DeviceBuffer nodes, tris, shading, materials, lights, bins, binsPower, materialTextures, entry, nodes2;
         std::vector<std::unique_ptr<TextureObject>> textures;
         uint32_t nodeCount = 0, triangleCount = 0, depth = 0, lightCount = 0, materialCount = 0;
         uint32_t nodeCount2 = 0, depth2 = 0;  // binary FP32 BVH, built when the scene is uploaded with it
@@ -109,6 +109,7 @@ namespace pt
             v.textures = textures.empty() ? nullptr : materialTextures.get<MaterialTextures>();
             v.lights = lights.get<float4>();
             v.bins = bins.get<uint4>();
+            v.binsPower = binsPower.get<uint4>();
             v.lightCount = lightCount;
             v.nodeCount = nodeCount;
             v.triangleCount = triangleCount;

@@ -3,6 +3,12 @@
 The product is the C ABI; this module only marshals numpy arrays and torch
 device tensors into it. There is no fallback: if the shared library is missing
 or no CUDA device is present, the calls raise.
+
+Two builds export the same ABI (gpu-path-tracer_b200/Makefile):
+  "product"  libgpt_b200.so: the reference build's arithmetic (multiply-add contraction, CUDA's
+             sinf/cosf/powf/rsqrtf); what bench.py measures.
+  "det"      libgpt_b200_det.so: no contraction and IEEE definitions of the transcendentals, so
+             results are reproducible bit for bit by the CPU oracle.
 """
 from __future__ import annotations
 
@@ -14,10 +20,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgpt_b200.so")
+LIB_PATHS = {"product": LIB_PATH, "det": os.path.join(HERE, "libgpt_b200_det.so")}
 QUEUE_LOG_COLUMNS = 9
 INVALID = 0xFFFFFFFF
 
-_lib = None
+_libs = {}
 
 
 class GptError(RuntimeError):
@@ -62,9 +69,12 @@ class gpt_render_settings(ctypes.Structure):
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
                 ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
-                ("bvh_format", ctypes.c_uint32), ("wavefront_layout", ctypes.c_uint32)]
+                ("bvh_format", ctypes.c_uint32), ("wavefront_layout", ctypes.c_uint32), ("rng_policy", ctypes.c_uint32),
+                ("light_sampling", ctypes.c_uint32)]
 
 LOOP_GRAPH, LOOP_HOST = 0, 1
+RNG_PHILOX, RNG_PCG32 = 0, 1
+LIGHTS_AREA, LIGHTS_POWER = 0, 1
 BVH8_Q8, BVH2_FP32 = 0, 1
 WAVEFRONT_B200, WAVEFRONT_QUEUES = 0, 1
 SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST = 1, 2
@@ -91,7 +101,7 @@ class gpt_job_desc(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_uint32), ("width", ctypes.c_uint32), ("height", ctypes.c_uint32),
                 ("samples_per_pixel", ctypes.c_uint32), ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32),
                 ("rng_offset", ctypes.c_uint64), ("camera", gpt_device_camera), ("keep_accumulation", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("rng_policy", ctypes.c_uint32), ("light_sampling", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 
 class gpt_job_status(ctypes.Structure):
@@ -162,6 +172,7 @@ _SIGNATURES = [
     ("gpt_scene_info_binary", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                              ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
+    ("gpt_read_alias_table_power", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_bvh8_check", ctypes.c_int, [ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(ctypes.c_uint64)]),
@@ -188,23 +199,26 @@ _SIGNATURES = [
 
 
 def build(verbose: bool = False) -> str:
-    """Compile libgpt_b200.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    """Compile both library builds for sm_100a (nvcc cross-compiles without a GPU)."""
     subprocess.run(["make", "-C", HERE] + ([] if verbose else ["-s"]), check=True)
     return LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise GptError(-1, f"{LIB_PATH} is missing: run `make -C {HERE}` (or __graft_entry__.build())")
-        L = ctypes.CDLL(LIB_PATH)
+def lib(variant: str = "product"):
+    """The loaded library of one build: "product" (libgpt_b200.so) or "det" (libgpt_b200_det.so)."""
+    if variant not in LIB_PATHS:
+        raise ValueError(f"unknown library build {variant!r}; expected one of {sorted(LIB_PATHS)}")
+    if variant not in _libs:
+        path = LIB_PATHS[variant]
+        if not os.path.exists(path):
+            raise GptError(-1, f"{path} is missing: run `make -C {HERE}` (or __graft_entry__.build())")
+        L = ctypes.CDLL(path)
         for name, res, args in _SIGNATURES:
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def declared_symbols() -> list[str]:
@@ -229,8 +243,9 @@ def camera_struct(camera12) -> gpt_device_camera:
 class Renderer:
     """Handle on one gpt_renderer (one device, one render stream)."""
 
-    def __init__(self, device: int = 0):
-        self.L = lib()
+    def __init__(self, device: int = 0, variant: str = "product"):
+        self.L = lib(variant)
+        self.variant = variant
         h = ctypes.c_void_p()
         rc = self.L.gpt_create(ctypes.byref(h), device)
         if rc != 0:
@@ -277,20 +292,25 @@ class Renderer:
         return dict(nodes=n.value, depth=d.value, lights=l.value, triangles=t.value, binary_nodes=n2.value,
                     binary_depth=d2.value)
 
-    def alias_table(self) -> np.ndarray:
+    def alias_table(self, power: bool = False) -> np.ndarray:
+        """[lights, 4] words (q, p, alias, value): the area-weighted table, or with power=True the
+        power-weighted one."""
         lights = self.scene_info()["lights"]
         out = np.zeros((lights, 4), dtype=np.uint32)
         if lights:
-            self._check(self.L.gpt_read_alias_table(self.h, _ptr(out), lights), "gpt_read_alias_table")
+            fn = self.L.gpt_read_alias_table_power if power else self.L.gpt_read_alias_table
+            self._check(fn(self.h, _ptr(out), lights), "gpt_read_alias_table")
         return out
 
     def render_frame(self, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
                      rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0,
-                     bvh_format: int = BVH8_Q8, wavefront_layout: int = WAVEFRONT_B200) -> dict:
+                     bvh_format: int = BVH8_Q8, wavefront_layout: int = WAVEFRONT_B200, rng_policy: int = RNG_PHILOX,
+                     light_sampling: int = LIGHTS_AREA) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
-                                 trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, wavefront_layout)
+                                 trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, wavefront_layout,
+                                 rng_policy, light_sampling)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")
@@ -471,10 +491,30 @@ def bvh8_check(scene) -> dict:
     return dict(nodes=n.value, depth=d.value, violations=v.value, misplaced=m.value)
 
 
-def build_alias_table_noalloc(weights_dev, bins_dev, stream=None) -> int:
-    """Allocation-free alias-table build on device tensors (float32 weights [n], int32 bins [n, 4])."""
-    return lib().gpt_build_alias_table_noalloc(ctypes.c_void_p(weights_dev.data_ptr()), weights_dev.shape[0],
-                                                ctypes.c_void_p(bins_dev.data_ptr()), ctypes.c_void_p(stream))
+def build_alias_table_noalloc(weights_dev, bins_dev, stream=None, variant: str = "product") -> int:
+    """Allocation-free alias-table build on device tensors: float32 weights [n] in, 4-byte bins [n, 4] out.
+
+    Both tensors must be contiguous CUDA tensors on the same device, with bins 16-byte aligned (the
+    kernel stores whole 16-byte bins). The build is ordered on `stream` (a cudaStream_t handle as an
+    int), by default torch's current stream on the tensors' device. Returns the C status code.
+    """
+    import torch
+    if weights_dev.dtype != torch.float32 or weights_dev.dim() != 1:
+        raise ValueError("weights must be a 1-D float32 tensor")
+    n = int(weights_dev.shape[0])
+    if bins_dev.dtype not in (torch.int32, torch.uint32) or tuple(bins_dev.shape) != (n, 4):
+        raise ValueError(f"bins must be an int32/uint32 tensor of shape ({n}, 4)")
+    if not (weights_dev.is_cuda and bins_dev.is_cuda) or weights_dev.device != bins_dev.device:
+        raise ValueError("weights and bins must be CUDA tensors on the same device")
+    if not (weights_dev.is_contiguous() and bins_dev.is_contiguous()):
+        raise ValueError("weights and bins must be contiguous")
+    if bins_dev.data_ptr() % 16 != 0:
+        raise ValueError("bins must be 16-byte aligned")
+    if stream is None:
+        stream = torch.cuda.current_stream(weights_dev.device).cuda_stream
+    with torch.cuda.device(weights_dev.device):
+        return lib(variant).gpt_build_alias_table_noalloc(ctypes.c_void_p(weights_dev.data_ptr()), n,
+                                                          ctypes.c_void_p(bins_dev.data_ptr()), ctypes.c_void_p(stream))
 
 
 def load_obj(path: str, transform=None):
@@ -532,8 +572,8 @@ class Server:
 
     def __init__(self, device: int = 0, pool_size: int = 0, max_jobs: int = 0, max_active_jobs: int = 0,
                  ring_passes: int = 0, hbm_budget_bytes: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                 trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0):
-        self.L = lib()
+                 trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0, variant: str = "product"):
+        self.L = lib(variant)
         cfg = gpt_server_config(pool_size, max_jobs, max_active_jobs, ring_passes, hbm_budget_bytes, trace_block,
                                 trace_refill, trace_occupancy, max_slice_iterations, schedule, 0)
         h = ctypes.c_void_p()
@@ -568,9 +608,10 @@ class Server:
         return sid.value
 
     def submit(self, scene_id: int, camera12, width: int, height: int, spp: int, depth: int, nee: bool = True,
-               rng_offset: int = 0, keep_accumulation: bool = False) -> int:
+               rng_offset: int = 0, keep_accumulation: bool = False, rng_policy: int = RNG_PHILOX,
+               light_sampling: int = LIGHTS_AREA) -> int:
         d = gpt_job_desc(scene_id, width, height, spp, depth, 1 if nee else 0, rng_offset, camera_struct(camera12),
-                         1 if keep_accumulation else 0, 0)
+                         1 if keep_accumulation else 0, rng_policy, light_sampling, 0)
         jid = ctypes.c_uint64()
         self._check(self.L.gpt_server_submit(self.h, ctypes.byref(d), ctypes.byref(jid)), "gpt_server_submit")
         self._jobs[jid.value] = (width, height)

@@ -140,6 +140,13 @@ typedef struct gpt_render_settings {
                                      GPT_WAVEFRONT_QUEUES: the reference's structure, a queue of finished slots in the
                                      order paths ended (RegenQueue, PathGeneration.cu:74-102) and the shading kernels
                                      one after another (Renderer.cpp:540-566). Same results, bit for bit. */
+    uint32_t rng_policy;          /* GPT_RNG_PHILOX (default): the reference's streams, cuRAND Philox4_32_10 with seed
+                                     1234 and subsequence = sample index (PathData.hpp:37-73); GPT_RNG_PCG32: one PCG32
+                                     stream per sample, seeded by a hash of (seed, pixel, sample) */
+    uint32_t light_sampling;      /* GPT_LIGHTS_AREA (default): NEE picks an emitter with probability proportional to
+                                     its area, the reference's light sampler (LightSampler.cpp:16-19); GPT_LIGHTS_POWER:
+                                     proportional to area x luminance of its emission (the production mode; the alias
+                                     table is built from an FP64 prefix sum by a parallel split on the device) */
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
@@ -148,6 +155,10 @@ typedef struct gpt_render_settings {
 #define GPT_BVH2_FP32 1u
 #define GPT_WAVEFRONT_B200 0u
 #define GPT_WAVEFRONT_QUEUES 1u
+#define GPT_RNG_PHILOX 0u
+#define GPT_RNG_PCG32 1u
+#define GPT_LIGHTS_AREA 0u
+#define GPT_LIGHTS_POWER 1u
 
 typedef struct gpt_frame_stats {
     uint32_t iterations;          /* wavefront iterations (Renderer.cpp:517-623) */
@@ -276,6 +287,10 @@ int gpt_scene_info_binary(const gpt_renderer* renderer, uint32_t* node_count, ui
 /* The light alias table built on the device, [lights][4] words (q, p, alias, value)
  * (AliasTableView.hpp:8-14). */
 int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
+/* The power-weighted alias table of GPT_LIGHTS_POWER (area x emission luminance, FP64 prefix sums,
+ * parallel split on the device), same layout. No counterpart in the reference, whose light sampler
+ * weights by area only (LightSampler.cpp:16-19). */
+int gpt_read_alias_table_power(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
 
 /*
  * Host-side validation of the BVH builder (no device work): builds the wide BVH and the binary FP32
@@ -294,13 +309,17 @@ int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* 
  * or code that cannot afford cudaMalloc/cudaFree stalls, since cudaFree synchronises the device).
  * It builds the same table as the scene upload (AliasTable.hpp:22-84 semantics: FP64 sum of the
  * weights, p = w / sum, the reference's sequential pairing) from light_count float weights into
- * bins ([light_count][4] uint32 = q, p, alias, value; 16-byte aligned). Both pointers are device
- * memory; stream may be NULL (the legacy default stream); the call is asynchronous on it.
+ * bins ([light_count][4] uint32 = q, p, alias, value). Both pointers are device memory; bins must be
+ * 16-byte aligned and weights 4-byte aligned (GPT_ERR_INVALID_ARGUMENT otherwise). The weights must
+ * be finite and non-negative with a positive sum; other weights give NaN or infinite entries.
+ * light_count 0 returns GPT_OK and touches nothing. stream may be NULL (the legacy default
+ * stream); the call is asynchronous on it.
  * Working memory is a fixed array of about 2 MiB compiled into the library, held by every GPU that
  * loads it until the process exits; light_count above GPT_NOALLOC_MAX_LIGHTS returns
  * GPT_ERR_CAPACITY. The first call on a device looks up that array's device address (set-up),
- * so make the first call before any stream capture. All calls share the array: calls that can
- * overlap on the GPU race and must be ordered by the caller.
+ * so make the first call before any stream capture; that address is kept for the process, so a
+ * device reset (cudaDeviceReset) after the first call is not supported. All calls share the
+ * array: calls that can overlap on the GPU race and must be ordered by the caller.
  */
 #define GPT_NOALLOC_MAX_LIGHTS 65536u
 int gpt_build_alias_table_noalloc(const float* weights, uint32_t light_count, uint32_t* bins, void* stream);
@@ -364,6 +383,8 @@ typedef struct gpt_job_desc {
     uint64_t rng_offset;           /* added to the sample index to form the Philox subsequence */
     gpt_device_camera camera;
     uint32_t keep_accumulation;    /* nonzero: keep the float4 accumulation for gpt_server_read */
+    uint32_t rng_policy;           /* GPT_RNG_PHILOX (default) or GPT_RNG_PCG32, as in gpt_render_settings */
+    uint32_t light_sampling;       /* GPT_LIGHTS_AREA (default) or GPT_LIGHTS_POWER, as in gpt_render_settings */
     uint32_t reserved;
 } gpt_job_desc;
 

@@ -21,6 +21,14 @@
 //    sample order after the frame, instead of float atomics per contribution
 //    (Kernels/Common.hpp:8-16). At spp = 1 the two are identical.
 //
+// Production modes of the product that the reference does not have (restated here
+// from the product's definition, so the checker covers them too):
+//  * RNG policy PCG32: PCG-XSH-RR 64/32 (O'Neill 2014) per sample, seeded by a
+//    splitmix64 hash of (seed, sample key) and positioned by LCG jump-ahead.
+//  * Power-weighted light selection: weights area x luminance(emission) in FP64, the
+//    alias table built by the parallel sweep; the prefix sums are taken in the
+//    product's device order (its block scan), so the table is bit-for-bit the same.
+//
 // Compile with -ffp-contract=off (see oracle/Makefile): no FMA contraction.
 #include "oracle_detmath.h"
 
@@ -196,13 +204,80 @@ namespace oracle
         return PhiloxBlock{{c0, c1, c2, c3}};
     }
 
+    // ------------------------------------------------------------------
+    // PCG32 (PCG-XSH-RR, 64-bit state; O'Neill, "PCG: A Family of Simple Fast
+    // Space-Efficient Statistically Good Algorithms for Random Number Generation",
+    // 2014): the product's second RNG policy. One stream per sample: seeded by a
+    // splitmix64 hash (Steele, Lea, Flood, OOPSLA 2014) of (seed, key), key = the
+    // sample index plus the shard offset, positioned by LCG jump-ahead (Brown 1994).
+    // ------------------------------------------------------------------
+    enum RngPolicy : uint32_t { RngPhilox = 0, RngPcg32 = 1 };
+
+    inline uint64_t Mix64(uint64_t z)
+    {
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    }
+
+    struct Pcg32
+    {
+        static constexpr uint64_t Multiplier = 6364136223846793005ull;
+        uint64_t state = 0, inc = 1;
+        uint32_t Next()
+        {
+            const uint64_t old = state;
+            state = old * Multiplier + inc;
+            const uint32_t xorshifted = static_cast<uint32_t>(((old >> 18u) ^ old) >> 27u);
+            const uint32_t rot = static_cast<uint32_t>(old >> 59u);
+            return (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+        }
+        void Seed(uint64_t initstate, uint64_t initseq)
+        {
+            state = 0;
+            inc = (initseq << 1u) | 1u;
+            Next();
+            state += initstate;
+            Next();
+        }
+        void Advance(uint64_t delta)
+        {
+            uint64_t accMult = 1, accPlus = 0, curMult = Multiplier, curPlus = inc;
+            while (delta > 0)
+            {
+                if (delta & 1u)
+                {
+                    accMult *= curMult;
+                    accPlus = accPlus * curMult + curPlus;
+                }
+                curPlus = (curMult + 1) * curPlus;
+                curMult *= curMult;
+                delta >>= 1;
+            }
+            state = accMult * state + accPlus;
+        }
+        static Pcg32 ForKey(uint64_t key)
+        {
+            Pcg32 g;
+            g.Seed(Mix64(RandomSeed ^ Mix64(key)), Mix64(key ^ 0x9E3779B97F4A7C15ull));
+            return g;
+        }
+    };
+
     struct Random
     {
         uint64_t subsequence;
         uint64_t position;
+        uint32_t policy = RngPhilox;
 
         uint32_t Word(uint64_t pos) const
         {
+            if (policy == RngPcg32)
+            {
+                Pcg32 g = Pcg32::ForKey(subsequence);
+                g.Advance(pos);
+                return g.Next();
+            }
             uint64_t block = pos >> 2;
             PhiloxBlock b = Philox4x32_10(
                 static_cast<uint32_t>(block), static_cast<uint32_t>(block >> 32),
@@ -215,10 +290,13 @@ namespace oracle
             const float inv2pow32 = 2.3283064e-10f;
             return static_cast<float>(u) * inv2pow32 + (inv2pow32 / 2.0f);
         }
-        float NextFloat() { return ToUniform(Word(position++)); }
+        // PCG32 uniforms: the top 24 bits, centred: (w >> 8) 2^-24 + 2^-25, in (0, 1]
+        static float ToUniformPcg(uint32_t u) { return static_cast<float>(u >> 8) * 0x1p-24f + 0x1p-25f; }
+        float Uniform(uint64_t pos) const { return policy == RngPcg32 ? ToUniformPcg(Word(pos)) : ToUniform(Word(pos)); }
+        float NextFloat() { return Uniform(position++); }
         float4 NextFloat4()
         {
-            float4 r{ToUniform(Word(position)), ToUniform(Word(position + 1)), ToUniform(Word(position + 2)), ToUniform(Word(position + 3))};
+            float4 r{Uniform(position), Uniform(position + 1), Uniform(position + 2), Uniform(position + 3)};
             position += 4;
             return r;
         }
@@ -282,6 +360,7 @@ namespace oracle
         // lights (LightSampler.cpp:5-40) and alias table (AliasTable.hpp:22-84)
         std::vector<LightTriangle> lights;
         std::vector<Bin> bins;
+        std::vector<Bin> binsPower;  // the product's power-weighted table
     };
 
     // ------------------------------------------------------------------
@@ -349,6 +428,132 @@ namespace oracle
         }
         *outIndex = bin.alias;
         *outPmf = bins[bin.alias].p;
+    }
+
+    // ------------------------------------------------------------------
+    // Power-weighted alias table of the product (no counterpart in the reference).
+    // ------------------------------------------------------------------
+    // Exclusive prefix sum in the product's device order (its block scan over 1024-element
+    // blocks): Hillis-Steele inclusive scan within each 32-lane warp (a lane adds the value
+    // of the lane o below it, o = 1, 2, 4, 8, 16), the same over the 32 warp totals, then
+    // exclusive = (lane value + warp offset) - x; block totals scanned recursively the same
+    // way and added to every later block.
+    template <typename T>
+    inline void DeviceOrderExclusiveScan(const T* in, T* out, size_t n)
+    {
+        if (n == 0) return;
+        const size_t blocks = (n + 1023) / 1024;
+        std::vector<T> sums(blocks);
+        std::vector<T> x(1024), v(1024), prev(1024);
+        for (size_t blk = 0; blk < blocks; blk++)
+        {
+            for (size_t t = 0; t < 1024; t++)
+            {
+                const size_t i = blk * 1024 + t;
+                x[t] = i < n ? in[i] : T(0);
+                v[t] = x[t];
+            }
+            for (size_t o = 1; o < 32; o <<= 1)
+            {
+                prev = v;
+                for (size_t t = 0; t < 1024; t++)
+                    if ((t & 31) >= o) v[t] = prev[t] + prev[t - o];
+            }
+            T ws[32], wprev[32];
+            for (size_t w = 0; w < 32; w++) ws[w] = v[w * 32 + 31];
+            for (size_t o = 1; o < 32; o <<= 1)
+            {
+                std::copy(ws, ws + 32, wprev);
+                for (size_t l = o; l < 32; l++) ws[l] = wprev[l] + wprev[l - o];
+            }
+            T last = T(0);
+            for (size_t t = 0; t < 1024; t++)
+            {
+                const size_t w = t >> 5;
+                const T warpOffset = w > 0 ? ws[w - 1] : T(0);
+                const T inclusive = v[t] + warpOffset;
+                const size_t i = blk * 1024 + t;
+                if (i < n) out[i] = inclusive - x[t];
+                last = inclusive;
+            }
+            sums[blk] = last;
+        }
+        if (blocks == 1) return;
+        DeviceOrderExclusiveScan(sums.data(), sums.data(), blocks);
+        for (size_t blk = 1; blk < blocks; blk++)
+            for (size_t t = 0; t < 1024; t++)
+            {
+                const size_t i = blk * 1024 + t;
+                if (i < n) out[i] = out[i] + sums[blk];
+            }
+    }
+
+    // The product's parallel sweep (scene-upload alias_*_kernel): classify by pHat = w n / W,
+    // prefix sums of deficits (lights) and excesses (heavies) in input order with zeros for the other
+    // class, running maxima over both, then the merge of the keys D_i (lights) and E_(j+1) (heavies,
+    // first on ties), here run sequentially. Area weights replace power weights whose sum is not positive.
+    inline std::vector<Bin> BuildPowerAliasTable(const std::vector<double>& power, const std::vector<double>& area)
+    {
+        const size_t n = power.size();
+        std::vector<Bin> bins(n);
+        if (n == 0) return bins;
+        std::vector<double> prefix(n), areaPrefix(n);
+        DeviceOrderExclusiveScan(power.data(), prefix.data(), n);
+        DeviceOrderExclusiveScan(area.data(), areaPrefix.data(), n);
+        const double totalPower = prefix[n - 1] + power[n - 1];
+        const bool usePower = totalPower > 0.0 && totalPower < 1e300;
+        const std::vector<double>& w = usePower ? power : area;
+        const double total = usePower ? totalPower : areaPrefix[n - 1] + area[n - 1];
+        std::vector<double> pHat(n), deficit(n), excess(n), dp(n), ep(n);
+        std::vector<uint32_t> lightIdx, heavyIdx;
+        for (size_t k = 0; k < n; k++)
+        {
+            const double ph = w[k] * static_cast<double>(n) / total;
+            const bool light = ph < 1.0;
+            pHat[k] = ph;
+            deficit[k] = light ? 1.0 - ph : 0.0;
+            excess[k] = light ? 0.0 : ph - 1.0;
+            (light ? lightIdx : heavyIdx).push_back(static_cast<uint32_t>(k));
+            bins[k] = Bin{1.0f, static_cast<float>(w[k] / total), InvalidIndex, static_cast<uint32_t>(k)};
+        }
+        DeviceOrderExclusiveScan(deficit.data(), dp.data(), n);
+        DeviceOrderExclusiveScan(excess.data(), ep.data(), n);
+        for (size_t k = 1; k < n; k++)
+        {
+            dp[k] = std::fmax(dp[k], dp[k - 1]);
+            ep[k] = std::fmax(ep[k], ep[k - 1]);
+        }
+        const size_t a = lightIdx.size(), b = heavyIdx.size();
+        const double deficitTotal = dp[n - 1] + deficit[n - 1];
+        const double excessTotal = ep[n - 1] + excess[n - 1];
+        auto D = [&](size_t i) { return i < a ? dp[lightIdx[i]] : deficitTotal; };
+        auto E = [&](size_t j) { return j < b ? ep[heavyIdx[j]] : excessTotal; };
+        size_t i = 0, j = 0;
+        for (size_t k = 0; k < n; k++)
+        {
+            if (i < a && (j >= b || D(i) < E(j + 1)))
+            {
+                const uint32_t item = lightIdx[i];
+                if (j < b)
+                {
+                    bins[item].q = static_cast<float>(pHat[item]);
+                    bins[item].alias = heavyIdx[j];
+                }
+                i++;
+            }
+            else
+            {
+                const uint32_t item = heavyIdx[j];
+                if (j + 1 < b)
+                {
+                    const double residual = E(j + 1) - D(i) + 1.0;
+                    bins[item].q = static_cast<float>(residual < 0.0 ? 0.0 : (residual > 1.0 ? 1.0 : residual));
+                    bins[item].alias = heavyIdx[j + 1];
+                }
+                j++;
+            }
+        }
+        return bins;
     }
 
     // ------------------------------------------------------------------
@@ -569,6 +774,7 @@ namespace oracle
         Random random;
         float3 radiance;  // accumulated contributions of this path, in arrival order
         Ray ray;
+        const std::vector<Bin>* bins;  // the light-selection table of the render (area or power weights)
     };
 
     inline void ComputePathSample(const PixelGrid& grid, uint64_t sampleIndex, float2 jitter, uint32_t* pixel, float2* uv)
@@ -597,10 +803,12 @@ namespace oracle
     }
 
     // PathGeneration.cu:56-102 for one sample: Philox stream, jitter, camera ray
-    inline void GeneratePath(const Camera& camera, const PixelGrid& grid, uint64_t sampleIndex, PathState& ps, uint64_t rngOffset = 0)
+    inline void GeneratePath(const Camera& camera, const PixelGrid& grid, uint64_t sampleIndex, PathState& ps, uint64_t rngOffset,
+                             uint32_t rngPolicy, const std::vector<Bin>* bins)
     {
         ps.sample = sampleIndex;
-        ps.random = Random{sampleIndex + rngOffset, 0};
+        ps.random = Random{sampleIndex + rngOffset, 0, rngPolicy};
+        ps.bins = bins;
         const float2 jitter = ps.random.NextFloat2();
         uint32_t pixel;
         float2 uv;
@@ -699,11 +907,12 @@ namespace oracle
         float pdf;
     };
 
-    inline ResolvedLightHit SampleLightTriangle(const Scene& scene, float lightSelectionSample, float2 xi, float3 hitPoint) // :171-192
+    inline ResolvedLightHit SampleLightTriangle(const Scene& scene, const std::vector<Bin>& bins, float lightSelectionSample, float2 xi,
+                                                float3 hitPoint) // :171-192
     {
         uint32_t lightIndex;
         float pmf;
-        SampleAlias(scene.bins, lightSelectionSample, &lightIndex, &pmf);
+        SampleAlias(bins, lightSelectionSample, &lightIndex, &pmf);
         const LightTriangle& light = scene.lights[lightIndex];
         float sqrtXi0 = std::sqrt(xi.x);
         const float b1 = sqrtXi0 * (1.0f - xi.y);
@@ -740,7 +949,7 @@ namespace oracle
 
     inline ShadowRay EvaluateDiffuseDirect(const PathState& path, float3 hitPosition, float3 gn, const Frame& frame, float3 rs, float3 albedo, const Scene& scene) // :231-268
     {
-        const ResolvedLightHit lightHit = SampleLightTriangle(scene, rs.x, make_float2(rs.y, rs.z), hitPosition);
+        const ResolvedLightHit lightHit = SampleLightTriangle(scene, *path.bins, rs.x, make_float2(rs.y, rs.z), hitPosition);
         if (lightHit.distanceSquared < 1e-6f) return ShadowRay{false, {}, {}};
         float cosThetaI = std::fmax(dot(frame.normal, lightHit.wi), 0.0f);
         float geometricCosThetaI = std::fmax(dot(gn, lightHit.wi), 0.0f);
@@ -795,7 +1004,7 @@ namespace oracle
     inline ShadowRay EvaluatePhongDirect(const PathState& path, const Ray& ray, float3 hitPosition, float3 gn, const Frame& frame, float3 rs,
                                          float3 albedo, float3 specular, float shininess, const Scene& scene) // :410-455
     {
-        const ResolvedLightHit lightHit = SampleLightTriangle(scene, rs.x, make_float2(rs.y, rs.z), hitPosition);
+        const ResolvedLightHit lightHit = SampleLightTriangle(scene, *path.bins, rs.x, make_float2(rs.y, rs.z), hitPosition);
         if (lightHit.distanceSquared < 1e-6f) return ShadowRay{false, {}, {}};
         float cosThetaI = std::fmax(dot(frame.normal, lightHit.wi), 0.0f);
         float geometricCosThetaI = std::fmax(dot(gn, lightHit.wi), 0.0f);
@@ -907,7 +1116,7 @@ namespace oracle
     inline ShadowRay EvaluateGgxDirect(const PathState& path, const Ray& ray, float3 hitPosition, float3 gn, const Frame& frame, float3 rs,
                                        float3 baseColor, float alpha, float metallic, float ior, const Scene& scene) // :652-718
     {
-        const ResolvedLightHit lightHit = SampleLightTriangle(scene, rs.x, make_float2(rs.y, rs.z), hitPosition);
+        const ResolvedLightHit lightHit = SampleLightTriangle(scene, *path.bins, rs.x, make_float2(rs.y, rs.z), hitPosition);
         if (lightHit.distanceSquared < 1e-6f || lightHit.pdf <= 0.0f) return ShadowRay{false, {}, {}};
         float geometricCosThetaI = dot(gn, lightHit.wi);
         if (geometricCosThetaI <= 0.0f) return ShadowRay{false, {}, {}};
@@ -1168,7 +1377,20 @@ namespace oracle
             scene->lights.push_back(lt);
         }
         if (!weights.empty())
+        {
             scene->bins = BuildAliasTable(weights, values);
+            // power weights: area x luminance of the emission constant (Rec. 709, as MaterialEval.cu's
+            // Luminance), in FP64
+            std::vector<double> power(weights.size()), area(weights.size());
+            for (size_t k = 0; k < weights.size(); k++)
+            {
+                const float* e = scene->materials[scene->shading[scene->lights[k].index].material].emission;
+                const double lum = 0.2126 * static_cast<double>(e[0]) + 0.7152 * static_cast<double>(e[1]) + 0.0722 * static_cast<double>(e[2]);
+                area[k] = static_cast<double>(weights[k]);
+                power[k] = lum * area[k];
+            }
+            scene->binsPower = BuildPowerAliasTable(power, area);
+        }
         // reference BVH
         scene->order.resize(triangleCount);
         std::iota(scene->order.begin(), scene->order.end(), 0u);
@@ -1191,6 +1413,8 @@ namespace oracle
         int threads;
         int accumulation;      // 0 = FP32 sequential, 1 = FP32 Kahan (sample order), 2 = FP64
         uint64_t rngOffset;    // added to the sample index to form the Philox subsequence
+        uint32_t rngPolicy;    // RngPhilox (the reference's) or RngPcg32
+        uint32_t lightMode;    // 0 = area weights (the reference's), 1 = power weights
     };
 
     // Renderer.cpp:468-647 replayed on the CPU, iteration by iteration, with the
@@ -1212,11 +1436,12 @@ namespace oracle
         // The reference's light sampler reads bin 0 of an empty table when NEE meets a scene without
         // emitters (AliasTableView.hpp:32-60); here NEE is off for such scenes (nothing to connect to).
         const bool nee = s.nee != 0 && !scene.lights.empty();
+        const std::vector<Bin>* bins = s.lightMode == 1 ? &scene.binsPower : &scene.bins;
 
         std::vector<PathState> active(generateCount);
         ParallelFor(generateCount, s.threads, [&](size_t b, size_t e)
         {
-            for (size_t i = b; i < e; i++) GeneratePath(camera, grid, i, active[i], s.rngOffset);
+            for (size_t i = b; i < e; i++) GeneratePath(camera, grid, i, active[i], s.rngOffset, s.rngPolicy, bins);
         });
         uint64_t launched = generateCount;
         uint32_t iter = 0;
@@ -1291,7 +1516,7 @@ namespace oracle
             next.resize(base + regenerate);
             ParallelFor(regenerate, s.threads, [&](size_t b, size_t e)
             {
-                for (size_t i = b; i < e; i++) GeneratePath(camera, grid, launched + i, next[base + i], s.rngOffset);
+                for (size_t i = b; i < e; i++) GeneratePath(camera, grid, launched + i, next[base + i], s.rngOffset, s.rngPolicy, bins);
             });
             launched += regenerate;
             active.swap(next);
@@ -1401,6 +1626,42 @@ extern "C"
         auto* s = static_cast<oracle::Scene*>(scene);
         std::memcpy(binsOut, s->bins.data(), s->bins.size() * sizeof(oracle::Bin));
     }
+    void oracle_scene_alias_power_export(void* scene, void* binsOut)
+    {
+        auto* s = static_cast<oracle::Scene*>(scene);
+        std::memcpy(binsOut, s->binsPower.data(), s->binsPower.size() * sizeof(oracle::Bin));
+    }
+
+    // The product's power-weighted alias table from FP64 power and area weights. bins [n][4] words.
+    void oracle_power_alias_build(const double* power, const double* area, uint32_t n, void* binsOut)
+    {
+        std::vector<double> p(power, power + n), a(area, area + n);
+        auto bins = oracle::BuildPowerAliasTable(p, a);
+        std::memcpy(binsOut, bins.data(), bins.size() * sizeof(oracle::Bin));
+    }
+
+    // Exclusive FP64 prefix sum in the product's device order.
+    void oracle_device_order_scan(const double* in, uint32_t n, double* out) { oracle::DeviceOrderExclusiveScan(in, out, n); }
+
+    // Raw PCG32 stream of a sample key: count words from position, and their uniforms.
+    void oracle_pcg_words(uint64_t key, uint64_t position, uint32_t count, uint32_t* wordsOut, float* uniformsOut)
+    {
+        oracle::Random r{key, position, oracle::RngPcg32};
+        for (uint32_t i = 0; i < count; i++)
+        {
+            uint32_t w = r.Word(position + i);
+            if (wordsOut) wordsOut[i] = w;
+            if (uniformsOut) uniformsOut[i] = oracle::Random::ToUniformPcg(w);
+        }
+    }
+
+    // PCG32 with an explicit (initstate, initseq) seeding, for the generator's published sequence.
+    void oracle_pcg_seeded_words(uint64_t initstate, uint64_t initseq, uint32_t count, uint32_t* wordsOut)
+    {
+        oracle::Pcg32 g;
+        g.Seed(initstate, initseq);
+        for (uint32_t i = 0; i < count; i++) wordsOut[i] = g.Next();
+    }
 
     // Closest hit for a ray batch: rays [n][8] = origin3, dir3, tMin, tMax.
     // Output: triangle (original index or 0xFFFFFFFF), u, v, t.
@@ -1481,12 +1742,13 @@ extern "C"
     int oracle_render(void* scene, const float* camera, uint32_t width, uint32_t height, uint32_t spp, uint32_t depth, uint32_t nee,
                       uint32_t poolSize, uint64_t maxSamples, int threads, int accumulationMode, float* sampleRadiance,
                       float* accumulation, uint32_t* framebuffer, uint32_t* queueLog, uint32_t queueLogCapacity, uint32_t* iterations,
-                      uint64_t rngOffset)
+                      uint64_t rngOffset, uint32_t rngPolicy, uint32_t lightMode)
     {
         auto* s = static_cast<oracle::Scene*>(scene);
         oracle::Camera cam{{camera[0], camera[1], camera[2]}, {camera[3], camera[4], camera[5]},
                            {camera[6], camera[7], camera[8]}, {camera[9], camera[10], camera[11]}};
-        oracle::RenderSettings rs{width, height, spp, depth, nee, poolSize, maxSamples, threads, accumulationMode, rngOffset};
+        oracle::RenderSettings rs{width, height, spp, depth, nee, poolSize, maxSamples, threads, accumulationMode, rngOffset,
+                                  rngPolicy, lightMode};
         return oracle::Render(*s, cam, rs, sampleRadiance, accumulation, framebuffer, queueLog, queueLogCapacity, iterations);
     }
 

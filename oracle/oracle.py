@@ -52,7 +52,12 @@ def lib():
         L.oracle_sincos.argtypes = [vp, u32, vp, vp]
         L.oracle_pow.argtypes = [vp, vp, u32, vp]
         L.oracle_render.restype = i32
-        L.oracle_render.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, u64, i32, i32, vp, vp, vp, vp, u32, vp, u64]
+        L.oracle_render.argtypes = [vp, vp, u32, u32, u32, u32, u32, u32, u64, i32, i32, vp, vp, vp, vp, u32, vp, u64, u32, u32]
+        L.oracle_scene_alias_power_export.argtypes = [vp, vp]
+        L.oracle_power_alias_build.argtypes = [vp, vp, u32, vp]
+        L.oracle_device_order_scan.argtypes = [vp, u32, vp]
+        L.oracle_pcg_words.argtypes = [u64, u64, u32, vp, vp]
+        L.oracle_pcg_seeded_words.argtypes = [u64, u64, u32, vp]
         L.oracle_make_camera.argtypes = [f32, f32, vp, vp, vp]
         _lib = L
     return _lib
@@ -95,11 +100,12 @@ class OracleScene:
         lib().oracle_scene_bvh_export(self.handle, _p(nodes), _p(order))
         return nodes, order, lib().oracle_scene_bvh_depth(self.handle)
 
-    def alias_table(self):
+    def alias_table(self, power: bool = False):
+        """The light alias table: area weights (the reference's), or the product's power weights."""
         n = lib().oracle_scene_light_count(self.handle)
         bins = np.zeros(n, dtype=BIN_DTYPE)
         if n:
-            lib().oracle_scene_alias_export(self.handle, _p(bins))
+            (lib().oracle_scene_alias_power_export if power else lib().oracle_scene_alias_export)(self.handle, _p(bins))
         return bins
 
     def trace_closest(self, rays: np.ndarray, threads: int | None = None):
@@ -118,9 +124,10 @@ class OracleScene:
 
     def render(self, camera: np.ndarray, width: int, height: int, spp: int, depth: int, nee: bool = True,
                pool_size: int = 1 << 20, max_samples: int = 0, threads: int | None = None, accumulation: int = 1,
-               log_capacity: int = 1 << 16, rng_offset: int = 0):
+               log_capacity: int = 1 << 16, rng_offset: int = 0, rng_policy: int = 0, light_sampling: int = 0):
         """Replay of Renderer::RenderFrame on the CPU. accumulation: 0 = FP32 in
-        sample order, 1 = FP32 Kahan in sample order, 2 = FP64."""
+        sample order, 1 = FP32 Kahan in sample order, 2 = FP64. rng_policy: 0 = Philox
+        (the reference's), 1 = PCG32; light_sampling: 0 = area (the reference's), 1 = power."""
         spa = int(np.sqrt(spp))
         spp_eff = spa * spa
         total = spp_eff * width * height
@@ -134,7 +141,8 @@ class OracleScene:
         iters = ctypes.c_uint32(0)
         rc = lib().oracle_render(self.handle, _p(camera), width, height, spp, depth, 1 if nee else 0, pool_size,
                                  max_samples, threads or default_threads(), accumulation, _p(radiance), _p(accum),
-                                 _p(fb), _p(qlog), log_capacity, ctypes.byref(iters), rng_offset)
+                                 _p(fb), _p(qlog), log_capacity, ctypes.byref(iters), rng_offset, rng_policy,
+                                 light_sampling)
         if rc != 0:
             raise RuntimeError(f"oracle_render failed: {rc}")
         it = iters.value
@@ -162,6 +170,48 @@ def philox_words(subsequence: int, position: int, count: int):
     uni = np.zeros(count, dtype=np.float32)
     lib().oracle_philox_words(subsequence, position, count, _p(words), _p(uni))
     return words, uni
+
+
+def power_alias_build(power: np.ndarray, area: np.ndarray) -> np.ndarray:
+    """The product's power-weighted alias table (parallel sweep, device-order FP64 prefix sums)."""
+    power = np.ascontiguousarray(power, dtype=np.float64)
+    area = np.ascontiguousarray(area, dtype=np.float64)
+    bins = np.zeros(power.size, dtype=BIN_DTYPE)
+    lib().oracle_power_alias_build(_p(power), _p(area), power.size, _p(bins))
+    return bins
+
+
+def device_order_scan(x: np.ndarray) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.zeros_like(x)
+    lib().oracle_device_order_scan(_p(x), x.size, _p(out))
+    return out
+
+
+def pcg_words(key: int, position: int, count: int):
+    words = np.zeros(count, dtype=np.uint32)
+    uni = np.zeros(count, dtype=np.float32)
+    lib().oracle_pcg_words(key, position, count, _p(words), _p(uni))
+    return words, uni
+
+
+def pcg_seeded_words(initstate: int, initseq: int, count: int) -> np.ndarray:
+    words = np.zeros(count, dtype=np.uint32)
+    lib().oracle_pcg_seeded_words(initstate, initseq, count, _p(words))
+    return words
+
+
+def alias_implied_pmf(bins: np.ndarray) -> np.ndarray:
+    """Probability of every outcome that an alias table encodes: (q_k + sum over bins aliasing k of
+    (1 - q)) / n, in FP64. Equals the target pmf for a correct table."""
+    n = bins.size
+    q = bins["q"].astype(np.float64)
+    out = q.copy()
+    alias = bins["alias"]
+    valid = alias != 0xFFFFFFFF
+    np.add.at(out, alias[valid].astype(np.int64), 1.0 - q[valid])
+    out[~valid] += 1.0 - q[~valid]  # leftovers keep their own outcome (q is 1 there)
+    return out / n
 
 
 def sincos(x: np.ndarray):

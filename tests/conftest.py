@@ -45,7 +45,17 @@ def oracle_scene():
 
 @pytest.fixture(scope="session")
 def gpu_renderer():
+    """The deterministic build (libgpt_b200_det.so): bit-for-bit comparable with the oracle."""
     import pathtracer
-    r = pathtracer.Renderer(0)
+    r = pathtracer.Renderer(0, variant="det")
+    yield r
+    r.close()
+
+
+@pytest.fixture(scope="session")
+def gpu_renderer_product():
+    """The product build (libgpt_b200.so): the reference build's arithmetic."""
+    import pathtracer
+    r = pathtracer.Renderer(0, variant="product")
     yield r
     r.close()

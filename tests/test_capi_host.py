@@ -24,11 +24,13 @@ def header_functions():
     return sorted(set(re.findall(r"\b(gpt_[a-z0-9_]+)\s*\(", text)))
 
 
-def test_library_loads_and_exports_every_declared_symbol():
-    lib = pathtracer.lib()
+@pytest.mark.parametrize("variant", ["product", "det"])
+def test_library_loads_and_exports_every_declared_symbol(variant):
+    lib = pathtracer.lib(variant)
     declared = header_functions()
     assert len(declared) >= 30
-    out = subprocess.run(["nm", "-D", "--defined-only", pathtracer.LIB_PATH], capture_output=True, text=True, check=True).stdout
+    out = subprocess.run(["nm", "-D", "--defined-only", pathtracer.LIB_PATHS[variant]], capture_output=True, text=True,
+                         check=True).stdout
     exported = set(re.findall(r" T (gpt_[a-z0-9_]+)", out))
     missing = [f for f in declared if f not in exported]
     assert not missing, missing
@@ -45,6 +47,28 @@ def test_library_is_built_for_sm100a():
     assert arch == [("compute_100a", "sm_100a")]
     assert re.search(r"^ARCH\s*=", makefile, re.M)
     assert makefile.count("$(ARCH)") >= 2
+
+
+def test_product_and_deterministic_builds_differ_only_in_the_wavefront_arithmetic():
+    # the product compiles the wavefront kernels with contraction and CUDA's transcendentals; the
+    # deterministic build without contraction and with the IEEE definitions; the scene-upload kernels
+    # (host-code restatements) are shared and never contracted
+    makefile = (Path(pathtracer.LIB_PATH).parent / "Makefile").read_text()
+    flags = dict(re.findall(r"^(NVFLAGS_\w+)\s*=\s*(.*)$", makefile, re.M))
+    assert "-fmad=false" in flags["NVFLAGS_DET"] and "-DPT_CUDA_MATH=0" in flags["NVFLAGS_DET"]
+    assert "-fmad=false" not in flags["NVFLAGS_PROD"] and "-DPT_CUDA_MATH=1" in flags["NVFLAGS_PROD"]
+    assert re.search(r"scene_kernels\.o: .*\n\t\$\(NVCC\) \$\(NVFLAGS_DET\)", makefile)
+    assert re.search(r"kernels_prod\.o: .*\n\t\$\(NVCC\) \$\(NVFLAGS_PROD\)", makefile)
+
+
+def test_noalloc_rejects_misaligned_or_missing_pointers_before_any_device_work():
+    # argument checks run before the library touches the device, so fake addresses are safe here
+    lib = pathtracer.lib()
+    vp = ctypes.c_void_p
+    assert lib.gpt_build_alias_table_noalloc(vp(0x10000), 4, vp(0x20008), None) == 1   # bins not 16-byte aligned
+    assert lib.gpt_build_alias_table_noalloc(vp(0x10002), 4, vp(0x20000), None) == 1   # weights not 4-byte aligned
+    assert lib.gpt_build_alias_table_noalloc(None, 4, vp(0x20000), None) == 1
+    assert lib.gpt_build_alias_table_noalloc(vp(0x10000), 0, vp(0x20008), None) == 0   # no lights: nothing to do
 
 
 def test_status_strings():

@@ -79,6 +79,31 @@ def test_noalloc_alias_table_matches_scene_upload_two_calls_in_a_row():
     assert np.array_equal(got_a, ref_a)
 
 
+def test_noalloc_on_a_non_default_stream_and_with_no_lights():
+    """The build is ordered on the caller's stream (here a side stream, not the default one), and a
+    call with no lights succeeds without touching the output."""
+    import ctypes
+
+    import torch
+    b = many_lights_scene(3000, seed=9)
+    ref = reference_table(b)
+    w = torch.from_numpy(light_weights(b)).cuda()
+    bins = torch.full((w.shape[0], 4), -1, dtype=torch.int32, device="cuda")
+    side = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        rc = pathtracer.build_alias_table_noalloc(w, bins)   # binds torch's current stream: the side stream
+        done = bins.cpu()                                   # ordered after the build on the same stream
+    assert rc == 0
+    assert np.array_equal(done.numpy().view(np.uint32), ref)
+    before = bins.clone()
+    rc = pathtracer.lib().gpt_build_alias_table_noalloc(ctypes.c_void_p(w.data_ptr()), 0, ctypes.c_void_p(bins.data_ptr()),
+                                                        ctypes.c_void_p(side.cuda_stream))
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert torch.equal(bins, before)
+
+
 def test_noalloc_rejects_tables_above_its_limit():
     import torch
     n = 65537  # GPT_NOALLOC_MAX_LIGHTS + 1
