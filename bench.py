@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--trace-refill", type=int, default=0, help="with --no-autotune: idle lanes before a warp refills")
     ap.add_argument("--trace-block", type=int, default=0, help="with --no-autotune: traversal threads per block")
     ap.add_argument("--sections", default="all",
-                    help="comma list of extra one-GPU sections: plain,cornell,batched,serving,precision (all/none)")
+                    help="comma list of extra one-GPU sections: plain,cornell,batched,serving,precision,lights (all/none)")
     ap.add_argument("--serve-jobs", type=int, default=48, help="jobs per arrival rate in the serving section")
     ap.add_argument("--no-reference-build", action="store_true",
                     help="skip timing the reference's own kernels (oracle/_ref) on the same frame")
@@ -79,7 +79,7 @@ def parse():
     return ap.parse_args()
 
 
-SECTIONS = ("plain", "cornell", "batched", "serving", "precision")
+SECTIONS = ("plain", "cornell", "batched", "serving", "precision", "lights")
 
 
 def wanted_sections(args):
@@ -481,6 +481,8 @@ def summary(line):
            "reference_build_b200_value": get(line, "reference_build_b200", "value"),
            "reference_build_b200_speedup_of_value": get(line, "reference_build_b200", "speedup_of_value"),
            "batched_speedup_vs_plain_form": get(line, "batched", "speedup_vs_plain_form"),
+           "power_sampling_samples_for_equal_rmse_c2": get(line, "light_sampling", "spheres-1m", "power", "samples_for_equal_rmse_vs_area"),
+           "power_sampling_samples_for_equal_rmse_c4": get(line, "light_sampling", "spheres-8m", "power", "samples_for_equal_rmse_vs_area"),
            "cpu_baseline_value": get(line, "cpu_baseline", "value")}
     serving = line.get("serving")
     if isinstance(serving, dict) and isinstance(serving.get("served"), dict):
@@ -488,6 +490,72 @@ def summary(line):
             rate: {"served_p50": v.get("p50_latency_s"), "served_p99": v.get("p99_latency_s"),
                    "plain_p50": get(serving, "plain", rate, "p50_latency_s"), "plain_p99": get(serving, "plain", rate, "p99_latency_s")}
             for rate, v in serving["served"].items() if isinstance(v, dict)}
+    return out
+
+
+def light_sampling_section(knobs, scene_names=("spheres-1m", "spheres-8m"), res=(480, 270), spp=64, ref_spp=4096, trials=3):
+    """Power-weighted against area-weighted light selection (and PCG32 against Philox) at equal paths.
+    Per scene and mode: the RMSE of a spp-sample frame against a converged ref_spp-sample frame of the
+    same mode, accumulated in FP64 and rendered by the deterministic build (whose arithmetic equals the
+    CPU oracle's bit for bit), averaged over `trials` independent frames (distinct stream offsets); and
+    the product's paths/s on the full-size frame of the headline workload in each mode. "Paths/s at
+    equal RMSE" scales a mode's paths/s by (RMSE area / RMSE mode)^2, the factor by which the area mode
+    needs more samples for the same error. The shadow-radiance clamp (Intersect.cu:178) makes the two
+    modes' converged images differ slightly; that difference is reported too."""
+    import pathtracer
+    import scenes
+    W, H = res
+    out = {"config": f"{W}x{H}, {spp} spp vs a {ref_spp}-spp FP64-accumulated frame of the same mode (deterministic build), "
+                     f"{trials} trials, depth per workload, NEE",
+           "modes": {"area": "LightSampler.cpp:16-19 weights (the reference's)", "power": "area x luminance(emission), FP64 prefix sums",
+                     "power_pcg32": "power weights, PCG32 streams"}}
+    modes = {"area": (pathtracer.LIGHTS_AREA, pathtracer.RNG_PHILOX), "power": (pathtracer.LIGHTS_POWER, pathtracer.RNG_PHILOX),
+             "power_pcg32": (pathtracer.LIGHTS_POWER, pathtracer.RNG_PCG32)}
+    for name in scene_names:
+        s = scenes.config_scene(name)
+        depth = 12 if name == "spheres-1m" else 10
+        cam = scenes.scene_camera(s, W, H)
+        det = pathtracer.Renderer(0, variant="det")
+        prod = pathtracer.Renderer(0)
+        res_out = {}
+        try:
+            det.upload_scene(s)
+            prod.upload_scene(s)
+            refs = {}
+            for m, (lights, rng) in modes.items():
+                if m == "power_pcg32":
+                    refs[m] = refs["power"]
+                    continue
+                det.render_frame(cam, W, H, ref_spp, depth, True, light_sampling=lights, rng_offset=1 << 44)
+                refs[m] = det.accumulation_fp64() / ref_spp
+            for m, (lights, rng) in modes.items():
+                errs = []
+                for k in range(trials):
+                    prod.render_frame(cam, W, H, spp, depth, True, light_sampling=lights, rng_policy=rng, rng_offset=k * W * H * spp,
+                                      **knobs)
+                    img = prod.accumulation()[:, :3].astype(np.float64) / spp
+                    errs.append(float(np.sqrt(np.mean((img - refs[m]) ** 2))))
+                res_out[m] = {"rmse": float(np.mean(errs)), "rmse_trials": errs}
+            base = res_out["area"]["rmse"]
+            for m in res_out:
+                res_out[m]["samples_for_equal_rmse_vs_area"] = (res_out[m]["rmse"] / base) ** 2
+            res_out["converged_difference_rmse_power_vs_area"] = float(np.sqrt(np.mean((refs["power"] - refs["area"]) ** 2)))
+            res_out["converged_rms"] = float(np.sqrt(np.mean(refs["area"] ** 2)))
+            if name == WORKLOAD["scene"]:
+                fw, fh, fspp = WORKLOAD["width"], WORKLOAD["height"], WORKLOAD["spp"]
+                fcam = scenes.scene_camera(s, fw, fh)
+                for m, (lights, rng) in modes.items():
+                    prod.render_frame(fcam, fw, fh, fspp, depth, True, light_sampling=lights, rng_policy=rng, **knobs)
+                    st = [prod.render_frame(fcam, fw, fh, fspp, depth, True, light_sampling=lights, rng_policy=rng, **knobs) for _ in range(2)]
+                    ms = sum(x["device_ms"] for x in st) / len(st)
+                    pps = st[0]["samples"] / (ms / 1000.0)
+                    res_out[m]["full_frame_paths_per_second"] = pps
+                    res_out[m]["full_frame_ms"] = ms
+                    res_out[m]["paths_per_second_at_equal_rmse"] = pps / res_out[m]["samples_for_equal_rmse_vs_area"]
+        finally:
+            det.close()
+            prod.close()
+        out[name] = res_out
     return out
 
 
@@ -682,6 +750,8 @@ def b200_arm(args):
         if "bvh" in pr:
             per_scene["spheres-8m"] = {"value": pr["bvh"]["bvh8_q8"]["paths_per_second"], "unit": "paths/s",
                                        "config": "3840x2160, 16 spp, depth 10, NEE"}
+    if "lights" in sections:
+        line["light_sampling"] = run_section("lights", lambda: light_sampling_section(knobs))
     if sections:
         line["per_scene"] = per_scene
         line["section_seconds"] = timings

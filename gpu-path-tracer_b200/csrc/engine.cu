@@ -243,7 +243,8 @@ namespace pt
             refillShadow_ = ((cfg_.trace_refill >> 8) & 0xFFu) ? std::min(32u, std::max(1u, (cfg_.trace_refill >> 8) & 0xFFu))
                                                                 : std::max(1u, refill_ / 2u);
             occupancy_ = cfg_.trace_occupancy == 0 ? 10 : (cfg_.trace_occupancy >= 12 ? 12 : (cfg_.trace_occupancy >= 10 ? 10 : 1));
-            shortestFirst_ = cfg_.schedule != GPT_SCHEDULE_OLDEST_FIRST;
+            schedule_ = cfg_.schedule == 0 ? GPT_SCHEDULE_SHORTEST_FIRST : cfg_.schedule;
+            if (!(cfg_.deadline_slowdown > 0.0f)) cfg_.deadline_slowdown = 4.0f;
             t0_ = std::chrono::steady_clock::now();
         }
 
@@ -275,7 +276,7 @@ namespace pt
 
         Status Init()
         {
-            if (cfg_.schedule > GPT_SCHEDULE_OLDEST_FIRST) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
+            if (cfg_.schedule > GPT_SCHEDULE_DEADLINE) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking));
@@ -662,14 +663,19 @@ namespace pt
                 pending_.pop_front();
             }
             // Slot priority of the next slice: the device plan hands idle slots to the jobs in this order.
-            std::vector<std::pair<uint64_t, uint32_t>> ranked;
+            std::vector<std::pair<double, uint32_t>> ranked;
             ranked.reserve(active_.size());
             for (uint64_t id : active_)
             {
-                const uint32_t t = records_[id].tableIndex;
+                const JobRecord& J = records_[id];
+                const uint32_t t = J.tableIndex;
                 const JobView& v = mirror_[t];
                 const uint64_t left = v.totalSamples > v.launched ? v.totalSamples - v.launched : 0;
-                ranked.emplace_back(shortestFirst_ ? left : 0, t);  // stable: submission order among equals
+                double key = 0.0;  // oldest first: all equal, the stable sort keeps submission order
+                if (schedule_ == GPT_SCHEDULE_SHORTEST_FIRST) key = static_cast<double>(left);
+                else if (schedule_ == GPT_SCHEDULE_DEADLINE)
+                    key = J.tSubmit + cfg_.deadline_slowdown * static_cast<double>(v.totalSamples) / rateEstimate_;
+                ranked.emplace_back(key, t);
             }
             std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
             uint32_t n = 0;
@@ -706,6 +712,14 @@ namespace pt
             PT_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, startEvent_, stopEvent_));
             deviceMs_ += ms;
             slices_++;
+            // paths per second of the server (device time), smoothed over slices; deadline scheduling's clock
+            const uint64_t samples = hostCounters_->launched;
+            if (ms > 0.5f && samples > lastSliceSamples_)
+            {
+                const double rate = static_cast<double>(samples - lastSliceSamples_) / (ms / 1000.0);
+                rateEstimate_ = 0.8 * rateEstimate_ + 0.2 * rate;
+            }
+            lastSliceSamples_ = samples;
             if (hostCounters_->errorFlags)
                 return Status::Err(GPT_ERR_DEVICE_FAULT, "Traversal reported error flags " + std::to_string(hostCounters_->errorFlags));
             if (hostCtl_->stalled) return Status::Err(GPT_ERR_DEVICE_FAULT, "Job engine stalled with unfinished jobs");
@@ -859,7 +873,9 @@ namespace pt
         int device_;
         gpt_server_config cfg_;
         int threads_ = 128, occupancy_ = 10;
-        bool shortestFirst_ = true;
+        uint32_t schedule_ = GPT_SCHEDULE_SHORTEST_FIRST;
+        double rateEstimate_ = 1e9;        // paths per second, smoothed (initial guess: one B200 on a mid-size scene)
+        uint64_t lastSliceSamples_ = 0;
         uint32_t refill_ = 16, refillShadow_ = 8;
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;

@@ -27,6 +27,17 @@
 
 namespace pt
 {
+    // gpt_inject_allocation_failure: allocations left until the injected failure (0 = none armed).
+    std::atomic<uint32_t> g_allocationCountdown{0};
+
+    bool InjectedAllocationFailure()
+    {
+        uint32_t c = g_allocationCountdown.load();
+        while (c != 0)
+            if (g_allocationCountdown.compare_exchange_weak(c, c - 1)) return c == 1;
+        return false;
+    }
+
     static Status CreateTexture(const gpt_texture_desc& d, TextureObject& t)
     {
         if (d.width == 0 || d.height == 0 || !d.data || (d.channels != 1 && d.channels != 3 && d.channels != 4) || d.format > GPT_TEXEL_F32)
@@ -405,6 +416,8 @@ namespace pt
             int occupancy;
             uint32_t bvh;
             bool queues;   // the reference's wavefront structure (regeneration queue, shading in sequence)
+            uint32_t maxIterations;  // 0 = automatic
+            uint32_t stack;          // traversal stack entries chosen by the caller, 0 = the tree's depth
         };
 
         Status resolveConfig(const gpt_render_settings& s, FrameConfig& c) const
@@ -439,7 +452,18 @@ namespace pt
                 return Status::Err(GPT_ERR_STATE, "The scene has no binary BVH");
             if (s.wavefront_layout > GPT_WAVEFRONT_QUEUES) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown wavefront layout");
             c.queues = s.wavefront_layout == GPT_WAVEFRONT_QUEUES;
+            c.maxIterations = s.max_iterations;
+            if (s.trace_stack > kMaxStack) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "trace_stack above 64 entries");
+            c.stack = s.trace_stack == 0 ? 0u : (s.trace_stack <= 8 ? 8u : (s.trace_stack <= 16 ? 16u : (s.trace_stack <= 32 ? 32u : 64u)));
             return Status::Ok();
+        }
+
+        // The scene as the frame's kernels see it: the traversal stack variant follows view.depth.
+        SceneView frameView(const FrameConfig& c) const
+        {
+            SceneView v = scene_->view();
+            if (c.stack) v.depth = c.stack;
+            return v;
         }
 
         void releaseGraph()
@@ -455,7 +479,7 @@ namespace pt
             releaseGraph();
             int sms = 0;
             PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-            const SceneView sv = scene_->view();
+            const SceneView sv = frameView(c);
             const Wavefront wf = wavefront(c.queues);
             const JobView* jobDev = job_.get<JobView>();
             // prologue and resolve as captured child graphs
@@ -527,7 +551,7 @@ namespace pt
         {
             int sms = 0;
             PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
-            const SceneView sv = scene_->view();
+            const SceneView sv = frameView(c);
             const Wavefront wf = wavefront(c.queues);
             const JobView* jobDev = job_.get<JobView>();
             if (!traceStart_) PT_CUDA("cudaEventCreate", cudaEventCreate(&traceStart_));
@@ -579,8 +603,8 @@ namespace pt
         std::string key(const FrameConfig& c) const
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%d/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
-                          c.nee, c.traceThreads, c.refill | (c.refillShadow << 8), c.occupancy, c.bvh, c.queues ? 1 : 0, width_, height_,
+            std::snprintf(buf, sizeof(buf), "%llu/%u/%u/%d/%u/%d/%u/%d/%u/%u/%u/%p/%p", static_cast<unsigned long long>(scene_->version), c.pool,
+                          c.nee, c.traceThreads, c.refill | (c.refillShadow << 8), c.occupancy, c.bvh, c.queues ? 1 : 0, c.stack, width_, height_,
                           static_cast<void*>(accumulation_.get<void>()),
                           static_cast<void*>(framebuffer_.get<void>()));
             return buf;
@@ -619,6 +643,7 @@ namespace pt
             jv.lightMode = s.light_sampling;
             const uint64_t rounds = (c.totalSamples + c.pool - 1) / c.pool;
             jv.maxIterations = static_cast<uint32_t>(std::min<uint64_t>(0xFFFFFFF0ull, static_cast<uint64_t>(c.depth) * (rounds + 2) + 64));
+            if (c.maxIterations) jv.maxIterations = std::min(jv.maxIterations, c.maxIterations);
             hostJob_ = jv;
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(job_.get<void>(), &hostJob_, sizeof(JobView), cudaMemcpyHostToDevice, stream_));
             lastTotalSamples_ = c.totalSamples;
@@ -1231,6 +1256,12 @@ extern "C"
         return Report(r, pt::CudaStatus("cudaMemcpy", e));
     }
 
+    int gpt_inject_allocation_failure(uint32_t after)
+    {
+        pt::g_allocationCountdown.store(after);
+        return GPT_OK;
+    }
+
     int gpt_read_alias_table_power(gpt_renderer* r, uint32_t* bins, uint32_t count)
     {
         if (!r || !bins) return GPT_ERR_INVALID_ARGUMENT;
@@ -1283,10 +1314,10 @@ extern "C"
     int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count)
     {
         if (!sizes) return GPT_ERR_INVALID_ARGUMENT;
-        const uint32_t all[11] = {sizeof(gpt_material), sizeof(gpt_scene_desc), sizeof(gpt_device_camera), sizeof(gpt_motion_state),
+        const uint32_t all[12] = {sizeof(gpt_material), sizeof(gpt_scene_desc), sizeof(gpt_device_camera), sizeof(gpt_motion_state),
                                   sizeof(gpt_render_settings), sizeof(gpt_frame_stats), sizeof(gpt_texture_desc), sizeof(gpt_server_config),
-                                  sizeof(gpt_job_desc), sizeof(gpt_job_status), sizeof(gpt_server_stats)};
-        for (uint32_t i = 0; i < count && i < 11; i++) sizes[i] = all[i];
+                                  sizeof(gpt_job_desc), sizeof(gpt_job_status), sizeof(gpt_server_stats), sizeof(gpt_motion_sample)};
+        for (uint32_t i = 0; i < count && i < 12; i++) sizes[i] = all[i];
         return GPT_OK;
     }
 

@@ -39,6 +39,9 @@ namespace pt
     } while (0)
 #define PT_CUDA(op, expr) PT_TRY(CudaStatus(op, (expr)))
 
+    // True when this device allocation is the one gpt_inject_allocation_failure chose to fail.
+    bool InjectedAllocationFailure();
+
     // RAII device allocation (the reference's DeviceBuffer1D, Runtime/Memory/DeviceBuffer1D.cpp:33-80).
     class DeviceBuffer
     {
@@ -52,6 +55,8 @@ namespace pt
             if (bytes <= bytes_ && ptr_) return Status::Ok();
             reset();
             if (bytes == 0) return Status::Ok();
+            if (InjectedAllocationFailure())
+                return Status::Err(GPT_ERR_OUT_OF_MEMORY, "cudaMalloc failed: out of memory (injected by gpt_inject_allocation_failure)");
             PT_CUDA("cudaMalloc", cudaMalloc(&ptr_, bytes));
             bytes_ = bytes;
             return Status::Ok();

@@ -64,20 +64,24 @@ class gpt_motion_state(ctypes.Structure):
     _fields_ = [("position", ctypes.c_float * 3), ("rotation", ctypes.c_float * 4)]
 
 
+class gpt_motion_sample(ctypes.Structure):
+    _fields_ = [("state", gpt_motion_state), ("time", ctypes.c_float)]
+
+
 class gpt_render_settings(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("samples_per_pixel", ctypes.c_uint32),
                 ("path_depth", ctypes.c_uint32), ("use_nee", ctypes.c_uint32), ("pool_size", ctypes.c_uint32),
                 ("max_samples", ctypes.c_uint64), ("trace_block", ctypes.c_uint32), ("trace_refill", ctypes.c_uint32),
                 ("rng_offset", ctypes.c_uint64), ("loop_mode", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
                 ("bvh_format", ctypes.c_uint32), ("wavefront_layout", ctypes.c_uint32), ("rng_policy", ctypes.c_uint32),
-                ("light_sampling", ctypes.c_uint32)]
+                ("light_sampling", ctypes.c_uint32), ("max_iterations", ctypes.c_uint32), ("trace_stack", ctypes.c_uint32)]
 
 LOOP_GRAPH, LOOP_HOST = 0, 1
 RNG_PHILOX, RNG_PCG32 = 0, 1
 LIGHTS_AREA, LIGHTS_POWER = 0, 1
 BVH8_Q8, BVH2_FP32 = 0, 1
 WAVEFRONT_B200, WAVEFRONT_QUEUES = 0, 1
-SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST = 1, 2
+SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST, SCHEDULE_DEADLINE = 1, 2, 3
 NODE_BYTES = {BVH8_Q8: 64 + 4, BVH2_FP32: 64}  # bytes a node visit reads: BVH8 header + its child reference; the whole binary node
 
 
@@ -94,7 +98,7 @@ class gpt_server_config(ctypes.Structure):
     _fields_ = [("pool_size", ctypes.c_uint32), ("max_jobs", ctypes.c_uint32), ("max_active_jobs", ctypes.c_uint32),
                 ("ring_passes", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_uint64), ("trace_block", ctypes.c_uint32),
                 ("trace_refill", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
-                ("max_slice_iterations", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("max_slice_iterations", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("deadline_slowdown", ctypes.c_float)]
 
 
 class gpt_job_desc(ctypes.Structure):
@@ -173,6 +177,7 @@ _SIGNATURES = [
                                              ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_read_alias_table_power", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
+    ("gpt_inject_allocation_failure", ctypes.c_int, [ctypes.c_uint32]),
     ("gpt_bvh8_check", ctypes.c_int, [ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32),
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(ctypes.c_uint64)]),
@@ -184,6 +189,8 @@ _SIGNATURES = [
     ("gpt_abi_struct_sizes", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32]),
     ("gpt_make_device_camera", ctypes.c_int, [ctypes.c_float, ctypes.c_float, ctypes.POINTER(gpt_motion_state),
                                               ctypes.POINTER(gpt_device_camera)]),
+    ("gpt_resample_motion", ctypes.c_int, [ctypes.POINTER(gpt_motion_sample), ctypes.c_uint32, ctypes.c_float,
+                                           ctypes.POINTER(gpt_motion_state), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_server_create", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.POINTER(gpt_server_config)]),
     ("gpt_server_destroy", ctypes.c_int, [ctypes.c_void_p]),
     ("gpt_server_add_scene", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc), ctypes.POINTER(ctypes.c_uint32)]),
@@ -306,11 +313,11 @@ class Renderer:
                      pool_size: int = 0, max_samples: int = 0, trace_block: int = 0, trace_refill: int = 0,
                      rng_offset: int = 0, loop_mode: int = LOOP_GRAPH, trace_occupancy: int = 0,
                      bvh_format: int = BVH8_Q8, wavefront_layout: int = WAVEFRONT_B200, rng_policy: int = RNG_PHILOX,
-                     light_sampling: int = LIGHTS_AREA) -> dict:
+                     light_sampling: int = LIGHTS_AREA, max_iterations: int = 0, trace_stack: int = 0) -> dict:
         cam = camera_struct(camera12)
         st = gpt_render_settings(width, height, spp, depth, 1 if nee else 0, pool_size, max_samples, trace_block,
                                  trace_refill, rng_offset, loop_mode, trace_occupancy, bvh_format, wavefront_layout,
-                                 rng_policy, light_sampling)
+                                 rng_policy, light_sampling, max_iterations, trace_stack)
         stats = gpt_frame_stats()
         self._check(self.L.gpt_render_frame(self.h, ctypes.byref(cam), ctypes.byref(st), ctypes.byref(stats)),
                     "gpt_render_frame")
@@ -474,10 +481,32 @@ def abi_struct_sizes() -> dict:
     """sizeof() of the public structs as compiled into the library."""
     names = ["gpt_material", "gpt_scene_desc", "gpt_device_camera", "gpt_motion_state", "gpt_render_settings",
              "gpt_frame_stats", "gpt_texture_desc", "gpt_server_config", "gpt_job_desc", "gpt_job_status",
-             "gpt_server_stats"]
+             "gpt_server_stats", "gpt_motion_sample"]
     out = (ctypes.c_uint32 * len(names))()
     lib().gpt_abi_struct_sizes(out, len(names))
     return {n: out[i] for i, n in enumerate(names)}
+
+
+def resample_motion(samples, interval: float):
+    """Recorded camera path -> one (position, quaternion wxyz) state per frame (gpt_resample_motion).
+    samples: iterable of (position3, quaternion4 wxyz, time)."""
+    samples = list(samples)
+    arr = (gpt_motion_sample * max(1, len(samples)))()
+    for i, (pos, quat, t) in enumerate(samples):
+        for k in range(3):
+            arr[i].state.position[k] = pos[k]
+        for k in range(4):
+            arr[i].state.rotation[k] = quat[k]
+        arr[i].time = t
+    n = ctypes.c_uint32()
+    rc = lib().gpt_resample_motion(arr, len(samples), ctypes.c_float(interval), None, 0, ctypes.byref(n))
+    if rc not in (0, 6):
+        raise GptError(rc, "gpt_resample_motion")
+    out = (gpt_motion_state * max(1, n.value))()
+    rc = lib().gpt_resample_motion(arr, len(samples), ctypes.c_float(interval), out, n.value, ctypes.byref(n))
+    if rc != 0:
+        raise GptError(rc, "gpt_resample_motion")
+    return [(tuple(out[i].position), tuple(out[i].rotation)) for i in range(n.value)]
 
 
 def bvh8_check(scene) -> dict:
@@ -572,10 +601,11 @@ class Server:
 
     def __init__(self, device: int = 0, pool_size: int = 0, max_jobs: int = 0, max_active_jobs: int = 0,
                  ring_passes: int = 0, hbm_budget_bytes: int = 0, trace_block: int = 0, trace_refill: int = 0,
-                 trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0, variant: str = "product"):
+                 trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0, deadline_slowdown: float = 0.0,
+                 variant: str = "product"):
         self.L = lib(variant)
         cfg = gpt_server_config(pool_size, max_jobs, max_active_jobs, ring_passes, hbm_budget_bytes, trace_block,
-                                trace_refill, trace_occupancy, max_slice_iterations, schedule, 0)
+                                trace_refill, trace_occupancy, max_slice_iterations, schedule, deadline_slowdown)
         h = ctypes.c_void_p()
         rc = self.L.gpt_server_create(ctypes.byref(h), device, ctypes.byref(cfg))
         if rc != 0:

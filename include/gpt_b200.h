@@ -114,6 +114,12 @@ typedef struct gpt_motion_state {
     float rotation[4];
 } gpt_motion_state;
 
+/* Capture::MotionSample (Core/Include/Core/Capture/Sample.hpp:12-16): a recorded state and its time (s). */
+typedef struct gpt_motion_sample {
+    gpt_motion_state state;
+    float time;
+} gpt_motion_sample;
+
 /* Per-frame settings of StartSimulation (Renderer.cpp:330-376) plus B200 tuning knobs. */
 typedef struct gpt_render_settings {
     uint32_t width;
@@ -147,6 +153,12 @@ typedef struct gpt_render_settings {
                                      its area, the reference's light sampler (LightSampler.cpp:16-19); GPT_LIGHTS_POWER:
                                      proportional to area x luminance of its emission (the production mode; the alias
                                      table is built from an FP64 prefix sum by a parallel split on the device) */
+    uint32_t max_iterations;      /* 0 = the automatic bound of the device loop, depth x (ceil(samples / pool) + 2) + 64;
+                                     else at most this many wavefront iterations: a frame that still has paths in flight
+                                     then ends with GPT_ERR_DEVICE_FAULT (the loop's bounded wait running out) */
+    uint32_t trace_stack;         /* 0 = traversal stack sized to the BVH8 depth; else 8, 16, 32 or 64 entries (rounded up
+                                     to one of them): a stack shallower than the tree can overflow, and a ray that
+                                     overflows stops traversing and the frame ends with GPT_ERR_DEVICE_FAULT */
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
@@ -293,6 +305,14 @@ int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count)
 int gpt_read_alias_table_power(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
 
 /*
+ * Fault-injection hook for tests of the error paths (no counterpart in the reference): the
+ * after-th device allocation made by this library from now on (1 = the next one) fails as if the
+ * device were out of memory, on the host, before cudaMalloc is called; 0 disarms. Calls that fail
+ * this way return GPT_ERR_OUT_OF_MEMORY and leave the renderer or server as it was before the call.
+ */
+int gpt_inject_allocation_failure(uint32_t after);
+
+/*
  * Host-side validation of the BVH builder (no device work): builds the wide BVH and the binary FP32
  * BVH for a scene and checks in exact arithmetic that every quantised BVH8 child box and every
  * binary child box contains its subtree, and that every triangle sits in exactly one leaf of each
@@ -367,12 +387,16 @@ typedef struct gpt_server_config {
     uint32_t trace_occupancy;
     uint32_t max_slice_iterations; /* wavefront iterations per graph launch at most (0 = 4096) */
     uint32_t schedule;             /* which active job gets idle path slots first: 0/GPT_SCHEDULE_SHORTEST_FIRST = the
-                                      job with the fewest samples left, GPT_SCHEDULE_OLDEST_FIRST = submission order */
-    uint32_t reserved;
+                                      job with the fewest samples left, GPT_SCHEDULE_OLDEST_FIRST = submission order,
+                                      GPT_SCHEDULE_DEADLINE = the earliest deadline, submit time + deadline_slowdown x the
+                                      job's samples / the server's measured paths per second (small jobs still go
+                                      first, and a large job is not passed over past its deadline) */
+    float deadline_slowdown;       /* GPT_SCHEDULE_DEADLINE: deadline in units of the job's own render time (0 = 4) */
 } gpt_server_config;
 
 #define GPT_SCHEDULE_SHORTEST_FIRST 1u
 #define GPT_SCHEDULE_OLDEST_FIRST 2u
+#define GPT_SCHEDULE_DEADLINE 3u
 
 typedef struct gpt_job_desc {
     uint32_t scene;                /* id from gpt_server_add_scene */
@@ -435,12 +459,24 @@ int gpt_server_peek_last_error(gpt_server* server, char* buffer, size_t length);
 
 /* sizeof() of the public structs as compiled into this library, in the order gpt_material,
  * gpt_scene_desc, gpt_device_camera, gpt_motion_state, gpt_render_settings, gpt_frame_stats,
- * gpt_texture_desc, gpt_server_config, gpt_job_desc, gpt_job_status, gpt_server_stats (for
- * binding checks from other languages). */
+ * gpt_texture_desc, gpt_server_config, gpt_job_desc, gpt_job_status, gpt_server_stats,
+ * gpt_motion_sample (for binding checks from other languages). */
 int gpt_abi_struct_sizes(uint32_t* sizes, uint32_t count);
 
 /* DeviceCamera from fov_y (radians), aspect and a motion state: MakeDeviceCamera (Renderer.cpp:237-257). */
 int gpt_make_device_camera(float fov_y, float aspect, const gpt_motion_state* state, gpt_device_camera* out);
+
+/*
+ * Capture::ResampleMotion (Core/Source/Capture/Resampling.cpp:17-55): a recorded camera path (samples
+ * at strictly increasing times) to one state per frame at a fixed interval from the first sample's
+ * time: position linearly interpolated, rotation by spherical linear interpolation along the shorter
+ * arc and renormalised (Utils/Math/Interpolation.hpp SlerpShortest). The states feed
+ * gpt_start_simulation. *state_count receives the number of states; if it exceeds capacity nothing
+ * is written and GPT_ERR_CAPACITY is returned. interval <= 0 or times that do not increase:
+ * GPT_ERR_INVALID_ARGUMENT. No samples give no states; one sample gives its own state.
+ */
+int gpt_resample_motion(const gpt_motion_sample* samples, uint32_t sample_count, float interval,
+                        gpt_motion_state* states, uint32_t capacity, uint32_t* state_count);
 
 #ifdef __cplusplus
 }

@@ -236,3 +236,41 @@ def make_camera_from_motion(fov_y: float, aspect: float, position, quat_wxyz) ->
     out = np.zeros(12, dtype=np.float32)
     lib().oracle_make_camera(ctypes.c_float(fov_y), ctypes.c_float(aspect), _p(pos), _p(q), _p(out))
     return out
+
+
+def resample_motion(samples, interval: float):
+    """Capture::ResampleMotion (Core/Source/Capture/Resampling.cpp:17-55), in float32 arithmetic:
+    samples (position3, quaternion wxyz, time) at increasing times -> one state per interval from the
+    first time; position by glm::mix (a (1 - t) + b t), rotation by SlerpShortest
+    (Utils/Math/Interpolation.hpp: b negated onto a's hemisphere, slerp with a linear fallback when
+    cos(theta) > 1 - FLT_EPSILON, then normalised)."""
+    f = np.float32
+    samples = [(np.asarray(p, f), np.asarray(q, f), f(t)) for p, q, t in samples]
+    if not samples:
+        return []
+    if len(samples) == 1:
+        return [(samples[0][0], samples[0][1])]
+
+    def slerp_shortest(a, b, t):
+        if f(np.dot(a, b)) < f(0):
+            b = -b
+        cos_theta = f(a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3])
+        if cos_theta > f(1) - np.finfo(f).eps:
+            q = a * (f(1) - t) + b * t
+        else:
+            theta = np.arccos(cos_theta, dtype=f)
+            q = (a * np.sin((f(1) - t) * theta, dtype=f) + b * np.sin(t * theta, dtype=f)) * (f(1) / np.sin(theta, dtype=f))
+        n = np.sqrt(f(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]), dtype=f)
+        return q * (f(1) / n) if n > 0 else np.array([1, 0, 0, 0], f)
+
+    first = samples[0][2]
+    out = [(samples[0][0], samples[0][1])]
+    for i in range(1, len(samples)):
+        (p0, q0, t0), (p1, q1, t1) = samples[i - 1], samples[i]
+        while True:
+            target = f(first + f(len(out)) * f(interval))
+            if target > t1:
+                break
+            t = f((target - t0) / (t1 - t0))
+            out.append((p0 * (f(1) - t) + p1 * t, slerp_shortest(q0, q1, t)))
+    return out

@@ -327,3 +327,83 @@ def test_fp64_reference_accumulation_on_device(gpu_renderer, scene_factory):
     assert np.array_equal(fp64.view(np.uint64), ref.view(np.uint64))
     kahan = gpu_renderer.accumulation()[:, :3].astype(np.float64)
     assert np.all(np.abs(kahan - fp64) <= 4 * np.spacing(np.abs(fp64).astype(np.float32)).astype(np.float64) + 1e-30)
+
+
+def decode_png_rgba8(path):
+    """A PNG's RGBA8 pixels [h, w, 4], rows top to bottom, with every chunk CRC checked (filters 0-4)."""
+    import struct
+    import zlib
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat, w, h = 8, b"", None, None
+    while pos < len(data):
+        length, ctype = struct.unpack(">I4s", data[pos:pos + 8])
+        body = data[pos + 8:pos + 8 + length]
+        assert zlib.crc32(ctype + body) & 0xFFFFFFFF == struct.unpack(">I", data[pos + 8 + length:pos + 12 + length])[0]
+        if ctype == b"IHDR":
+            w, h, bit_depth, color = struct.unpack(">IIBB", body[:10])
+            assert (bit_depth, color) == (8, 6)
+        elif ctype == b"IDAT":
+            idat += body
+        elif ctype == b"IEND":
+            break
+        pos += 12 + length
+    raw = zlib.decompress(idat)
+    stride = 4 * w
+    out = np.zeros((h, stride), np.int64)
+    prev = np.zeros(stride, np.int64)
+    for y in range(h):
+        f = raw[y * (stride + 1)]
+        line = np.frombuffer(raw, np.uint8, stride, y * (stride + 1) + 1).astype(np.int64)
+        cur = np.zeros(stride, np.int64)
+        for i in range(stride):
+            a = cur[i - 4] if i >= 4 else 0
+            b = prev[i]
+            c = prev[i - 4] if i >= 4 else 0
+            if f == 0:
+                pred = 0
+            elif f == 1:
+                pred = a
+            elif f == 2:
+                pred = b
+            elif f == 3:
+                pred = (a + b) // 2
+            else:
+                p = a + b - c
+                pa, pb, pc = abs(p - a), abs(p - b), abs(p - c)
+                pred = a if pa <= pb and pa <= pc else (b if pb <= pc else c)
+            cur[i] = (line[i] + pred) & 255
+        out[y] = cur
+        prev = cur
+    return out.astype(np.uint8).reshape(h, w, 4)
+
+
+def test_simulation_sequence_frames_and_pngs_match_oracle(gpu_renderer, scene_factory, oracle_scene):
+    """A recorded camera path resampled to frames (gpt_resample_motion), rendered by the simulation
+    thread (StartSimulation, Renderer.cpp:401-466): every saved PNG holds, vertically flipped
+    (SaveRenderedFrame, Renderer.cpp:649-675), the oracle's framebuffer for that frame's camera
+    (MakeDeviceCamera from the resampled state), bit for bit; the locked frame is the last one."""
+    s = scene_factory("cornell-all")
+    o = oracle_scene("cornell-all")
+    gpu_renderer.upload_scene(s)
+    W, H, spp, depth = 40, 30, 4, 8
+    fov = np.float32(np.radians(40.0))
+    path = [((0.5, 0.5, 2.2), (1.0, 0.0, 0.0, 0.0), 0.0),
+            ((0.6, 0.55, 2.0), (0.9962, 0.0, 0.0872, 0.0), 0.5),
+            ((0.7, 0.5, 1.9), (0.9848, 0.0, 0.1736, 0.0), 1.2)]
+    states = pathtracer.resample_motion(path, 0.4)
+    assert len(states) == 4
+    with tempfile.TemporaryDirectory() as d:
+        gpu_renderer.start_simulation(W, H, float(fov), states, spp, depth, d, True)
+        t0 = time.time()
+        while gpu_renderer.is_rendering() and time.time() - t0 < 60:
+            time.sleep(0.01)
+        assert gpu_renderer.progress()["done_frames"] == len(states)
+        aspect = float(np.float32(W) / np.float32(H))
+        for k, (pos, quat) in enumerate(states):
+            cam = pathtracer.make_device_camera(float(fov), aspect, pos, quat)
+            ref = o.render(cam, W, H, spp, depth, True)["framebuffer"]
+            png = decode_png_rgba8(os.path.join(d, f"frame_{k:04d}.png"))
+            expect = ref.view(np.uint8).reshape(H, W, 4)[::-1]
+            assert np.array_equal(png, expect), k
+        assert np.array_equal(gpu_renderer.lock_frame(), ref)

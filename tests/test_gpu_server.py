@@ -1,6 +1,8 @@
 """Job server (gpt_server_*): jobs rendered together over resident scenes must give, bit for bit,
 the images the frame renderer (gpt_render_frame) gives for the same scene, camera and settings,
 whether a job runs alone, mixed with others, one at a time, or through a tiny path pool."""
+import time
+
 import numpy as np
 import pytest
 
@@ -107,10 +109,12 @@ def test_mixed_jobs_match_alone(resident, frame_renderers):
         srv.close()
 
 
-@pytest.mark.parametrize("schedule", [pathtracer.SCHEDULE_SHORTEST_FIRST, pathtracer.SCHEDULE_OLDEST_FIRST])
+@pytest.mark.parametrize("schedule", [pathtracer.SCHEDULE_SHORTEST_FIRST, pathtracer.SCHEDULE_OLDEST_FIRST,
+                                      pathtracer.SCHEDULE_DEADLINE])
 def test_schedule_orders_completion_not_images(resident, frame_renderers, schedule):
-    """Shortest-first hands idle slots to the job with the fewest samples left: a small job
-    submitted after a large one finishes first. Either policy gives the same images."""
+    """Shortest-first hands idle slots to the job with the fewest samples left, and earliest-deadline
+    first to the job whose deadline (submit time + slowdown x its size / rate) comes first: in both, a
+    small job submitted right after a large one finishes first. Every policy gives the same images."""
     srv, ids = make_server(resident, pool_size=4096, schedule=schedule)
     try:
         big = ("spheres-small", 128, 128, 64, 12, True, 0)
@@ -119,12 +123,32 @@ def test_schedule_orders_completion_not_images(resident, frame_renderers, schedu
         j_small = submit(srv, ids, resident, small)
         check_job(srv, j_small, frame_renderers, resident, small)
         check_job(srv, j_big, frame_renderers, resident, big)
-        if schedule == pathtracer.SCHEDULE_SHORTEST_FIRST:
+        if schedule != pathtracer.SCHEDULE_OLDEST_FIRST:
             assert srv.poll(j_small)["done_s"] < srv.poll(j_big)["done_s"]
     finally:
         srv.close()
     with pytest.raises(pathtracer.GptError):
-        pathtracer.Server(0, schedule=3)
+        pathtracer.Server(0, schedule=4)
+
+
+def test_deadline_schedule_does_not_pass_over_a_late_job(resident, frame_renderers):
+    """With a deadline of one render time (slowdown 1), a large job that has waited past it ranks
+    before small jobs submitted later: it finishes before the last of a stream of small jobs."""
+    srv, ids = make_server(resident, pool_size=4096, schedule=pathtracer.SCHEDULE_DEADLINE, deadline_slowdown=1.0)
+    try:
+        big = ("spheres-small", 96, 96, 16, 10, True, 0)
+        small = ("cornell-all", 32, 32, 4, 6, True, 0)
+        j_big = submit(srv, ids, resident, big)
+        smalls = []
+        for _ in range(40):
+            smalls.append(submit(srv, ids, resident, small))
+            time.sleep(0.005)
+        check_job(srv, j_big, frame_renderers, resident, big)
+        for j in smalls:
+            check_job(srv, j, frame_renderers, resident, small)
+        assert srv.poll(j_big)["done_s"] < max(srv.poll(j)["done_s"] for j in smalls)
+    finally:
+        srv.close()
 
 
 def test_tiny_pool_and_single_pass_ring(resident, frame_renderers):
