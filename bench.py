@@ -678,6 +678,7 @@ def b200_arm(args):
         "iterations_per_step": iters / args.steps,
         "phase_ms_per_step": {k: sum(s["phase_ms"][k] for s in stats) / args.steps for k in ("trace", "shade", "shadow", "regen")},
         "scene_upload_s": upload_s,
+        "traversal": traversal_summary(stats[-1], NODE_BYTES),
         "roofline": {"kernel": "trace_kernel<closest> (BVH8 closest hit)", "bound": "latency", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "dram_frac": (traffic / per_launch_s / 1e9 / peak) if traffic else None,

@@ -15,7 +15,12 @@
 //     map_RMA texture is given;
 //   BuildTriangles (Core/Source/Graphics/Cuda/PathTracing/Renderer.cpp:116-213): an optional affine
 //     world transform, normals by the inverse transpose, tangents re-orthogonalised to the normal.
-// Texture maps named in the MTL file are recorded but not loaded (image decoding is not on the path).
+//   Texture maps (ObjLoader.cpp:197-225, Manager.cpp:311-385): map_Kd (albedo, sRGB), map_Ks (specular,
+//     sRGB), map_Ns (shininess, linear, first channel), map_RMA (linear), map_Ke (emission, linear), norm
+//     or else map_Bump/bump (normal map, linear), flipped vertically when the material says
+//     flip_textures true; paths relative to the MTL file. PNG and binary PPM/PGM files are decoded
+//     (image_io.cpp); the reference reads any format its image library knows, and other formats are
+//     rejected here with an error naming the file.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -31,6 +36,7 @@
 #include <vector>
 
 #include "../../include/gpt_b200.h"
+#include "image_io.hpp"
 
 struct gpt_obj_scene
 {
@@ -38,6 +44,9 @@ struct gpt_obj_scene
     std::vector<uint32_t> materialIds;
     std::vector<gpt_material> materials;
     std::vector<std::string> materialNames;
+    std::vector<std::vector<uint8_t>> textureData;
+    std::vector<gpt_texture_desc> textures;
+    std::vector<int32_t> materialTextures;  // [materials][GPT_TEX_SLOTS], -1 = the constant
     std::string error;
 };
 
@@ -51,6 +60,10 @@ namespace
         uint32_t model = GPT_MODEL_DIFFUSE;  // Unlit maps to Diffuse (Material.hpp:122-146)
         float kd[3] = {0, 0, 0}, ks[3] = {0, 0, 0}, ke[3] = {0, 0, 0};
         float ns = 1.0f, ni = 1.0f, tf = 0.0f, pr = 0.0f, pm = 0.0f;
+        std::string maps[GPT_TEX_SLOTS];  // texture file per slot (color, specular, shininess, rma, emission, normal)
+        std::string bump;                 // map_Bump / bump: the normal map when there is no norm
+        bool flip = false;
+        std::filesystem::path dir;        // the MTL file's folder
     };
 
     uint8_t lround_u8(float v)
@@ -125,6 +138,7 @@ namespace
             {
                 out.emplace_back();
                 ss >> out.back().name;
+                out.back().dir = file.parent_path();
                 cur = &out.back();
                 continue;
             }
@@ -144,6 +158,28 @@ namespace
                 ss >> v;
                 for (const auto& [name, model] : models)
                     if (v == name) cur->model = model;
+            }
+            else if (key == "flip_textures")
+            {
+                std::string v;
+                ss >> v;
+                cur->flip = v == "true";
+            }
+            else
+            {
+                // texture statements: options (-bm 1.0 ...) first, the file name last
+                static const std::pair<const char*, int> maps[] = {{"map_Kd", GPT_TEX_COLOR}, {"map_Ks", GPT_TEX_SPECULAR},
+                                                                   {"map_Ns", GPT_TEX_SHININESS}, {"map_RMA", GPT_TEX_RMA},
+                                                                   {"map_Ke", GPT_TEX_EMISSION}, {"norm", GPT_TEX_NORMAL},
+                                                                   {"map_Bump", -1}, {"bump", -1}};
+                for (const auto& [name, slot] : maps)
+                {
+                    if (key != name) continue;
+                    std::string tok, last;
+                    while (ss >> tok) last = tok;
+                    if (slot >= 0) cur->maps[slot] = last;
+                    else cur->bump = last;
+                }
             }
         }
         return true;
@@ -364,6 +400,74 @@ extern "C"
             scene->materialNames.push_back(defaultMaterial.name);
         }
         if (scene->materialIds.empty()) return GPT_ERR_INVALID_ARGUMENT;
+        // texture maps: one texture per (file, colour space, flip), shared by the materials naming it
+        bool anyMap = false;
+        for (const MtlEntry& e : mtl)
+            for (int k = 0; k < GPT_TEX_SLOTS; k++) anyMap = anyMap || !e.maps[k].empty() || !e.bump.empty();
+        if (anyMap)
+        {
+            scene->materialTextures.assign(scene->materials.size() * GPT_TEX_SLOTS, -1);
+            std::map<std::string, int32_t> loaded;
+            for (size_t m = 0; m < mtl.size(); m++)
+                for (int k = 0; k < GPT_TEX_SLOTS; k++)
+                {
+                    std::string file = mtl[m].maps[k];
+                    if (k == GPT_TEX_NORMAL && file.empty()) file = mtl[m].bump;
+                    if (file.empty()) continue;
+                    const bool srgb = k == GPT_TEX_COLOR || k == GPT_TEX_SPECULAR;
+                    const bool scalar = k == GPT_TEX_SHININESS;
+                    std::filesystem::path full = mtl[m].dir / file;
+                    if (!std::filesystem::exists(full)) full = file;
+                    const std::string key = full.string() + (srgb ? "|s" : "|l") + (scalar ? "|1" : "|n") + (mtl[m].flip ? "|f" : "|u");
+                    auto it = loaded.find(key);
+                    if (it == loaded.end())
+                    {
+                        pt::Image8 img;
+                        std::string err;
+                        if (!pt::LoadImage8(full.string(), img, err))
+                        {
+                            scene->error = err;
+                            std::fprintf(stderr, "gpt_obj_load: %s\n", err.c_str());
+                            return GPT_ERR_INVALID_ARGUMENT;
+                        }
+                        uint32_t ch = img.channels;
+                        std::vector<uint8_t> data;
+                        if (scalar && ch != 1)
+                        {
+                            // one-channel slot: the first channel (ChannelLayout::R)
+                            data.resize(static_cast<size_t>(img.width) * img.height);
+                            for (size_t i = 0; i < data.size(); i++) data[i] = img.pixels[i * ch];
+                            ch = 1;
+                        }
+                        else if (!scalar && ch == 1)
+                        {
+                            // grey map in a colour slot: replicated to RGB
+                            data.resize(static_cast<size_t>(img.width) * img.height * 3);
+                            for (size_t i = 0; i < img.pixels.size(); i++) data[i * 3] = data[i * 3 + 1] = data[i * 3 + 2] = img.pixels[i];
+                            ch = 3;
+                        }
+                        else
+                            data = std::move(img.pixels);
+                        if (mtl[m].flip)
+                        {
+                            const size_t row = static_cast<size_t>(img.width) * ch;
+                            for (uint32_t y = 0; y < img.height / 2; y++)
+                                std::swap_ranges(data.begin() + static_cast<long>(y * row), data.begin() + static_cast<long>((y + 1) * row),
+                                                 data.begin() + static_cast<long>((img.height - 1 - y) * row));
+                        }
+                        scene->textureData.push_back(std::move(data));
+                        gpt_texture_desc t{};
+                        t.width = img.width;
+                        t.height = img.height;
+                        t.channels = ch;
+                        t.format = srgb ? GPT_TEXEL_U8_SRGB : GPT_TEXEL_U8_LINEAR;
+                        scene->textures.push_back(t);
+                        it = loaded.emplace(key, static_cast<int32_t>(scene->textures.size() - 1)).first;
+                    }
+                    scene->materialTextures[m * GPT_TEX_SLOTS + k] = it->second;
+                }
+            for (size_t i = 0; i < scene->textures.size(); i++) scene->textures[i].data = scene->textureData[i].data();
+        }
         *out = scene.release();
         return GPT_OK;
     }
@@ -379,6 +483,9 @@ extern "C"
         desc->material_ids = s->materialIds.data();
         desc->material_count = static_cast<uint32_t>(s->materials.size());
         desc->materials = s->materials.data();
+        desc->texture_count = static_cast<uint32_t>(s->textures.size());
+        desc->textures = s->textures.empty() ? nullptr : s->textures.data();
+        desc->material_textures = s->textures.empty() ? nullptr : s->materialTextures.data();
         return GPT_OK;
     }
 

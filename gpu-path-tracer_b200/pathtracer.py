@@ -547,7 +547,8 @@ def build_alias_table_noalloc(weights_dev, bins_dev, stream=None, variant: str =
 
 
 def load_obj(path: str, transform=None):
-    """OBJ/MTL file -> scenes.Scene (world-space triangles, constant materials encoded as texels)."""
+    """OBJ/MTL file -> scenes.Scene (world-space triangles, materials encoded as texels, texture maps
+    decoded into scene.textures / scene.material_textures)."""
     import scenes
     L = lib()
     h = ctypes.c_void_p()
@@ -578,6 +579,14 @@ def load_obj(path: str, transform=None):
             names.append(buf.value.decode())
         s = scenes.Scene(pos, nrm, tan, uv, mid, mats, name=os.path.basename(path)).contiguous()
         s.material_names = names
+        if d.texture_count:
+            descs = ctypes.cast(d.textures, ctypes.POINTER(gpt_texture_desc))
+            for i in range(d.texture_count):
+                t = descs[i]
+                count = t.width * t.height * t.channels
+                data = np.ctypeslib.as_array(ctypes.cast(t.data, ctypes.POINTER(ctypes.c_uint8)), shape=(count,)).copy()
+                s.textures.append(dict(data=data.reshape(t.height, t.width, t.channels), format=int(t.format)))
+            s.material_textures = arr(d.material_textures, m * 6, ctypes.c_int32).reshape(m, 6)
         return s
     finally:
         L.gpt_obj_free(h)
