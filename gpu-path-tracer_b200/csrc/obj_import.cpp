@@ -5,10 +5,8 @@
 //     per material id (ascending, faces without a material first), vertex normals and uvs
 //     required, normals normalised, MTL keys Kd Ks Ns Pr Pm Ke Ni Tf d and the extension keys
 //     `surface` (unlit normal diffuse lambert mirror phong microfacet ggx emissive) and `flip_textures`;
-//   GenerateTangentSpace (Core/Source/Utils/Math/TangentSpace.cpp): per-vertex tangents with a
-//     handedness sign. MikkTSpace is not available here; tangents are accumulated from each
-//     triangle's uv derivatives and Gram-Schmidt orthogonalised (Lengyel's method), which agrees
-//     with MikkTSpace on planar and smoothly parameterised meshes;
+//   GenerateTangentSpace (Core/Source/Utils/Math/TangentSpace.cpp:66-89): per-vertex tangents with a
+//     handedness sign by Mikkelsen's method, per submesh (tangent_space.cpp, gpt_generate_tangents);
 //   Manager::ImportMaterial (Core/Source/Assets/Manager.cpp:311-412): constants become the texels of
 //     1x1 textures (sRGB u8 colour and specular, linear u8 shininess (Ns-1)/999, float emission,
 //     default normal texel); like the reference, the RMA texel is the default (255, 0, 255) when no
@@ -192,11 +190,13 @@ namespace
         return -1;
     }
 
+    // glm::normalize: v * (1 / sqrt(dot(v, v)))
     V3 normalize3(V3 v)
     {
-        float l = std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z);
-        if (l > 0.0f) return {v.x / l, v.y / l, v.z / l};
-        return v;
+        const float d = v.x * v.x + v.y * v.y + v.z * v.z;
+        if (!(d > 0.0f)) return v;
+        const float inv = 1.0f / std::sqrt(d);
+        return {v.x * inv, v.y * inv, v.z * inv};
     }
 }
 
@@ -328,26 +328,21 @@ extern "C"
                     }
                     tris.push_back(t);
                 }
-                std::vector<V3> tanAcc(verts.size(), V3{0, 0, 0}), bitAcc(verts.size(), V3{0, 0, 0});
-                for (const auto& t : tris)
+                // MikkTSpace tangents of the submesh in object space (the loader's normalised normals)
+                std::vector<float> vp(verts.size() * 3), vn(verts.size() * 3), vt(verts.size() * 2), vtan(verts.size() * 4);
+                for (size_t k = 0; k < verts.size(); k++)
                 {
-                    const V3 p0 = pos[verts[t[0]].v], p1 = pos[verts[t[1]].v], p2 = pos[verts[t[2]].v];
-                    const auto& w0 = tex[verts[t[0]].t];
-                    const auto& w1 = tex[verts[t[1]].t];
-                    const auto& w2 = tex[verts[t[2]].t];
-                    const V3 e1{p1.x - p0.x, p1.y - p0.y, p1.z - p0.z}, e2{p2.x - p0.x, p2.y - p0.y, p2.z - p0.z};
-                    const float du1 = w1[0] - w0[0], dv1 = w1[1] - w0[1], du2 = w2[0] - w0[0], dv2 = w2[1] - w0[1];
-                    const float den = du1 * dv2 - du2 * dv1;
-                    if (std::fabs(den) < 1e-20f) continue;
-                    const float r = 1.0f / den;
-                    const V3 sdir{(dv2 * e1.x - dv1 * e2.x) * r, (dv2 * e1.y - dv1 * e2.y) * r, (dv2 * e1.z - dv1 * e2.z) * r};
-                    const V3 tdir{(du1 * e2.x - du2 * e1.x) * r, (du1 * e2.y - du2 * e1.y) * r, (du1 * e2.z - du2 * e1.z) * r};
-                    for (int k = 0; k < 3; k++)
-                    {
-                        tanAcc[t[k]].x += sdir.x; tanAcc[t[k]].y += sdir.y; tanAcc[t[k]].z += sdir.z;
-                        bitAcc[t[k]].x += tdir.x; bitAcc[t[k]].y += tdir.y; bitAcc[t[k]].z += tdir.z;
-                    }
+                    const V3 p = pos[verts[k].v], n = normalize3(nrm[verts[k].n]);
+                    vp[3 * k] = p.x; vp[3 * k + 1] = p.y; vp[3 * k + 2] = p.z;
+                    vn[3 * k] = n.x; vn[3 * k + 1] = n.y; vn[3 * k + 2] = n.z;
+                    vt[2 * k] = tex[verts[k].t][0]; vt[2 * k + 1] = tex[verts[k].t][1];
                 }
+                std::vector<uint32_t> vi(tris.size() * 3);
+                for (size_t k = 0; k < tris.size(); k++)
+                    for (int c = 0; c < 3; c++) vi[3 * k + c] = tris[k][c];
+                const int trc = gpt_generate_tangents(vp.data(), vn.data(), vt.data(), static_cast<uint32_t>(verts.size()), vi.data(),
+                                                      static_cast<uint32_t>(tris.size()), vtan.data());
+                if (trc != GPT_OK) return trc;
                 const uint32_t material = matId >= 0 ? static_cast<uint32_t>(matId) : defaultIndex;
                 if (matId < 0) usesDefault = true;
                 for (const auto& t : tris)
@@ -358,13 +353,9 @@ extern "C"
                         const V3 wp = xformP(pos[vk.v]);
                         const V3 n = normalize3(nrm[vk.n]);
                         const V3 wn = normalize3(xformN(n));
-                        // object-space tangent: Gram-Schmidt against the normal, handedness from the bitangent
-                        V3 tg = tanAcc[t[k]];
-                        const float nd = n.x * tg.x + n.y * tg.y + n.z * tg.z;
-                        tg = V3{tg.x - n.x * nd, tg.y - n.y * nd, tg.z - n.z * nd};
-                        const V3 bt = bitAcc[t[k]];
-                        const V3 cr{n.y * tg.z - n.z * tg.y, n.z * tg.x - n.x * tg.z, n.x * tg.y - n.y * tg.x};
-                        const float sign = (cr.x * bt.x + cr.y * bt.y + cr.z * bt.z) < 0.0f ? -1.0f : 1.0f;
+                        const float* mt = &vtan[4 * static_cast<size_t>(t[k])];
+                        const V3 tg{mt[0], mt[1], mt[2]};
+                        const float sign = mt[3];
                         // ComputeWorldTangent (Renderer.cpp:116-142)
                         V3 wt = xformL(tg);
                         float l2 = wt.x * wt.x + wt.y * wt.y + wt.z * wt.z;

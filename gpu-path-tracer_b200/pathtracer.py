@@ -182,6 +182,8 @@ _SIGNATURES = [
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64),
                                       ctypes.POINTER(ctypes.c_uint64)]),
     ("gpt_build_alias_table_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]),
+    ("gpt_generate_tangents", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                             ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]),
     ("gpt_obj_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
     ("gpt_obj_scene_desc", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_scene_desc)]),
     ("gpt_obj_material_name", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t]),
@@ -544,6 +546,19 @@ def build_alias_table_noalloc(weights_dev, bins_dev, stream=None, variant: str =
     with torch.cuda.device(weights_dev.device):
         return lib(variant).gpt_build_alias_table_noalloc(ctypes.c_void_p(weights_dev.data_ptr()), n,
                                                           ctypes.c_void_p(bins_dev.data_ptr()), ctypes.c_void_p(stream))
+
+
+def generate_tangents(positions, normals, uvs, indices) -> np.ndarray:
+    """[V, 4] tangents (xyz, sign) of an indexed mesh by Mikkelsen's method (gpt_generate_tangents)."""
+    p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    n = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2)
+    i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+    out = np.zeros((p.shape[0], 4), dtype=np.float32)
+    rc = lib().gpt_generate_tangents(_ptr(p), _ptr(n), _ptr(t), p.shape[0], _ptr(i), i.shape[0], _ptr(out))
+    if rc != 0:
+        raise GptError(rc, "gpt_generate_tangents")
+    return out
 
 
 def load_obj(path: str, transform=None):

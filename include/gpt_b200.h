@@ -345,6 +345,16 @@ int gpt_bvh8_check(const gpt_scene_desc* scene, uint32_t* node_count, uint32_t* 
 int gpt_build_alias_table_noalloc(const float* weights, uint32_t light_count, uint32_t* bins, void* stream);
 
 /*
+ * Per-vertex tangents of an indexed triangle mesh by Mikkelsen's method, the tangent space the
+ * reference generates for imported meshes (GenerateTangentSpace, Core/Source/Utils/Math/TangentSpace.cpp:
+ * 66-89, MikkTSpace with its default 180-degree threshold): positions [V][3], normals [V][3] (unit),
+ * uvs [V][2], indices [T][3]; tangents [V][4] = unit tangent xyz and handedness sign (+1 where the uv
+ * mapping preserves orientation). A vertex takes the frame of the last triangle corner naming it.
+ */
+int gpt_generate_tangents(const float* positions, const float* normals, const float* uvs, uint32_t vertex_count,
+                          const uint32_t* indices, uint32_t triangle_count, float* tangents);
+
+/*
  * Headless OBJ/MTL ingest (the reference's LoadObj + GenerateTangentSpace + Manager::ImportMaterial +
  * BuildTriangles: Core/Source/Import/ObjLoader.cpp:67-234, Core/Source/Assets/Manager.cpp:311-412,
  * Renderer.cpp:116-213). Produces the arrays of a gpt_scene_desc: triangles grouped per shape and

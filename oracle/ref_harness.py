@@ -23,6 +23,33 @@ assert REF_MATERIAL_DTYPE.itemsize == 48
 IMAGE_DTYPE = np.dtype([("width", "<u4"), ("height", "<u4"), ("channels", "<u4"), ("format", "<u4"), ("data", "<u8")])
 
 
+LIB_PATH_MIKK = os.path.join(_HERE, "_ref", "libmikk_ref.so")
+
+
+def mikk_available() -> bool:
+    return os.path.exists(LIB_PATH_MIKK)
+
+
+def mikk_tangents(positions, normals, uvs, indices) -> np.ndarray:
+    """Per-vertex tangents [V, 4] from the reference's own MikkTSpace build (oracle/_ref/libmikk_ref.so)."""
+    if "mikk" not in _libs:
+        L = ctypes.CDLL(LIB_PATH_MIKK)
+        L.mikk_ref_tangents.restype = ctypes.c_int
+        L.mikk_ref_tangents.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int, ctypes.c_void_p]
+        _libs["mikk"] = L
+    p = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+    n = np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2)
+    i = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+    out = np.zeros((p.shape[0], 4), dtype=np.float32)
+    out[:, 0] = 1.0
+    out[:, 3] = -1.0
+    rc = _libs["mikk"].mikk_ref_tangents(_p(p), _p(n), _p(t), _p(i), i.shape[0], _p(out))
+    if rc:
+        raise RuntimeError("genTangSpaceDefault failed")
+    return out
+
+
 def available() -> bool:
     return os.path.exists(LIB_PATH) and os.path.exists(LIB_PATH_NOFMA)
 
