@@ -298,13 +298,16 @@ def _run_jobs_on_server(srv, ids, jobs, open_loop):
                 time.sleep(delay)
         jids.append(srv.submit(ids[j.scene], j.camera, j.width, j.height, j.spp, j.depth, True))
     lat = []
+    service = []
     for jid in jids:
         st = srv.wait(jid, 3600.0)
         if st["state"] != "done":
             raise RuntimeError(f"job {jid} ended as {st['state']}: {srv.last_error()}")
         srv.result(jid)
         lat.append(st["done_s"] - st["submit_s"])
+        service.append(st["done_s"] - st["admit_s"])
         srv.release(jid)
+    _run_jobs_on_server.service = service
     return time.perf_counter() - t0, lat
 
 
@@ -369,7 +372,7 @@ def batched_section(knobs):
     return out
 
 
-def serving_section(knobs, rates, n_jobs, max_pool):
+def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
     """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time.
     Both servers hold at most max_pool path slots: an iteration's time grows with the slots in flight,
     and a small job needs a fixed number of iterations, so its latency grows with the pool."""
@@ -385,8 +388,9 @@ def serving_section(knobs, rates, n_jobs, max_pool):
     warm = [workloads.Job(n, 64, 64, 4, 8, scenes.scene_camera(s, 64, 64)) for n, s in resident.items()]
     pool = min(knobs["pool_size"], max_pool)
     out["pool_size"] = pool
-    for mode, active in (("served", 0), ("plain", 1)):
-        srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30,
+    latencies, alone = {}, {}
+    for mode, active, schedule in (("served", 0, schedule_served), ("plain", 1, 0)):
+        srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30, schedule=schedule,
                                 **_server_knobs(knobs))
         res = {}
         try:
@@ -398,15 +402,27 @@ def serving_section(knobs, rates, n_jobs, max_pool):
                 wall, lat = _run_jobs_on_server(srv, ids, jobs, True)
                 st = srv.stats()
                 paths = sum(j.paths for j in jobs)
+                latencies[(mode, rate)] = lat
+                if mode == "plain":  # one job at a time: admission to completion is the job's time alone
+                    alone[rate] = list(_run_jobs_on_server.service)
                 res[f"{rate:g}_jobs_per_s"] = {
                     "p50_latency_s": workloads.percentile(lat, 50), "p99_latency_s": workloads.percentile(lat, 99),
                     "mean_latency_s": sum(lat) / len(lat), "paths_per_second": paths / wall, "wall_s": wall,
                     "device_paths_per_second": paths / ((st["device_ms"] - before["device_ms"]) / 1000.0),
-                    "offered_paths_per_second": paths / jobs[-1].arrival_s}
+                    "device_busy_fraction": (st["device_ms"] - before["device_ms"]) / 1000.0 / wall,
+                    "offered_paths_per_second": paths / jobs[-1].arrival_s,
+                    "slices": st["slices"] - before["slices"], "iterations": st["iterations"] - before["iterations"]}
             res["admitted_high_water_bytes"] = srv.stats()["admitted_high_water"]
         finally:
             srv.close()
         out[mode] = res
+    # per-job slowdown: latency over the job's own render time alone (one-at-a-time server, admission
+    # to completion)
+    for rate in rates:
+        for mode in ("served", "plain"):
+            sd = sorted(l / max(a, 1e-6) for l, a in zip(latencies[(mode, rate)], alone[rate]))
+            out[mode][f"{rate:g}_jobs_per_s"]["p50_slowdown"] = workloads.percentile(sd, 50)
+            out[mode][f"{rate:g}_jobs_per_s"]["p99_slowdown"] = workloads.percentile(sd, 99)
     return out
 
 

@@ -1,16 +1,19 @@
-"""Pin of the oracle against the reference itself: the reference's own kernel sources
-(Intersect.cu, PathGeneration.cu, MaterialEval.cu, Iteration.cu, HostBvh.cpp) compiled for
-sm_100a into oracle/_ref/ and driven through their launchers (oracle/ref_harness).
+"""The product against the reference itself: the reference's own kernel sources (Intersect.cu,
+PathGeneration.cu, MaterialEval.cu, Iteration.cu, HostBvh.cpp) compiled for sm_100a into
+oracle/_ref/ and driven through their launchers (oracle/ref_harness), GPU against GPU.
 
-Two builds of the reference sources are used:
-  * -fmad=false: the same operator-by-operator rounding the oracle restates. Closest-hit
-    triangle ids and (u, v, t) must then be bit-identical to the oracle, except that at an
-    exact tie (two triangles at the same t) the reference keeps the first one its DFS visits.
-  * the reference's own flags (FMA contraction on) with CUDA's sinf/cosf/powf/rsqrtf: the
-    oracle fixes deterministic IEEE definitions of those, so agreement is statistical and the
-    bounds are stated below.
-The materials handed to the oracle are the texel values the reference's own sRGB textures
-return on the device (hardware decode), read back from the reference harness.
+* The product build (libgpt_b200.so) computes as the reference's build does (multiply-add
+  contraction, CUDA's sinf/cosf/powf/rsqrtf), so against the reference built with its own flags:
+  hit triangle ids and (u, v, t) bit-exact on 2^20 rays except at exact ties (two triangles at the
+  bit-identical t: the reference keeps the first its DFS visits, the product the smaller input
+  index; such rays are counted), per-iteration queue counts bit-exact, and every path's radiance
+  within 1e-4 relative at spp = 1.
+* The oracle's pin: against the reference built with -fmad=false (the oracle's operator-by-operator
+  rounding) the oracle's hits are bit-exact except exact ties; its deterministic transcendentals
+  differ from CUDA's in the last bits, so its frames agree with the reference's statistically, with
+  the bounds stated below.
+The materials handed to the product and the oracle are the texel values the reference's own sRGB
+textures return on the device (hardware decode), read back from the reference harness.
 """
 import numpy as np
 import pytest
@@ -40,6 +43,46 @@ def pair(name, fma):
         decoded = with_materials(s, R.decoded_materials())
         _cache[key] = (s, R, decoded, oracle.OracleScene(decoded))
     return _cache[key]
+
+
+def hits_against_reference(tg, ug, tr, ur):
+    """Counts of (id mismatches at an exact tie, other mismatches, (u, v, t) bit mismatches on equal ids)."""
+    diff = tg != tr
+    tie = diff & (tg != INVALID) & (tr != INVALID) & (ug[:, 2].view(np.uint32) == ur[:, 2].view(np.uint32))
+    same_hit = ~diff & (tr != INVALID)
+    uvt = same_hit & np.any(ug.view(np.uint32) != ur.view(np.uint32), axis=1)
+    return int(tie.sum()), int((diff & ~tie).sum()), int(uvt.sum())
+
+
+@pytest.mark.parametrize("name", ["cornell", "cornell-all", "spheres-small", "spheres-200k"])
+def test_product_hits_bit_exact_against_reference_build(gpu_renderer_product, name):
+    s, R, decoded, _ = pair(name, True)
+    gpu_renderer_product.upload_scene(decoded)
+    rays = scenes.hit_ray_set(s, 1 << 20, seed=11)
+    tr, ur = R.trace_closest(rays)
+    tg, ug = gpu_renderer_product.trace_closest_np(rays)
+    ties, other, uvt = hits_against_reference(tg, ug, tr, ur)
+    assert other == 0 and uvt == 0, (ties, other, uvt)
+    assert ties <= 1e-3 * rays.shape[0]
+
+
+@pytest.mark.parametrize("name,w,h", [("cornell-all", 256, 256), ("spheres-small", 192, 128)])
+@pytest.mark.parametrize("nee", [False, True])
+def test_product_frames_against_reference_build(gpu_renderer_product, name, w, h, nee):
+    """spp = 1 (one path per pixel, so the reference's float-atomic pixel sum is that path's
+    radiance): identical per-iteration queue counts and every path within 1e-4 relative."""
+    s, R, decoded, _ = pair(name, True)
+    r = gpu_renderer_product
+    r.upload_scene(decoded)
+    cam = scenes.scene_camera(s, w, h)
+    rr = R.render(cam, w, h, 1, 10, nee)
+    st = r.render_frame(cam, w, h, 1, 10, nee, pool_size=1 << 20)
+    assert st["iterations"] == rr["iterations"]
+    assert np.array_equal(r.queue_log(), rr["queue_log"][:len(r.queue_log())])
+    a = r.sample_radiance().astype(np.float64)
+    b = rr["accumulation"][:, :3].astype(np.float64)
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+    assert np.all(rel <= 1e-4), (int(np.sum(np.any(rel > 1e-4, axis=1))), float(rel.max()))
 
 
 def test_reference_texture_decode_is_close_to_the_srgb_formula():
