@@ -386,9 +386,15 @@ namespace pt
             J.id = nextId_++;
             J.tSubmit = seconds_since(t0_);
             id = J.id;
+            // End the running slice only when the new job can be admitted now: jobs are admitted in
+            // submission order, so behind a waiting job, or with the budget, the job table or the
+            // active-job limit full, a new slice could not start it (a completing job ends the slice and
+            // admits waiting jobs anyway). Under overload this keeps arrivals from cutting slices short.
+            const bool admittable = pending_.empty() && admitted_ + J.admittedBytes <= cfg_.hbm_budget_bytes && !freeTable_.empty() &&
+                                    (cfg_.max_active_jobs == 0 || active_.size() + toCopy_.size() < cfg_.max_active_jobs);
             records_.emplace(J.id, std::move(J));
             pending_.push_back(id);
-            *static_cast<volatile uint32_t*>(hostMapped_) = 1u;  // end the running slice: a job is waiting
+            if (admittable) *static_cast<volatile uint32_t*>(hostMapped_) = 1u;
             cv_.notify_all();
             return Status::Ok();
         }
