@@ -31,6 +31,7 @@
 #include <future>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 namespace pt
 {
@@ -75,6 +76,44 @@ namespace pt
         constexpr int kBins = 32;
         constexpr uint32_t kMaxLeaf = 1;
         constexpr float kTraversalCost = 1.2f;
+        // Nodes of at least this many triangles compute their bounds, bins and partition on several
+        // threads, in fixed chunks of kChunk triangles (the tree does not depend on the thread count).
+        // Near the root the SAH peels off one cluster of triangles at a time, so a serial build spends
+        // most of its time in a chain of large nodes that no subtree-level parallelism shortens.
+        constexpr uint32_t kParallelNode = 1u << 18;
+        constexpr uint32_t kChunk = 1u << 16;
+
+        // f(c) for every chunk c in [0, chunks), on at most `threads` threads
+        template <class F>
+        void for_chunks(uint32_t chunks, int threads, F&& f)
+        {
+            std::atomic<uint32_t> next{0};
+            auto worker = [&]
+            {
+                for (uint32_t c; (c = next.fetch_add(1)) < chunks;) f(c);
+            };
+            const int t = static_cast<int>(std::min<uint32_t>(static_cast<uint32_t>(std::max(threads, 1)), chunks));
+            std::vector<std::thread> pool;
+            for (int i = 1; i < t; i++) pool.emplace_back(worker);
+            worker();
+            for (auto& th : pool) th.join();
+        }
+
+        // Bins of one range of triangles along all three axes.
+        struct Bins
+        {
+            uint32_t cnt[3][kBins] = {};
+            Box box[3][kBins];
+            void merge(const Bins& o)
+            {
+                for (int k = 0; k < 3; k++)
+                    for (int b = 0; b < kBins; b++)
+                    {
+                        cnt[k][b] += o.cnt[k][b];
+                        box[k][b].grow(o.box[k][b]);
+                    }
+            }
+        };
 
         struct BinaryBuilder
         {
@@ -95,16 +134,58 @@ namespace pt
                 return i;
             }
 
+            int bin_of(uint32_t t, int k, float lo, float scale) const
+            {
+                const int b = static_cast<int>((cent[static_cast<size_t>(t) * 3 + k] - lo) * scale);
+                return std::min(std::max(b, 0), kBins - 1);
+            }
+
+            void bin_range(uint32_t begin, uint32_t end, const Box& cbox, const float scale[3], Bins& out) const
+            {
+                for (uint32_t i = begin; i < end; i++)
+                {
+                    const uint32_t t = idx[i];
+                    for (int k = 0; k < 3; k++)
+                    {
+                        if (!(scale[k] > 0.0f)) continue;
+                        const int b = bin_of(t, k, cbox.lo[k], scale[k]);
+                        out.cnt[k][b]++;
+                        out.box[k][b].grow(triBox[t]);
+                    }
+                }
+            }
+
             uint32_t build(uint32_t first, uint32_t count, int depth)
             {
                 const uint32_t me = alloc();
+                const bool parallel = count >= kParallelNode && maxThreads > 1;
+                const uint32_t chunks = (count + kChunk - 1) / kChunk;
                 Box box, cbox;
-                for (uint32_t i = first; i < first + count; i++)
+                if (parallel)
                 {
-                    const uint32_t t = idx[i];
-                    box.grow(triBox[t]);
-                    cbox.grow(&cent[static_cast<size_t>(t) * 3]);
+                    std::vector<Box> boxes(chunks), cboxes(chunks);
+                    for_chunks(chunks, maxThreads, [&](uint32_t c)
+                    {
+                        const uint32_t b = first + c * kChunk, e = std::min(first + count, b + kChunk);
+                        for (uint32_t i = b; i < e; i++)
+                        {
+                            boxes[c].grow(triBox[idx[i]]);
+                            cboxes[c].grow(&cent[static_cast<size_t>(idx[i]) * 3]);
+                        }
+                    });
+                    for (uint32_t c = 0; c < chunks; c++)
+                    {
+                        box.grow(boxes[c]);
+                        cbox.grow(cboxes[c]);
+                    }
                 }
+                else
+                    for (uint32_t i = first; i < first + count; i++)
+                    {
+                        const uint32_t t = idx[i];
+                        box.grow(triBox[t]);
+                        cbox.grow(&cent[static_cast<size_t>(t) * 3]);
+                    }
                 BNode node;
                 node.box = box;
                 node.first = first;
@@ -114,25 +195,34 @@ namespace pt
                     nodes[me] = node;
                     return me;
                 }
-                // binned SAH over the three axes
+                // binned SAH over the three axes, one pass over the triangles for all three
                 float bestCost = FLT_MAX;
                 int bestAxis = -1, bestBin = -1;
                 const float parentArea = std::max(box.area(), 1e-30f);
+                float scales[3];
                 for (int k = 0; k < 3; k++)
                 {
                     const float ext = cbox.hi[k] - cbox.lo[k];
-                    if (!(ext > 0.0f)) continue;
-                    uint32_t cnt[kBins] = {};
-                    Box bb[kBins];
-                    const float scale = kBins / ext;
-                    for (uint32_t i = first; i < first + count; i++)
+                    scales[k] = ext > 0.0f ? kBins / ext : 0.0f;
+                }
+                Bins bins;
+                if (parallel)
+                {
+                    std::vector<Bins> part(chunks);
+                    for_chunks(chunks, maxThreads, [&](uint32_t c)
                     {
-                        const uint32_t t = idx[i];
-                        int b = static_cast<int>((cent[static_cast<size_t>(t) * 3 + k] - cbox.lo[k]) * scale);
-                        b = std::min(std::max(b, 0), kBins - 1);
-                        cnt[b]++;
-                        bb[b].grow(triBox[t]);
-                    }
+                        const uint32_t b = first + c * kChunk, e = std::min(first + count, b + kChunk);
+                        bin_range(b, e, cbox, scales, part[c]);
+                    });
+                    for (uint32_t c = 0; c < chunks; c++) bins.merge(part[c]);
+                }
+                else
+                    bin_range(first, first + count, cbox, scales, bins);
+                for (int k = 0; k < 3; k++)
+                {
+                    if (!(scales[k] > 0.0f)) continue;
+                    const uint32_t* cnt = bins.cnt[k];
+                    const Box* bb = bins.box[k];
                     float areaL[kBins], areaR[kBins];
                     uint32_t cntL[kBins], cntR[kBins];
                     Box acc;
@@ -183,22 +273,61 @@ namespace pt
                 else
                 {
                     const float lo = cbox.lo[bestAxis];
-                    const float scale = kBins / (cbox.hi[bestAxis] - lo);
-                    auto it = std::partition(idx.begin() + first, idx.begin() + first + count, [&](uint32_t t)
+                    const float scale = scales[bestAxis];
+                    auto left = [&](uint32_t t) { return bin_of(t, bestAxis, lo, scale) <= bestBin; };
+                    if (parallel)
                     {
-                        int b = static_cast<int>((cent[static_cast<size_t>(t) * 3 + bestAxis] - lo) * scale);
-                        b = std::min(std::max(b, 0), kBins - 1);
-                        return b <= bestBin;
-                    });
-                    mid = static_cast<uint32_t>(it - idx.begin());
+                        // stable partition by chunks: left entries of every chunk in order, then the right ones
+                        std::vector<uint32_t> nLeft(chunks + 1, 0);
+                        for_chunks(chunks, maxThreads, [&](uint32_t c)
+                        {
+                            const uint32_t b = first + c * kChunk, e = std::min(first + count, b + kChunk);
+                            uint32_t n = 0;
+                            for (uint32_t i = b; i < e; i++) n += left(idx[i]) ? 1u : 0u;
+                            nLeft[c + 1] = n;
+                        });
+                        for (uint32_t c = 0; c < chunks; c++) nLeft[c + 1] += nLeft[c];
+                        const uint32_t totalLeft = nLeft[chunks];
+                        std::vector<uint32_t> tmp(count);
+                        for_chunks(chunks, maxThreads, [&](uint32_t c)
+                        {
+                            const uint32_t b = first + c * kChunk, e = std::min(first + count, b + kChunk);
+                            uint32_t l = nLeft[c], r = totalLeft + (b - first) - nLeft[c];
+                            for (uint32_t i = b; i < e; i++)
+                            {
+                                const uint32_t t = idx[i];
+                                if (left(t)) tmp[l++] = t;
+                                else tmp[r++] = t;
+                            }
+                        });
+                        std::copy(tmp.begin(), tmp.end(), idx.begin() + first);
+                        mid = first + totalLeft;
+                    }
+                    else
+                    {
+                        auto it = std::partition(idx.begin() + first, idx.begin() + first + count, left);
+                        mid = static_cast<uint32_t>(it - idx.begin());
+                    }
                     if (mid == first || mid == first + count) mid = first + count / 2;
                 }
                 uint32_t l, r;
                 if (count > 65536 && spawned.fetch_add(1) < maxThreads)
                 {
-                    auto fut = std::async(std::launch::async, [&, first, mid, depth]() { return build(first, mid - first, depth + 1); });
+                    // a subtree on its own thread; the slot is given back when it is done
+                    auto fut = std::async(std::launch::async, [&, first, mid, depth]()
+                    {
+                        const uint32_t res = build(first, mid - first, depth + 1);
+                        spawned.fetch_sub(1);
+                        return res;
+                    });
                     r = build(mid, first + count - mid, depth + 1);
                     l = fut.get();
+                }
+                else if (count > 65536)
+                {
+                    spawned.fetch_sub(1);
+                    l = build(first, mid - first, depth + 1);
+                    r = build(mid, first + count - mid, depth + 1);
                 }
                 else
                 {
@@ -222,6 +351,27 @@ namespace pt
             std::vector<float> cost;     // [node * 8 + i - 1]: least cost of the subtree in at most i slots
             std::vector<uint8_t> how;    // i == 1: 0 leaf, 1 wide node; i > 1: 0 = as in i - 1 slots, k = k slots to the left child
             std::vector<uint8_t> split;  // slots of the left child in the node's own wide node
+            std::vector<uint32_t> wide;  // wide nodes of the subtree of a binary node that becomes a wide node
+            int maxThreads = 1;
+            std::atomic<int> spawned{0};
+
+            // a subtree on another thread while one is free (large subtrees only)
+            template <class F>
+            bool spawn_if_free(uint32_t triangles, F&& f, std::future<void>& fut)
+            {
+                if (triangles < kParallelNode) return false;
+                if (spawned.fetch_add(1) >= maxThreads)
+                {
+                    spawned.fetch_sub(1);
+                    return false;
+                }
+                fut = std::async(std::launch::async, [this, f]()
+                {
+                    f();
+                    spawned.fetch_sub(1);
+                });
+                return true;
+            }
 
             void plan(uint32_t n)
             {
@@ -238,8 +388,12 @@ namespace pt
                     }
                     return;
                 }
-                plan(b.left);
+                std::future<void> fut;
+                const uint32_t left = b.left;
+                const bool async = spawn_if_free(bin.nodes[left].count, [this, left] { plan(left); }, fut);
+                if (!async) plan(b.left);
                 plan(b.right);
+                if (async) fut.get();
                 const float* L = &cost[static_cast<size_t>(b.left) * 8];
                 const float* R = &cost[static_cast<size_t>(b.right) * 8];
                 float D[9];
@@ -296,14 +450,56 @@ namespace pt
                 collect(b.left, h, kids, leaf);
                 collect(b.right, i - h, kids, leaf);
             }
+
+            // The child list of the wide node a binary node becomes.
+            void children(uint32_t n, std::vector<uint32_t>& kids, std::vector<uint8_t>& leaf) const
+            {
+                kids.clear();
+                leaf.clear();
+                const BNode& b = bin.nodes[n];
+                if (b.leaf())
+                {
+                    kids.push_back(n);
+                    leaf.push_back(1);
+                    return;
+                }
+                collect(b.left, split[n], kids, leaf);
+                collect(b.right, 8 - split[n], kids, leaf);
+            }
+
+            // wide[n] for binary node n and every wide node below it; returns it
+            uint32_t count_wide(uint32_t n)
+            {
+                std::vector<uint32_t> kids;
+                std::vector<uint8_t> leaf;
+                children(n, kids, leaf);
+                uint32_t total = 1;
+                std::vector<std::future<void>> futs;
+                for (size_t i = 0; i < kids.size(); i++)
+                {
+                    if (leaf[i]) continue;
+                    const uint32_t k = kids[i];
+                    std::future<void> fut;
+                    if (spawn_if_free(bin.nodes[k].count, [this, k] { count_wide(k); }, fut)) futs.push_back(std::move(fut));
+                    else count_wide(k);
+                }
+                for (auto& f : futs) f.get();
+                for (size_t i = 0; i < kids.size(); i++)
+                    if (!leaf[i]) total += wide[kids[i]];
+                wide[n] = total;
+                return total;
+            }
         };
 
+        // Wide nodes in depth-first pre-order (a node, then the subtrees of its inner children in slot
+        // assignment order). Every subtree's place is known from the plan's node counts, so large
+        // subtrees are written by other threads into their own ranges of the preallocated array.
         struct WideBuilder
         {
             const BinaryBuilder& bin;
-            const CollapsePlan& plan;
+            CollapsePlan& plan;
             std::vector<Node8> out;
-            uint32_t maxDepth = 0;
+            std::atomic<uint32_t> maxDepth{0};
 
             static void padBox(const Box& in, double lo[3], double hi[3])
             {
@@ -321,26 +517,14 @@ namespace pt
                 }
             }
 
-            uint32_t emit(uint32_t bnode, uint32_t depth)
+            void emit(uint32_t bnode, uint32_t depth, uint32_t me)
             {
-                maxDepth = std::max(maxDepth, depth + 1);
-                const uint32_t me = static_cast<uint32_t>(out.size());
-                out.push_back(Node8{});
+                uint32_t seen = maxDepth.load();
+                while (seen < depth + 1 && !maxDepth.compare_exchange_weak(seen, depth + 1)) {}
                 // children list
                 std::vector<uint32_t> kids;
                 std::vector<uint8_t> kidLeaf;
-                const BNode& root = bin.nodes[bnode];
-                if (root.leaf())
-                {
-                    kids.push_back(bnode);
-                    kidLeaf.push_back(1);
-                }
-                else
-                {
-                    const int k = plan.split[bnode];
-                    plan.collect(root.left, k, kids, kidLeaf);
-                    plan.collect(root.right, 8 - k, kids, kidLeaf);
-                }
+                plan.children(bnode, kids, kidLeaf);
                 // slot assignment by octant
                 Box nodeBox;
                 for (uint32_t k : kids) nodeBox.grow(bin.nodes[k].box);
@@ -375,10 +559,12 @@ namespace pt
                     slotUsed[bs] = true;
                     slotOf[bk] = bs;
                 }
-                // child references (recursion first: indices of internal children)
+                // child references: inner children's subtrees follow this node in the order of the children list
                 uint32_t childRef[8] = {0, 0, 0, 0, 0, 0, 0, 0};
                 uint8_t counts[8] = {};
                 uint8_t innerMask = 0, leafMask = 0;
+                uint32_t next = me + 1;
+                std::vector<std::future<void>> futs;
                 for (size_t i = 0; i < kids.size(); i++)
                 {
                     const BNode& c = bin.nodes[kids[i]];
@@ -392,10 +578,16 @@ namespace pt
                     }
                     else
                     {
-                        childRef[s] = emit(kids[i], depth + 1);
+                        const uint32_t at = next, k = kids[i];
+                        next += plan.wide[k];
+                        childRef[s] = at;
                         innerMask |= static_cast<uint8_t>(1u << s);
+                        std::future<void> fut;
+                        if (plan.spawn_if_free(c.count, [this, k, depth, at] { emit(k, depth + 1, at); }, fut)) futs.push_back(std::move(fut));
+                        else emit(k, depth + 1, at);
                     }
                 }
+                for (auto& f : futs) f.get();
                 // quantisation
                 double clo[8][3], chi[8][3];
                 bool valid[8] = {};
@@ -486,7 +678,6 @@ namespace pt
                 node.w[6] = make_uint4(a0, a1, leafMask, 0);
                 node.w[7] = make_uint4(0, 0, 0, 0);
                 out[me] = node;
-                return me;
             }
         };
 
@@ -582,30 +773,35 @@ namespace pt
         b.maxThreads = std::max(1, threads);
         b.triBox.resize(n);
         b.cent.resize(static_cast<size_t>(n) * 3);
-        for (uint32_t t = 0; t < n; t++)
+        for_chunks((n + kChunk - 1) / kChunk, b.maxThreads, [&](uint32_t c)
         {
-            Box box;
-            for (int k = 0; k < 3; k++) box.grow(positions + (static_cast<size_t>(t) * 3 + k) * 3);
-            b.triBox[t] = box;
-            for (int a = 0; a < 3; a++) b.cent[static_cast<size_t>(t) * 3 + a] = 0.5f * (box.lo[a] + box.hi[a]);
-        }
+            for (uint32_t t = c * kChunk; t < std::min(n, (c + 1) * kChunk); t++)
+            {
+                Box box;
+                for (int k = 0; k < 3; k++) box.grow(positions + (static_cast<size_t>(t) * 3 + k) * 3);
+                b.triBox[t] = box;
+                for (int a = 0; a < 3; a++) b.cent[static_cast<size_t>(t) * 3 + a] = 0.5f * (box.lo[a] + box.hi[a]);
+            }
+        });
         b.idx.resize(n);
         std::iota(b.idx.begin(), b.idx.end(), 0u);
         b.nodes.resize(static_cast<size_t>(n) * 2);
         const uint32_t root = b.build(0, n, 0);
         if (root != 0) throw std::runtime_error("BVH root index");
-        CollapsePlan plan{b, {}, {}, {}};
+        CollapsePlan plan{b, {}, {}, {}, {}};
+        plan.maxThreads = b.maxThreads;
         const size_t binaryNodes = b.nodeCount.load();
         plan.cost.assign(binaryNodes * 8, 0.0f);
         plan.how.assign(binaryNodes * 8, 0);
         plan.split.assign(binaryNodes, 1);
+        plan.wide.assign(binaryNodes, 0);
         plan.plan(root);
-        WideBuilder w{b, plan, {}, 0};
-        w.out.reserve(static_cast<size_t>(n) / 4 + 8);
-        w.emit(root, 0);
+        WideBuilder w{b, plan, {}};
+        w.out.resize(plan.count_wide(root));
+        w.emit(root, 0, 0);
         Bvh8 result;
         result.nodes = std::move(w.out);
-        result.depth = w.maxDepth;
+        result.depth = w.maxDepth.load();
         if (withBinary)
         {
             BinaryFlattener f{b, {}, 0};
