@@ -312,6 +312,7 @@ namespace pt
         SceneView sc;
         Wavefront wf;
         const SceneEntry* scenes;  // nullptr: one scene rooted at node 0
+        int stackCap = 0;          // traversal stack entries a ray may use (0 = the kernel's whole stack)
         static constexpr int kPhase = 0;
         static constexpr bool kFixedTmin = true;   // every wavefront ray starts at kMinT
         __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
@@ -361,6 +362,7 @@ namespace pt
         SceneView sc;
         Wavefront wf;
         const SceneEntry* scenes;
+        int stackCap = 0;
         static constexpr int kPhase = 2;
         static constexpr bool kFixedTmin = true;
         __device__ uint32_t root(uint32_t tag) const { return scenes ? __ldg(&scenes[tag >> kSlotBits].root) : 0u; }
@@ -400,6 +402,7 @@ namespace pt
         float* uvtOut;
         uint8_t* occOut;
         uint32_t rootNode;
+        int stackCap = 0;
         static constexpr int kPhase = 0;
         static constexpr bool kFixedTmin = false;  // per-ray tMin of the caller's batch
         __device__ uint32_t root(uint32_t) const { return rootNode; }
@@ -457,6 +460,9 @@ namespace pt
         Counters* ctr = work.counters();
         phase_begin(ctr, Work::kPhase);
         const uint32_t n = work.count();
+        // entries a ray may push: the stack's capacity, or the caller's smaller bound (pushes beyond it
+        // are refused and reported as an overflow)
+        const int cap = (work.stackCap > 0 && work.stackCap < STACK) ? work.stackCap : STACK;
         uint32_t counts = 0;  // node visits | triangle tests << 16
         const uint32_t lane = lane_id();
         TraversalState st;
@@ -513,9 +519,9 @@ namespace pt
                 for (int k = 0; k < 4 && more; k++)
                 {
                     if constexpr (BINARY)
-                        more = traverse_step_binary<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, STACK, occluded, errorFlags, counts);
+                        more = traverse_step_binary<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, cap, occluded, errorFlags, counts);
                     else
-                        more = traverse_step<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, stride, STACK, occluded, errorFlags, counts);
+                        more = traverse_step<ANY, Work::kFixedTmin>(work.sc, st, cold, stack, stride, cap, occluded, errorFlags, counts);
                 }
                 if (!more)
                 {
@@ -2219,7 +2225,7 @@ namespace pt
     cudaError_t launch_iteration(const IterationLaunch& L, cudaStream_t s)
     {
         cudaError_t e;
-        WavefrontClosest wc{L.scene, L.wf, nullptr};
+        WavefrontClosest wc{L.scene, L.wf, nullptr, L.stackCap};
         const bool binary = L.bvhFormat == kBvh2Fp32;
         if (L.traceStart && (e = cudaEventRecord(L.traceStart, s)) != cudaSuccess) return e;
         if (binary)
@@ -2232,7 +2238,7 @@ namespace pt
             return e;
         if (L.nee && L.scene.lightCount > 0)
         {
-            WavefrontShadow ws{L.scene, L.wf, nullptr};
+            WavefrontShadow ws{L.scene, L.wf, nullptr, L.stackCap};
             if (binary)
                 e = launch_trace_binary<true>(ws, L.traceBlocks, L.traceThreads, L.refillShadow, &L.wf.ctr->errorFlags, s);
             else

@@ -24,6 +24,7 @@ namespace pt
         int sms;                   // multiprocessors: each shading grid is sms x that kernel's resident blocks per SM
         bool graphLoop;            // true: inside the frame graph's WHILE node; false: host-driven loop
         uint32_t bvhFormat;        // kBvh8Quantised or kBvh2Fp32 (scene.nodes2 must be present)
+        int stackCap;              // traversal stack entries a ray may use (0 = the whole stack)
         cudaEvent_t traceStart;    // optional events around the closest-hit traversal launch (host loop)
         cudaEvent_t traceStop;
         // Optional fork/join: the shading kernels of the models present run on their own streams,

@@ -454,17 +454,12 @@ namespace pt
             c.queues = s.wavefront_layout == GPT_WAVEFRONT_QUEUES;
             c.maxIterations = s.max_iterations;
             if (s.trace_stack > kMaxStack) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "trace_stack above 64 entries");
-            c.stack = s.trace_stack == 0 ? 0u : (s.trace_stack <= 8 ? 8u : (s.trace_stack <= 16 ? 16u : (s.trace_stack <= 32 ? 32u : 64u)));
+            c.stack = s.trace_stack;
             return Status::Ok();
         }
 
-        // The scene as the frame's kernels see it: the traversal stack variant follows view.depth.
-        SceneView frameView(const FrameConfig& c) const
-        {
-            SceneView v = scene_->view();
-            if (c.stack) v.depth = c.stack;
-            return v;
-        }
+        // The scene as the frame's kernels see it.
+        SceneView frameView(const FrameConfig&) const { return scene_->view(); }
 
         void releaseGraph()
         {
@@ -521,6 +516,7 @@ namespace pt
             L.refill = c.refill;
             L.refillShadow = c.refillShadow;
             L.bvhFormat = c.bvh;
+            L.stackCap = static_cast<int>(c.stack);
             L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
             {
@@ -570,6 +566,7 @@ namespace pt
             L.refill = c.refill;
             L.refillShadow = c.refillShadow;
             L.bvhFormat = c.bvh;
+            L.stackCap = static_cast<int>(c.stack);
             L.shadeFork = c.queues ? nullptr : shadeFork_;
             for (uint32_t m = 0; m < kModelCount; m++)
             {
@@ -617,7 +614,7 @@ namespace pt
             FrameConfig c;
             PT_TRY(resolveConfig(s, c));
             PT_TRY(ensurePool(c.pool));
-            if (c.width != width_ || c.height != height_ || !framebuffer_.get<void>())
+            if (c.width != width_ || c.height != height_ || !framebuffer_.get<void>() || !accumulation_.get<void>())
             {
                 releaseGraph();
                 PT_TRY(ensureFrame(c.width, c.height));

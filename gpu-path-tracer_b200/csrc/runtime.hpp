@@ -50,14 +50,18 @@ namespace pt
         DeviceBuffer(const DeviceBuffer&) = delete;
         DeviceBuffer& operator=(const DeviceBuffer&) = delete;
         ~DeviceBuffer() { reset(); }
+        // Grows the buffer to at least `bytes` (contents are not kept). The new allocation is made before
+        // the old one is freed, so a failed call leaves the buffer as it was.
         Status allocate(size_t bytes)
         {
             if (bytes <= bytes_ && ptr_) return Status::Ok();
-            reset();
             if (bytes == 0) return Status::Ok();
             if (InjectedAllocationFailure())
                 return Status::Err(GPT_ERR_OUT_OF_MEMORY, "cudaMalloc failed: out of memory (injected by gpt_inject_allocation_failure)");
-            PT_CUDA("cudaMalloc", cudaMalloc(&ptr_, bytes));
+            void* fresh = nullptr;
+            PT_CUDA("cudaMalloc", cudaMalloc(&fresh, bytes));
+            reset();
+            ptr_ = fresh;
             bytes_ = bytes;
             return Status::Ok();
         }

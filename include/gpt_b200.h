@@ -156,9 +156,9 @@ typedef struct gpt_render_settings {
     uint32_t max_iterations;      /* 0 = the automatic bound of the device loop, depth x (ceil(samples / pool) + 2) + 64;
                                      else at most this many wavefront iterations: a frame that still has paths in flight
                                      then ends with GPT_ERR_DEVICE_FAULT (the loop's bounded wait running out) */
-    uint32_t trace_stack;         /* 0 = traversal stack sized to the BVH8 depth; else 8, 16, 32 or 64 entries (rounded up
-                                     to one of them): a stack shallower than the tree can overflow, and a ray that
-                                     overflows stops traversing and the frame ends with GPT_ERR_DEVICE_FAULT */
+    uint32_t trace_stack;         /* 0 = traversal stack sized to the BVH8 depth; else at most this many entries (1-64)
+                                     per ray: a stack shallower than the tree can overflow, and a ray that would push
+                                     beyond it stops traversing and the frame ends with GPT_ERR_DEVICE_FAULT */
 } gpt_render_settings;
 
 #define GPT_LOOP_GRAPH 0u
