@@ -419,10 +419,13 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
     # per-job slowdown: latency over the job's own render time alone (one-at-a-time server, admission
     # to completion)
     for rate in rates:
+        key = f"{rate:g}_jobs_per_s"
         for mode in ("served", "plain"):
             sd = sorted(l / max(a, 1e-6) for l, a in zip(latencies[(mode, rate)], alone[rate]))
-            out[mode][f"{rate:g}_jobs_per_s"]["p50_slowdown"] = workloads.percentile(sd, 50)
-            out[mode][f"{rate:g}_jobs_per_s"]["p99_slowdown"] = workloads.percentile(sd, 99)
+            out[mode][key]["p50_slowdown"] = workloads.percentile(sd, 50)
+            out[mode][key]["p99_slowdown"] = workloads.percentile(sd, 99)
+        out["served"][key]["device_speedup_vs_plain"] = (out["served"][key]["device_paths_per_second"]
+                                                         / out["plain"][key]["device_paths_per_second"])
     return out
 
 

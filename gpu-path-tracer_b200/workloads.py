@@ -5,8 +5,8 @@ triangles). Each job draws its resolution log-uniform between 256x256 and 1920x1
 per pixel uniform in {1, 4, 16, 64}, its path depth uniform in 8..12, and its own camera: a seeded
 position on a sphere around the scene centre, looking at the centre.
 
-Served: open-loop Poisson arrivals at a given rate over 8 resident scenes of 50k to 4M triangles.
-Each job draws its resolution log-uniform between 128x128 and 2048x2048, its samples per pixel from
+Served: open-loop Poisson arrivals at a given rate over 8 resident scenes of 50k to 4M triangles;
+one seeded job list for every rate (only the arrival times scale with 1/rate). Each job draws its resolution log-uniform between 128x128 and 2048x2048, its samples per pixel from
 {4, 16, 64, 256}, its depth uniform in 8..12 and a random camera as above.
 
 The reference renders one job at a time (Renderer::StartSimulation, Renderer.cpp:330-466); these
@@ -78,17 +78,19 @@ def batched_jobs(n_jobs: int = 64, seed: int = BATCH_SEED) -> list[Job]:
 
 
 def served_jobs(rate: float, n_jobs: int, seed: int = SERVE_SEED) -> list[Job]:
-    """n_jobs arrivals of a Poisson process of `rate` jobs per second (exponential gaps)."""
-    rng = np.random.default_rng(seed + int(rate * 1000))
-    t = 0.0
+    """n_jobs arrivals of a Poisson process of `rate` jobs per second (exponential gaps). The jobs
+    themselves and the unit-mean gaps come from the seed alone, and the gaps are divided by the rate,
+    so every rate serves the same job list and only the offered load changes."""
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0, n_jobs)
+    t = np.cumsum(gaps) / rate
     jobs = []
-    for _ in range(n_jobs):
-        t += float(rng.exponential(1.0 / rate))
+    for k in range(n_jobs):
         scene = SERVE_SCENES[int(rng.integers(0, len(SERVE_SCENES)))]
         w, h = log_uniform_resolution(rng, (128, 128), (2048, 2048))
         spp = int(rng.choice([4, 16, 64, 256]))
         depth = int(rng.integers(8, 13))
-        jobs.append(Job(scene, w, h, spp, depth, orbit_camera(rng, w, h), arrival_s=t))
+        jobs.append(Job(scene, w, h, spp, depth, orbit_camera(rng, w, h), arrival_s=float(t[k])))
     return jobs
 
 

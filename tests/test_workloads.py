@@ -45,6 +45,11 @@ def test_served_arrivals_are_poisson_and_seeded():
         for j in jobs:
             assert j.scene in workloads.SERVE_SCENES and j.spp in (4, 16, 64, 256)
             assert 128 <= j.width <= 2048 and 128 <= j.height <= 2048 and j.width == j.height
+    # every rate serves the same jobs; only the arrival times scale with 1/rate
+    a, b = workloads.served_jobs(20.0, 48), workloads.served_jobs(100.0, 48)
+    assert [(j.scene, j.width, j.height, j.spp, j.depth) for j in a] == [(j.scene, j.width, j.height, j.spp, j.depth) for j in b]
+    assert all(np.array_equal(x.camera, y.camera) for x, y in zip(a, b))
+    assert np.allclose([j.arrival_s * 20.0 for j in a], [j.arrival_s * 100.0 for j in b], rtol=1e-12)
 
 
 def test_percentile_is_nearest_rank():
