@@ -112,11 +112,11 @@ namespace pt
         const float3 v0 = make_float3(a.x, a.y, a.z);
         const float3 e1 = make_float3(b.x, b.y, b.z);
         const float3 e2 = make_float3(c.x, c.y, c.z);
-        const float3 p = cross(d, e2);
-        const float det = dot(e1, p);
+        const float3 p = mt_cross(d, e2);
+        const float det = mt_dot(e1, p);
         if (fabsf(det) < 1e-7f) return false;
         const float3 s = o - v0;
-        const float sp = dot(s, p);
+        const float sp = mt_dot_sp(s, p);
         // u = sp * (1/det) is negative when sp and det have opposite signs and the product does not
         // round to zero; with |sp| > 1e-20 and |det| < 1e20 its magnitude exceeds 1e-40, so the
         // reference's u < 0 rejection is decided here without the division (same outcome, bit for bit).
@@ -124,10 +124,10 @@ namespace pt
         const float invDet = 1.0f / det;
         u = sp * invDet;
         if (u < 0.0f || u > 1.0f) return false;
-        const float3 q = cross(s, e1);
-        v = dot(d, q) * invDet;
+        const float3 q = mt_cross(s, e1);
+        v = mt_dot(d, q) * invDet;
         if (v < 0.0f || u + v > 1.0f) return false;
-        t = dot(e2, q) * invDet;
+        t = mt_dot(e2, q) * invDet;
         return true;
     }
 
