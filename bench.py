@@ -447,6 +447,7 @@ def precision_section(knobs):
         t0 = time.perf_counter()
         r.upload_scene(s)
         out["scene_upload_s"] = time.perf_counter() - t0
+        out["scene_upload_breakdown_s"] = r.upload_times()
         info = r.scene_info()
         out["triangles"], out["lights"] = info["triangles"], info["lights"]
         cam = scenes.scene_camera(s, W, H)
@@ -608,6 +609,7 @@ def b200_arm(args):
     t0 = time.perf_counter()
     renderer.upload_scene(scene)
     upload_s = time.perf_counter() - t0
+    upload_breakdown = renderer.upload_times()
     info = renderer.scene_info()
     cam = scenes.scene_camera(scene, W, H)
     import multigpu
@@ -704,6 +706,7 @@ def b200_arm(args):
         "iterations_per_step": iters / args.steps,
         "phase_ms_per_step": {k: sum(s["phase_ms"][k] for s in stats) / args.steps for k in ("trace", "shade", "shadow", "regen")},
         "scene_upload_s": upload_s,
+        "scene_upload_breakdown_s": upload_breakdown,
         "traversal": traversal_summary(stats[-1], NODE_BYTES),
         "roofline": {"kernel": "trace_kernel<closest> (BVH8 closest hit)", "bound": "latency", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,

@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -142,6 +143,7 @@ namespace pt
         if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
             d.material_count == 0)
             return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Scene description is incomplete");
+        const auto tUpload = std::chrono::steady_clock::now();
         const uint32_t n = d.triangle_count;
         std::vector<uint32_t> models(n);
         bool present[kModelCount] = {};
@@ -188,6 +190,7 @@ namespace pt
         }
         // BVH8 on the host (binned SAH, collapse, quantisation).
         Bvh8 bvh;
+        const auto tBvh = std::chrono::steady_clock::now();
         try
         {
             bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), withBinary);
@@ -196,6 +199,7 @@ namespace pt
         {
             return Status::Err(GPT_ERR_INVALID_ARGUMENT, std::string("BVH build failed: ") + e.what());
         }
+        scene->bvhSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tBvh).count();
         if (bvh.depth > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "BVH8 deeper than the traversal stack");
         if (bvh.nodes.size() >= (1u << 24)) return Status::Err(GPT_ERR_CAPACITY, "BVH8 has more than 2^24 nodes");
         scene->nodeCount = static_cast<uint32_t>(bvh.nodes.size());
@@ -269,6 +273,7 @@ namespace pt
         PT_TRY(scene->entry.allocate(sizeof(SceneEntry)));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->entry.get<void>(), &entry, sizeof(entry), cudaMemcpyHostToDevice, stream));
         PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream));
+        scene->uploadSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tUpload).count();
         out = std::move(scene);
         return Status::Ok();
     }
@@ -1228,6 +1233,15 @@ extern "C"
         if (!r->impl->scene_) return GPT_ERR_NO_SCENE;
         if (node_count) *node_count = r->impl->scene_->nodeCount2;
         if (depth) *depth = r->impl->scene_->depth2;
+        return GPT_OK;
+    }
+
+    int gpt_scene_upload_times(const gpt_renderer* r, double* bvh_build_seconds, double* upload_seconds)
+    {
+        if (!r) return GPT_ERR_INVALID_ARGUMENT;
+        if (!r->impl->scene_) return GPT_ERR_NO_SCENE;
+        if (bvh_build_seconds) *bvh_build_seconds = r->impl->scene_->bvhSeconds;
+        if (upload_seconds) *upload_seconds = r->impl->scene_->uploadSeconds;
         return GPT_OK;
     }
 

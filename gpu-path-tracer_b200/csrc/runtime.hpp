@@ -108,6 +108,7 @@ namespace pt
         uint32_t nodeCount2 = 0, depth2 = 0;  // binary FP32 BVH, built when the scene is uploaded with it
         bool modelPresent[kModelCount] = {};
         uint64_t version = 0;
+        double bvhSeconds = 0.0, uploadSeconds = 0.0;  // host BVH build; whole upload (wall clock)
         SceneView view() const
         {
             SceneView v{};

@@ -175,6 +175,8 @@ _SIGNATURES = [
                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_scene_info_binary", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32),
                                              ctypes.POINTER(ctypes.c_uint32)]),
+    ("gpt_scene_upload_times", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                              ctypes.POINTER(ctypes.c_double)]),
     ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_read_alias_table_power", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_inject_allocation_failure", ctypes.c_int, [ctypes.c_uint32]),
@@ -300,6 +302,12 @@ class Renderer:
         self._check(self.L.gpt_scene_info_binary(self.h, ctypes.byref(n2), ctypes.byref(d2)), "gpt_scene_info_binary")
         return dict(nodes=n.value, depth=d.value, lights=l.value, triangles=t.value, binary_nodes=n2.value,
                     binary_depth=d2.value)
+
+    def upload_times(self) -> dict:
+        """Seconds of the last upload: host BVH build, and the whole upload."""
+        b, u = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.gpt_scene_upload_times(self.h, ctypes.byref(b), ctypes.byref(u)), "gpt_scene_upload_times")
+        return dict(bvh_build_s=b.value, upload_s=u.value)
 
     def alias_table(self, power: bool = False) -> np.ndarray:
         """[lights, 4] words (q, p, alias, value): the area-weighted table, or with power=True the

@@ -296,6 +296,11 @@ int gpt_scene_info(const gpt_renderer* renderer, uint32_t* node_count, uint32_t*
 /* Node count and depth of the scene's binary FP32 BVH (HostBvh.cpp:22-100 builds the reference's
  * binary tree by median splits; this one is the binned-SAH tree the BVH8 is collapsed from). */
 int gpt_scene_info_binary(const gpt_renderer* renderer, uint32_t* node_count, uint32_t* depth);
+/* Wall-clock seconds of the last scene upload: the host BVH build (binned SAH, 8-wide collapse,
+ * quantisation; all host threads) and the whole gpt_init_scene_buffers call, which adds validation,
+ * textures, host-to-device copies and the device-built shading records, lights and alias tables
+ * (Renderer.cpp:292-306 is the reference's upload; it reports no timings). */
+int gpt_scene_upload_times(const gpt_renderer* renderer, double* bvh_build_seconds, double* upload_seconds);
 /* The light alias table built on the device, [lights][4] words (q, p, alias, value)
  * (AliasTableView.hpp:8-14). */
 int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
