@@ -22,8 +22,8 @@ On one GPU the line also carries (--sections, default all):
              device loop, against the same jobs one at a time (server, frame renderer, plain form)
   serving    open-loop Poisson arrivals (20, 50, 100 jobs/s) over 8 resident scenes (50k-4M
              triangles): p50/p99 latency, paths/s and admitted-bytes high-water mark, served
-             (continuous batching, shortest remaining work first and earliest deadline) against one
-             job at a time
+             (continuous batching: short jobs first, then the others in submission order; and shortest
+             remaining work first) against one job at a time
   precision  8M-triangle scene at 3840x2160, 16 spp, depth 10: BVH8 with 8-bit quantised boxes
              against the binary FP32 BVH (node bytes per ray, traversal Mrays/s), and the FP32 Kahan
              accumulation against FP64 accumulation of the same per-sample radiance (RMSE)
@@ -390,9 +390,10 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
     pool = min(knobs["pool_size"], max_pool)
     out["pool_size"] = pool
     latencies, alone = {}, {}
-    # served: continuous batching, shortest remaining work first (or schedule_served); deadline: the
-    # same server ordering jobs by submit time + 4 x their estimated render time; plain: one job at a time
-    modes = (("served", 0, schedule_served), ("deadline", 0, pathtracer.SCHEDULE_DEADLINE), ("plain", 1, 0))
+    # served: continuous batching in the server's default order (short jobs first, shortest remaining
+    # work first among them, the other jobs in submission order); shortest_first: the same server
+    # ordering every job by samples left; plain: one job at a time
+    modes = (("served", 0, schedule_served), ("shortest_first", 0, pathtracer.SCHEDULE_SHORTEST_FIRST), ("plain", 1, 0))
     for mode, active, schedule in modes:
         srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30, schedule=schedule,
                                 **_server_knobs(knobs))
@@ -428,7 +429,7 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
             sd = sorted(l / max(a, 1e-6) for l, a in zip(latencies[(mode, rate)], alone[rate]))
             out[mode][key]["p50_slowdown"] = workloads.percentile(sd, 50)
             out[mode][key]["p99_slowdown"] = workloads.percentile(sd, 99)
-        for mode in ("served", "deadline"):
+        for mode in ("served", "shortest_first"):
             out[mode][key]["device_speedup_vs_plain"] = (out[mode][key]["device_paths_per_second"]
                                                          / out["plain"][key]["device_paths_per_second"])
     return out
@@ -513,8 +514,8 @@ def summary(line):
     if isinstance(serving, dict) and isinstance(serving.get("served"), dict):
         out["serving_latency_s"] = {
             rate: {"served_p50": v.get("p50_latency_s"), "served_p99": v.get("p99_latency_s"),
-                   "deadline_p50": get(serving, "deadline", rate, "p50_latency_s"),
-                   "deadline_p99": get(serving, "deadline", rate, "p99_latency_s"),
+                   "shortest_first_p50": get(serving, "shortest_first", rate, "p50_latency_s"),
+                   "shortest_first_p99": get(serving, "shortest_first", rate, "p99_latency_s"),
                    "plain_p50": get(serving, "plain", rate, "p50_latency_s"), "plain_p99": get(serving, "plain", rate, "p99_latency_s")}
             for rate, v in serving["served"].items() if isinstance(v, dict)}
     return out

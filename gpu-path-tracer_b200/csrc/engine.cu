@@ -243,8 +243,9 @@ namespace pt
             refillShadow_ = ((cfg_.trace_refill >> 8) & 0xFFu) ? std::min(32u, std::max(1u, (cfg_.trace_refill >> 8) & 0xFFu))
                                                                 : std::max(1u, refill_ / 2u);
             occupancy_ = cfg_.trace_occupancy == 0 ? 10 : (cfg_.trace_occupancy >= 12 ? 12 : (cfg_.trace_occupancy >= 10 ? 10 : 1));
-            schedule_ = cfg_.schedule == 0 ? GPT_SCHEDULE_SHORTEST_FIRST : cfg_.schedule;
+            schedule_ = cfg_.schedule == 0 ? GPT_SCHEDULE_TWO_CLASS : cfg_.schedule;
             if (!(cfg_.deadline_slowdown > 0.0f)) cfg_.deadline_slowdown = 4.0f;
+            if (!(cfg_.short_job_seconds > 0.0f)) cfg_.short_job_seconds = 0.05f;
             t0_ = std::chrono::steady_clock::now();
         }
 
@@ -276,7 +277,7 @@ namespace pt
 
         Status Init()
         {
-            if (cfg_.schedule > GPT_SCHEDULE_DEADLINE) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
+            if (cfg_.schedule > GPT_SCHEDULE_TWO_CLASS) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking));
@@ -668,8 +669,15 @@ namespace pt
                 active_.push_back(J.id);
                 pending_.pop_front();
             }
-            // Slot priority of the next slice: the device plan hands idle slots to the jobs in this order.
-            std::vector<std::pair<double, uint32_t>> ranked;
+            // Slot priority of the next slice: the device plan hands idle slots to the jobs in this order
+            // (by class, then key; the stable sort keeps submission order among equal keys).
+            struct Rank
+            {
+                int cls;
+                double key;
+                uint32_t table;
+            };
+            std::vector<Rank> ranked;
             ranked.reserve(active_.size());
             for (uint64_t id : active_)
             {
@@ -677,15 +685,25 @@ namespace pt
                 const uint32_t t = J.tableIndex;
                 const JobView& v = mirror_[t];
                 const uint64_t left = v.totalSamples > v.launched ? v.totalSamples - v.launched : 0;
-                double key = 0.0;  // oldest first: all equal, the stable sort keeps submission order
+                int cls = 0;
+                double key = 0.0;  // oldest first: all equal
                 if (schedule_ == GPT_SCHEDULE_SHORTEST_FIRST) key = static_cast<double>(left);
                 else if (schedule_ == GPT_SCHEDULE_DEADLINE)
                     key = J.tSubmit + cfg_.deadline_slowdown * static_cast<double>(v.totalSamples) / rateEstimate_;
-                ranked.emplace_back(key, t);
+                else if (schedule_ == GPT_SCHEDULE_TWO_CLASS)
+                {
+                    // short jobs (estimated render time alone below short_job_seconds) first, fewest samples
+                    // left first; long jobs after them in submission order
+                    const bool isShort = static_cast<double>(v.totalSamples) / rateEstimate_ < cfg_.short_job_seconds;
+                    cls = isShort ? 0 : 1;
+                    key = isShort ? static_cast<double>(left) : 0.0;
+                }
+                ranked.push_back(Rank{cls, key, t});
             }
-            std::stable_sort(ranked.begin(), ranked.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            std::stable_sort(ranked.begin(), ranked.end(),
+                             [](const Rank& a, const Rank& b) { return a.cls != b.cls ? a.cls < b.cls : a.key < b.key; });
             uint32_t n = 0;
-            for (const auto& r : ranked) orderHost_[n++] = r.second;
+            for (const auto& r : ranked) orderHost_[n++] = r.table;
             sliceWords_[0] = n;
             sliceWords_[1] = 0;
             sliceWords_[2] = cfg_.max_slice_iterations;

@@ -385,9 +385,9 @@ void gpt_obj_free(gpt_obj_scene* scene);
  * Admission accounting per job: 64 bytes per path the job may have in flight (min(ring passes x
  * pixels, pool)) plus its framebuffers (pass ring 12 B, Kahan accumulator 32 B, RGBA8 4 B per
  * pixel and pass). Jobs are admitted in submission order; a job larger than the whole budget is
- * refused at submission with GPT_ERR_CAPACITY. Among admitted jobs, idle path slots go first to
- * the job with the fewest samples left (or to the oldest, by gpt_server_config.schedule); the order
- * changes which job finishes first, never an image. All gpt_server_* calls are thread-safe.
+ * refused at submission with GPT_ERR_CAPACITY. Among admitted jobs, idle path slots go to short
+ * jobs first, then to the others in submission order (or as gpt_server_config.schedule says); the
+ * order changes which job finishes first, never an image. All gpt_server_* calls are thread-safe.
  */
 typedef struct gpt_server gpt_server;
 
@@ -401,17 +401,22 @@ typedef struct gpt_server_config {
     uint32_t trace_refill;
     uint32_t trace_occupancy;
     uint32_t max_slice_iterations; /* wavefront iterations per graph launch at most (0 = 4096) */
-    uint32_t schedule;             /* which active job gets idle path slots first: 0/GPT_SCHEDULE_SHORTEST_FIRST = the
-                                      job with the fewest samples left, GPT_SCHEDULE_OLDEST_FIRST = submission order,
+    uint32_t schedule;             /* which active job gets idle path slots first: 0/GPT_SCHEDULE_TWO_CLASS = jobs whose
+                                      render time alone (samples / the server's measured paths per second) is below
+                                      short_job_seconds first, fewest samples left first, then the other jobs in
+                                      submission order; GPT_SCHEDULE_SHORTEST_FIRST = the job with the fewest samples
+                                      left; GPT_SCHEDULE_OLDEST_FIRST = submission order;
                                       GPT_SCHEDULE_DEADLINE = the earliest deadline, submit time + deadline_slowdown x the
                                       job's samples / the server's measured paths per second (small jobs still go
                                       first, and a large job is not passed over past its deadline) */
     float deadline_slowdown;       /* GPT_SCHEDULE_DEADLINE: deadline in units of the job's own render time (0 = 4) */
+    float short_job_seconds;       /* GPT_SCHEDULE_TWO_CLASS: render time alone below which a job is short (0 = 0.05) */
 } gpt_server_config;
 
 #define GPT_SCHEDULE_SHORTEST_FIRST 1u
 #define GPT_SCHEDULE_OLDEST_FIRST 2u
 #define GPT_SCHEDULE_DEADLINE 3u
+#define GPT_SCHEDULE_TWO_CLASS 4u
 
 typedef struct gpt_job_desc {
     uint32_t scene;                /* id from gpt_server_add_scene */

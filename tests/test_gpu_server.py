@@ -110,11 +110,12 @@ def test_mixed_jobs_match_alone(resident, frame_renderers):
 
 
 @pytest.mark.parametrize("schedule", [pathtracer.SCHEDULE_SHORTEST_FIRST, pathtracer.SCHEDULE_OLDEST_FIRST,
-                                      pathtracer.SCHEDULE_DEADLINE])
+                                      pathtracer.SCHEDULE_DEADLINE, pathtracer.SCHEDULE_TWO_CLASS])
 def test_schedule_orders_completion_not_images(resident, frame_renderers, schedule):
-    """Shortest-first hands idle slots to the job with the fewest samples left, and earliest-deadline
-    first to the job whose deadline (submit time + slowdown x its size / rate) comes first: in both, a
-    small job submitted right after a large one finishes first. Every policy gives the same images."""
+    """Shortest-first hands idle slots to the job with the fewest samples left, earliest-deadline
+    first to the job whose deadline (submit time + slowdown x its size / rate) comes first, and the
+    two-class order to short jobs (both are short here) by samples left: in all three, a small job
+    submitted right after a large one finishes first. Every policy gives the same images."""
     srv, ids = make_server(resident, pool_size=4096, schedule=schedule)
     try:
         big = ("spheres-small", 128, 128, 64, 12, True, 0)
@@ -128,7 +129,27 @@ def test_schedule_orders_completion_not_images(resident, frame_renderers, schedu
     finally:
         srv.close()
     with pytest.raises(pathtracer.GptError):
-        pathtracer.Server(0, schedule=4)
+        pathtracer.Server(0, schedule=5)
+
+
+def test_two_class_schedule_keeps_long_jobs_in_submission_order(resident, frame_renderers):
+    """Two classes: a short job (render time alone below short_job_seconds) passes the long jobs, and
+    the long jobs keep their submission order although the later one has fewer samples left, which
+    shortest-first would run first."""
+    srv, ids = make_server(resident, pool_size=4096, schedule=pathtracer.SCHEDULE_TWO_CLASS, short_job_seconds=1e-5)
+    try:
+        long_a = ("spheres-small", 128, 128, 16, 10, True, 0)   # 262,144 paths
+        long_b = ("spheres-small", 64, 64, 16, 10, True, 0)     # 65,536 paths
+        small = ("cornell-all", 16, 16, 1, 6, True, 0)          # 256 paths
+        j_a = submit(srv, ids, resident, long_a)
+        j_b = submit(srv, ids, resident, long_b)
+        j_s = submit(srv, ids, resident, small)
+        for j, job in ((j_a, long_a), (j_b, long_b), (j_s, small)):
+            check_job(srv, j, frame_renderers, resident, job)
+        done = {j: srv.poll(j)["done_s"] for j in (j_a, j_b, j_s)}
+        assert done[j_s] < done[j_a] < done[j_b]
+    finally:
+        srv.close()
 
 
 def test_deadline_schedule_does_not_pass_over_a_late_job(resident, frame_renderers):
