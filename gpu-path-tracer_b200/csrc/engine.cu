@@ -736,12 +736,20 @@ namespace pt
             PT_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, startEvent_, stopEvent_));
             deviceMs_ += ms;
             slices_++;
-            // paths per second of the server (device time), smoothed over slices; deadline scheduling's clock
+            // paths per second of the server (device time), the clock of the two-class and deadline
+            // orders. Samples are counted when launched, and a slice can refill the whole pool in its
+            // first iteration, so one short slice overstates the rate many times over: the estimate is
+            // taken over windows of at least 100 ms of device time (a pool-full then moves it by a few
+            // per cent) and smoothed across windows.
             const uint64_t samples = hostCounters_->launched;
-            if (ms > 0.5f && samples > lastSliceSamples_)
+            if (samples > lastSliceSamples_) rateSamples_ += samples - lastSliceSamples_;
+            rateMs_ += ms;
+            if (rateMs_ >= 100.0)
             {
-                const double rate = static_cast<double>(samples - lastSliceSamples_) / (ms / 1000.0);
-                rateEstimate_ = 0.8 * rateEstimate_ + 0.2 * rate;
+                const double rate = static_cast<double>(rateSamples_) / (rateMs_ / 1000.0);
+                rateEstimate_ = 0.5 * rateEstimate_ + 0.5 * rate;
+                rateSamples_ = 0;
+                rateMs_ = 0.0;
             }
             lastSliceSamples_ = samples;
             if (hostCounters_->errorFlags)
@@ -897,9 +905,11 @@ namespace pt
         int device_;
         gpt_server_config cfg_;
         int threads_ = 128, occupancy_ = 10;
-        uint32_t schedule_ = GPT_SCHEDULE_SHORTEST_FIRST;
+        uint32_t schedule_ = GPT_SCHEDULE_TWO_CLASS;
         double rateEstimate_ = 1e9;        // paths per second, smoothed (initial guess: one B200 on a mid-size scene)
         uint64_t lastSliceSamples_ = 0;
+        uint64_t rateSamples_ = 0;         // samples launched in the current rate window
+        double rateMs_ = 0.0;              // device milliseconds of the current rate window
         uint32_t refill_ = 16, refillShadow_ = 8;
         std::chrono::steady_clock::time_point t0_;
         cudaStream_t stream_ = nullptr;

@@ -200,7 +200,21 @@ def test_render_errors_and_clear(gpu_renderer, scene_factory):
     fresh.clear(10, 20, 30, 255)
     fb = fresh.lock_frame()
     assert fb.size == 128 and np.all(fb == (10 | 20 << 8 | 30 << 16 | 255 << 24))
+    with pytest.raises(P.GptError) as e:
+        fresh.upload_times()
+    assert e.value.code == 5
     fresh.close()
+
+
+def test_scene_upload_times(gpu_renderer, scene_factory):
+    """The upload reports the host BVH build inside the whole upload's wall time."""
+    import time as _time
+    s = scene_factory("spheres-200k")
+    t0 = _time.perf_counter()
+    gpu_renderer.upload_scene(s)
+    wall = _time.perf_counter() - t0
+    t = gpu_renderer.upload_times()
+    assert 0.0 < t["bvh_build_s"] < t["upload_s"] <= wall
 
 
 def test_simulation_thread_frames_stop_resume(gpu_renderer, scene_factory):
