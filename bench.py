@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--no-reference-build", action="store_true",
                     help="skip timing the reference's own kernels (oracle/_ref) on the same frame")
     ap.add_argument("--serve-rates", default="20,50,100", help="Poisson arrival rates (jobs/s) of the serving section")
+    ap.add_argument("--serve-short-seconds", type=float, default=0.0,
+                    help="render time alone below which the served server treats a job as short (0 = the server's default)")
     ap.add_argument("--serve-pool", type=int, default=1 << 23,
                     help="most path slots of the serving section's servers (latency of small jobs grows with the pool)")
     return ap.parse_args()
@@ -373,7 +375,7 @@ def batched_section(knobs):
     return out
 
 
-def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
+def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_seconds=0.0):
     """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time.
     Both servers hold at most max_pool path slots: an iteration's time grows with the slots in flight,
     and a small job needs a fixed number of iterations, so its latency grows with the pool."""
@@ -396,7 +398,7 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0):
     modes = (("served", 0, schedule_served), ("shortest_first", 0, pathtracer.SCHEDULE_SHORTEST_FIRST), ("plain", 1, 0))
     for mode, active, schedule in modes:
         srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30, schedule=schedule,
-                                **_server_knobs(knobs))
+                                short_job_seconds=short_seconds, **_server_knobs(knobs))
         res = {}
         try:
             ids = {n: srv.add_scene(s) for n, s in resident.items()}
@@ -774,7 +776,8 @@ def b200_arm(args):
         line["batched"] = run_section("batched", lambda: batched_section(knobs))
     if "serving" in sections:
         rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
-        line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs, args.serve_pool))
+        line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs, args.serve_pool,
+                                                                           short_seconds=args.serve_short_seconds))
     if "precision" in sections:
         pr = run_section("precision", lambda: precision_section(knobs))
         line["precision"] = pr

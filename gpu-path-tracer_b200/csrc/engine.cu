@@ -371,7 +371,8 @@ namespace pt
             uint32_t ring = cfg_.ring_passes;
             if (ring == 0)
             {
-                const uint64_t fill = (2ull * cfg_.pool_size + J.pixels - 1) / J.pixels;
+                // four pool-fulls of passes: a window this deep rarely waits on the oldest pass's longest paths
+                const uint64_t fill = (4ull * cfg_.pool_size + J.pixels - 1) / J.pixels;
                 ring = static_cast<uint32_t>(std::min<uint64_t>(std::max<uint64_t>(fill, 2), kMaxRing));
             }
             J.ring = std::min(ring, J.spp);
@@ -703,7 +704,9 @@ namespace pt
             std::stable_sort(ranked.begin(), ranked.end(),
                              [](const Rank& a, const Rank& b) { return a.cls != b.cls ? a.cls < b.cls : a.key < b.key; });
             uint32_t n = 0;
-            for (const auto& r : ranked) orderHost_[n++] = r.table;
+            // two classes: long jobs take their turns in submission order; a later one gets slots only once
+            // the ones ahead have launched everything (not merely while their pass windows are full)
+            for (const auto& r : ranked) orderHost_[n++] = r.table | (schedule_ == GPT_SCHEDULE_TWO_CLASS && r.cls == 1 ? kOrderInTurn : 0u);
             sliceWords_[0] = n;
             sliceWords_[1] = 0;
             sliceWords_[2] = cfg_.max_slice_iterations;

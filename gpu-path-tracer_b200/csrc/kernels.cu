@@ -1701,19 +1701,28 @@ namespace pt
         EngineCtl* e = ev.ctl;
         const uint32_t avail = wf.ctr->regenCount + e->freeCount;
         uint32_t launch = 0, segments = 0;
+        // a job marked kOrderInTurn gets slots only once every marked job before it has launched all
+        // its samples (its turn has come), even if an earlier one's pass window holds it back for now
+        bool waitTurn = false;
         for (uint32_t i = 0; i < e->orderCount && launch < avail; i++)
         {
-            const uint32_t j = ev.order[i];
+            const uint32_t o = ev.order[i];
+            const uint32_t j = o & ~kOrderInTurn;
             JobView& J = ev.jobs[j];
             if (J.state != kJobActive) continue;
+            const bool inTurn = (o & kOrderInTurn) != 0;
+            if (inTurn && waitTurn) continue;
             const uint64_t end = job_window_end(J);
-            if (end <= J.launched) continue;
-            const uint64_t can = end - J.launched;
-            const uint32_t take = static_cast<uint32_t>(can < static_cast<uint64_t>(avail - launch) ? can : avail - launch);
-            ev.segments[segments] = LaunchSegment{j, launch, J.launched};
-            segments++;
-            J.launched += take;
-            launch += take;
+            if (end > J.launched)
+            {
+                const uint64_t can = end - J.launched;
+                const uint32_t take = static_cast<uint32_t>(can < static_cast<uint64_t>(avail - launch) ? can : avail - launch);
+                ev.segments[segments] = LaunchSegment{j, launch, J.launched};
+                segments++;
+                J.launched += take;
+                launch += take;
+            }
+            if (inTurn && J.launched < J.totalSamples) waitTurn = true;
         }
         e->launchCount = launch;
         e->segmentCount = segments;
@@ -1890,7 +1899,7 @@ namespace pt
             uint32_t count = 0, j = 0;
             if (i < orderCount)
             {
-                j = ev.order[i];
+                j = ev.order[i] & ~kOrderInTurn;
                 const JobView& J = ev.jobs[j];
                 if (J.state == kJobActive) count = foldable_passes(J);
             }
@@ -1944,7 +1953,7 @@ namespace pt
             const uint32_t orderCount = ev.ctl->orderCount;
             for (uint32_t i = threadIdx.x; i < orderCount; i += blockDim.x)
             {
-                JobView& J = ev.jobs[ev.order[i]];
+                JobView& J = ev.jobs[ev.order[i] & ~kOrderInTurn];
                 if (J.state != kJobActive) continue;
                 const uint32_t count = foldable_passes(J);
                 for (uint32_t q = 0; q < count; q++) J.passDone[(static_cast<uint64_t>(J.folded) + q) % J.ring] = 0;

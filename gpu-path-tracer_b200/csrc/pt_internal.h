@@ -165,6 +165,10 @@ namespace pt
         uint32_t lightMode;       // LightMode
     };
 
+    // Bit of a job-server order entry (the rest is the job-table index): the job takes path slots only
+    // once every marked job ahead of it has launched all its samples.
+    constexpr uint32_t kOrderInTurn = 0x80000000u;
+
     enum JobState : uint32_t
     {
         kJobFree = 0,

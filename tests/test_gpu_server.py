@@ -216,8 +216,9 @@ def test_one_job_at_a_time(resident, frame_renderers):
 
 def test_budget_admission_and_refusal(resident, frame_renderers):
     name, w, h = "cornell-all", 64, 64
-    # a budget for one such job at a time (about 0.5 MB: 64 B x 4096 in-flight paths + framebuffers)
-    budget = 600_000
+    # a budget for one such job at a time (about 0.61 MB: 64 B x 4096 in-flight paths, a ring of its 4
+    # passes, accumulator and framebuffer; two jobs need 1.2 MB)
+    budget = 700_000
     srv, ids = make_server(resident, pool_size=1 << 12, hbm_budget_bytes=budget)
     try:
         with pytest.raises(pathtracer.GptError) as e:
