@@ -71,7 +71,10 @@ def parse():
     ap.add_argument("--trace-block", type=int, default=0, help="with --no-autotune: traversal threads per block")
     ap.add_argument("--sections", default="all",
                     help="comma list of extra one-GPU sections: plain,cornell,batched,serving,precision,lights (all/none)")
-    ap.add_argument("--serve-jobs", type=int, default=48, help="jobs per arrival rate in the serving section")
+    ap.add_argument("--serve-jobs", type=int, default=200,
+                    help="jobs per arrival rate in the serving section (p99 of fewer than 100 jobs is their maximum)")
+    ap.add_argument("--serve-shortest-first", action="store_true",
+                    help="serving section: also run the server ordering every job by samples left")
     ap.add_argument("--no-reference-build", action="store_true",
                     help="skip timing the reference's own kernels (oracle/_ref) on the same frame")
     ap.add_argument("--serve-rates", default="20,50,100", help="Poisson arrival rates (jobs/s) of the serving section")
@@ -328,9 +331,9 @@ def batched_section(knobs):
     out = {"jobs": len(jobs), "paths": total, "scenes": {n: s.triangle_count for n, s in resident.items()},
            "config": "64 jobs, resolution log-uniform 256x256..1920x1080, spp in {1,4,16,64}, depth 8..12, seeded orbit cameras"}
     warm = [workloads.Job(n, 64, 64, 1, 8, scenes.scene_camera(s, 64, 64)) for n, s in resident.items()]
-    for mode, active in (("batched", 0), ("server_one_at_a_time", 1)):
+    for mode, active, schedule in (("batched", 0, 0), ("server_one_at_a_time", 1, pathtracer.SCHEDULE_OLDEST_FIRST)):
         srv = pathtracer.Server(0, pool_size=knobs["pool_size"], max_active_jobs=active, hbm_budget_bytes=32 << 30,
-                                **_server_knobs(knobs))
+                                schedule=schedule, **_server_knobs(knobs))
         try:
             ids = {n: srv.add_scene(s) for n, s in resident.items()}
             _run_jobs_on_server(srv, ids, warm, False)
@@ -375,7 +378,7 @@ def batched_section(knobs):
     return out
 
 
-def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_seconds=0.0):
+def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_seconds=0.0, shortest_first=False):
     """Open-loop Poisson arrivals over 8 resident scenes: continuous batching against one job at a time.
     Both servers hold at most max_pool path slots: an iteration's time grows with the slots in flight,
     and a small job needs a fixed number of iterations, so its latency grows with the pool."""
@@ -394,8 +397,10 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_sec
     latencies, alone = {}, {}
     # served: continuous batching in the server's default order (short jobs first, shortest remaining
     # work first among them, the other jobs in submission order); shortest_first: the same server
-    # ordering every job by samples left; plain: one job at a time
-    modes = (("served", 0, schedule_served), ("shortest_first", 0, pathtracer.SCHEDULE_SHORTEST_FIRST), ("plain", 1, 0))
+    # ordering every job by samples left; plain: one job at a time in submission order
+    modes = (("served", 0, schedule_served),) + (
+        (("shortest_first", 0, pathtracer.SCHEDULE_SHORTEST_FIRST),) if shortest_first else ()) + (
+        ("plain", 1, pathtracer.SCHEDULE_OLDEST_FIRST),)
     for mode, active, schedule in modes:
         srv = pathtracer.Server(0, pool_size=pool, max_active_jobs=active, hbm_budget_bytes=16 << 30, schedule=schedule,
                                 short_job_seconds=short_seconds, **_server_knobs(knobs))
@@ -431,7 +436,7 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_sec
             sd = sorted(l / max(a, 1e-6) for l, a in zip(latencies[(mode, rate)], alone[rate]))
             out[mode][key]["p50_slowdown"] = workloads.percentile(sd, 50)
             out[mode][key]["p99_slowdown"] = workloads.percentile(sd, 99)
-        for mode in ("served", "shortest_first"):
+        for mode in [m for m, _, _ in modes if m != "plain"]:
             out[mode][key]["device_speedup_vs_plain"] = (out[mode][key]["device_paths_per_second"]
                                                          / out["plain"][key]["device_paths_per_second"])
     return out
@@ -515,11 +520,13 @@ def summary(line):
     serving = line.get("serving")
     if isinstance(serving, dict) and isinstance(serving.get("served"), dict):
         out["serving_latency_s"] = {
-            rate: {"served_p50": v.get("p50_latency_s"), "served_p99": v.get("p99_latency_s"),
-                   "shortest_first_p50": get(serving, "shortest_first", rate, "p50_latency_s"),
-                   "shortest_first_p99": get(serving, "shortest_first", rate, "p99_latency_s"),
-                   "plain_p50": get(serving, "plain", rate, "p50_latency_s"), "plain_p99": get(serving, "plain", rate, "p99_latency_s")}
+            rate: {k: x for k, x in (("served_p50", v.get("p50_latency_s")), ("served_p99", v.get("p99_latency_s")),
+                                      ("shortest_first_p50", get(serving, "shortest_first", rate, "p50_latency_s")),
+                                      ("shortest_first_p99", get(serving, "shortest_first", rate, "p99_latency_s")),
+                                      ("plain_p50", get(serving, "plain", rate, "p50_latency_s")),
+                                      ("plain_p99", get(serving, "plain", rate, "p99_latency_s"))) if x is not None}
             for rate, v in serving["served"].items() if isinstance(v, dict)}
+        out["serving_jobs_per_rate"] = serving.get("jobs_per_rate")
     return out
 
 
@@ -720,6 +727,7 @@ def b200_arm(args):
                      "algorithmic_bytes_per_launch": per_launch_bytes,
                      "bytes_model": f"{TRACE_ALGO_BYTES_PER_RAY} B/ray (ray in, material-queue entry out, every ray counted as a hit) + {NODE_BYTES} B/node visited + {TRIANGLE_BYTES} B/triangle tested",
                      "traffic_source": "ncu DRAM bytes per ray of a full-pool launch (profiles/trace_closest_spheres1m.json) x this run's rays per launch",
+                     "rays_per_launch": rays / iters,
                      "node_visits_per_ray": visits / max(rays, 1), "triangle_tests_per_ray": tests / max(rays, 1),
                      "avg_launch_ms": per_launch_s * 1000.0,
                      "avg_launch_ms_source": "CUDA events around each closest-hit launch of one host-looped frame of the same workload",
@@ -777,7 +785,8 @@ def b200_arm(args):
     if "serving" in sections:
         rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
         line["serving"] = run_section("serving", lambda: serving_section(knobs, rates, args.serve_jobs, args.serve_pool,
-                                                                           short_seconds=args.serve_short_seconds))
+                                                                           short_seconds=args.serve_short_seconds,
+                                                                           shortest_first=args.serve_shortest_first))
     if "precision" in sections:
         pr = run_section("precision", lambda: precision_section(knobs))
         line["precision"] = pr

@@ -152,6 +152,32 @@ def test_two_class_schedule_keeps_long_jobs_in_submission_order(resident, frame_
         srv.close()
 
 
+def test_two_class_admission_keeps_room_for_short_jobs(resident, frame_renderers):
+    """Two classes under a tight budget: with one long job admitted and the next long job waiting for
+    memory, a short job submitted after both is admitted at once from the eighth of the budget that
+    long jobs leave free, instead of queueing behind the waiting long job. The long jobs keep their
+    order, and every image equals the frame renderer's."""
+    # about 1.25 MB for a long job (64 B x 4096 in-flight paths, a ring of 2 passes of 16,384 pixels,
+    # accumulator and framebuffer), 30 kB for the short one: one long job fits in 7/8 of the budget, two do not
+    budget = 1_450_000
+    srv, ids = make_server(resident, pool_size=4096, schedule=pathtracer.SCHEDULE_TWO_CLASS, short_job_seconds=1e-5,
+                           hbm_budget_bytes=budget)
+    try:
+        long_job = ("spheres-small", 128, 128, 16, 10, True, 0)   # 262,144 paths
+        small = ("cornell-all", 16, 16, 1, 6, True, 0)            # 256 paths
+        j_a = submit(srv, ids, resident, long_job)
+        j_b = submit(srv, ids, resident, long_job)
+        j_s = submit(srv, ids, resident, small)
+        for j, job in ((j_a, long_job), (j_b, long_job), (j_s, small)):
+            check_job(srv, j, frame_renderers, resident, job)
+        done = {j: srv.poll(j)["done_s"] for j in (j_a, j_b, j_s)}
+        assert done[j_s] < done[j_a] < done[j_b]
+        assert srv.poll(j_s)["admit_s"] < srv.poll(j_b)["admit_s"]
+        assert srv.stats()["admitted_high_water"] <= budget
+    finally:
+        srv.close()
+
+
 def test_deadline_schedule_does_not_pass_over_a_late_job(resident, frame_renderers):
     """With a deadline of one render time (slowdown 1), a large job that has waited past it ranks
     before small jobs submitted later: it finishes before the last of a stream of small jobs."""
