@@ -27,6 +27,9 @@ On one GPU the line also carries (--sections, default all):
   precision  8M-triangle scene at 3840x2160, 16 spp, depth 10: BVH8 with 8-bit quantised boxes
              against the binary FP32 BVH (node bytes per ray, traversal Mrays/s), and the FP32 Kahan
              accumulation against FP64 accumulation of the same per-sample radiance (RMSE)
+  lights     power-weighted against area-weighted light selection at equal paths (RMSE)
+  bvh        the BVH8 built on the host against the same format built on the device: build seconds,
+             traversal work and frame time on the C2 and C4 frames, identical images
 """
 import argparse
 import json
@@ -85,7 +88,7 @@ def parse():
     return ap.parse_args()
 
 
-SECTIONS = ("plain", "cornell", "batched", "serving", "precision", "lights")
+SECTIONS = ("plain", "cornell", "batched", "serving", "precision", "lights", "bvh")
 
 
 def wanted_sections(args):
@@ -442,6 +445,41 @@ def serving_section(knobs, rates, n_jobs, max_pool, schedule_served=0, short_sec
     return out
 
 
+def bvh_build_section(knobs, cases=(("spheres-1m", 1920, 1080, 64, 12), ("spheres-8m", 3840, 2160, 16, 10)), frames=2):
+    """The BVH8 built on the host (binned SAH on all host threads) against the same format built on the
+    device (Morton order, clustering, the same 8-wide collapse): build seconds, tree size, traversal
+    work and frame time on the headline frame of each scene, and whether the images are identical."""
+    import pathtracer
+    import scenes
+    out = {"what": "host: binned SAH + surface-area-optimal collapse on all host threads; device: Morton order, "
+                   "PLOC clustering (radius 16), the same collapse and quantisation on the GPU"}
+    for name, W, H, spp, depth in cases:
+        s = scenes.config_scene(name)
+        cam = scenes.scene_camera(s, W, H)
+        res, images = {}, {}
+        for label, build in (("host", pathtracer.BVH_BUILD_HOST), ("device", pathtracer.BVH_BUILD_DEVICE)):
+            r = pathtracer.Renderer(0)
+            try:
+                r.set_bvh_build(build)
+                r.upload_scene(s)
+                times = r.upload_times()
+                info = r.scene_info()
+                r.render_frame(cam, W, H, spp, depth, True, **knobs)
+                stats = [r.render_frame(cam, W, H, spp, depth, True, **knobs) for _ in range(frames)]
+                ms = sum(st["device_ms"] for st in stats) / frames
+                images[label] = r.framebuffer()
+                res[label] = {"bvh_build_s": times["bvh_build_s"], "upload_s": times["upload_s"], "nodes": info["nodes"],
+                              "depth": info["depth"], "ms_per_frame": ms, "paths_per_second": stats[-1]["samples"] / (ms / 1000.0),
+                              "traversal": traversal_summary(stats[-1], pathtracer.NODE_BYTES[pathtracer.BVH8_Q8])}
+            finally:
+                r.close()
+        res["identical_images"] = bool(np.array_equal(images["host"], images["device"]))
+        res["build_speedup"] = res["host"]["bvh_build_s"] / res["device"]["bvh_build_s"]
+        res["config"] = f"{s.triangle_count} triangles, {W}x{H}, {spp} spp, depth {depth}, NEE"
+        out[name] = res
+    return out
+
+
 def precision_section(knobs):
     """8M-triangle scene, 3840x2160, 16 spp, depth 10: quantised BVH8 against binary FP32 BVH, and
     FP32 Kahan accumulation against FP64 accumulation of the same per-sample radiance."""
@@ -516,7 +554,9 @@ def summary(line):
            "batched_speedup_vs_plain_form": get(line, "batched", "speedup_vs_plain_form"),
            "power_sampling_samples_for_equal_rmse_c2": get(line, "light_sampling", "spheres-1m", "power", "samples_for_equal_rmse_vs_area"),
            "power_sampling_samples_for_equal_rmse_c4": get(line, "light_sampling", "spheres-8m", "power", "samples_for_equal_rmse_vs_area"),
-           "cpu_baseline_value": get(line, "cpu_baseline", "value")}
+           "cpu_baseline_value": get(line, "cpu_baseline", "value"),
+           "bvh_build_s_host_device": {n: [get(line, "bvh_build", n, "host", "bvh_build_s"), get(line, "bvh_build", n, "device", "bvh_build_s")]
+                                       for n in ("spheres-1m", "spheres-8m") if get(line, "bvh_build", n) is not None}}
     serving = line.get("serving")
     if isinstance(serving, dict) and isinstance(serving.get("served"), dict):
         out["serving_latency_s"] = {
@@ -795,6 +835,8 @@ def b200_arm(args):
                                        "config": "3840x2160, 16 spp, depth 10, NEE"}
     if "lights" in sections:
         line["light_sampling"] = run_section("lights", lambda: light_sampling_section(knobs))
+    if "bvh" in sections:
+        line["bvh_build"] = run_section("bvh", lambda: bvh_build_section(knobs))
     if sections:
         line["per_scene"] = per_scene
         line["section_seconds"] = timings

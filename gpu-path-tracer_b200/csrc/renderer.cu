@@ -23,6 +23,7 @@
 
 #include "../../include/gpt_b200.h"
 #include "bvh8.hpp"
+#include "bvh_device.hpp"
 #include "kernels.h"
 #include "runtime.hpp"
 
@@ -137,8 +138,8 @@ namespace pt
     }
 
     // Scene upload of Renderer::InitializeSceneBuffers (Renderer.cpp:292-306): validation, image textures,
-    // BVH8 (host), shading records, light list and alias table (device).
-    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary)
+    // BVH8 (host or device), shading records, light list and alias table (device).
+    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary, bool deviceBvh)
     {
         if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
             d.material_count == 0)
@@ -188,30 +189,52 @@ namespace pt
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materialTextures.get<void>(), slots.data(), slots.size() * sizeof(MaterialTextures),
                                                        cudaMemcpyHostToDevice, stream));
         }
-        // BVH8 on the host (binned SAH, collapse, quantisation).
-        Bvh8 bvh;
+        // Vertex positions go up first: the device BVH build and the shading records read them.
+        DeviceBuffer pos, nrm, tan, uv, mid;
+        PT_TRY(pos.allocate(static_cast<size_t>(n) * 9 * 4));
+        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(pos.get<void>(), d.positions, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream));
+        scene->triangleCount = n;
+        scene->materialCount = d.material_count;
+        scene->deviceBvh = deviceBvh;
         const auto tBvh = std::chrono::steady_clock::now();
-        try
+        Bvh8 bvh;
+        if (deviceBvh)
         {
-            bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), withBinary);
+            // BVH8 on the device (Morton order, clustering, collapse, quantisation); no binary BVH
+            DeviceBuffer modelsDev;
+            PT_TRY(modelsDev.allocate(static_cast<size_t>(n) * 4));
+            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(modelsDev.get<void>(), models.data(), static_cast<size_t>(n) * 4, cudaMemcpyHostToDevice, stream));
+            DeviceBvh dev;
+            PT_TRY(BuildBvh8Device(pos.get<float>(), modelsDev.get<uint32_t>(), n, stream, dev));
+            scene->nodes.swap(dev.nodes);
+            scene->tris.swap(dev.tris);
+            scene->nodeCount = dev.nodeCount;
+            scene->depth = dev.depth;
+            withBinary = false;
         }
-        catch (const std::exception& e)
+        else
         {
-            return Status::Err(GPT_ERR_INVALID_ARGUMENT, std::string("BVH build failed: ") + e.what());
+            // BVH8 on the host (binned SAH, collapse, quantisation).
+            try
+            {
+                bvh = BuildBvh8(d.positions, models.data(), n, static_cast<int>(std::max(1u, std::thread::hardware_concurrency())), withBinary);
+            }
+            catch (const std::exception& e)
+            {
+                return Status::Err(GPT_ERR_INVALID_ARGUMENT, std::string("BVH build failed: ") + e.what());
+            }
+            if (bvh.depth > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "BVH8 deeper than the traversal stack");
+            if (bvh.nodes.size() >= (1u << 24)) return Status::Err(GPT_ERR_CAPACITY, "BVH8 has more than 2^24 nodes");
+            scene->nodeCount = static_cast<uint32_t>(bvh.nodes.size());
+            scene->depth = bvh.depth;
+            PT_TRY(scene->nodes.allocate(bvh.nodes.size() * sizeof(Node8)));
+            PT_TRY(scene->tris.allocate(bvh.tris.size() * sizeof(float4)));
+            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes.get<void>(), bvh.nodes.data(), bvh.nodes.size() * sizeof(Node8), cudaMemcpyHostToDevice, stream));
+            PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
         }
         scene->bvhSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tBvh).count();
-        if (bvh.depth > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "BVH8 deeper than the traversal stack");
-        if (bvh.nodes.size() >= (1u << 24)) return Status::Err(GPT_ERR_CAPACITY, "BVH8 has more than 2^24 nodes");
-        scene->nodeCount = static_cast<uint32_t>(bvh.nodes.size());
-        scene->triangleCount = n;
-        scene->depth = bvh.depth;
-        scene->materialCount = d.material_count;
-        PT_TRY(scene->nodes.allocate(bvh.nodes.size() * sizeof(Node8)));
-        PT_TRY(scene->tris.allocate(bvh.tris.size() * sizeof(float4)));
         PT_TRY(scene->shading.allocate(static_cast<size_t>(n) * 9 * sizeof(float4)));
         PT_TRY(scene->materials.allocate(static_cast<size_t>(d.material_count) * sizeof(MaterialDev)));
-        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->nodes.get<void>(), bvh.nodes.data(), bvh.nodes.size() * sizeof(Node8), cudaMemcpyHostToDevice, stream));
-        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
         if (withBinary)
         {
             if (bvh.depth2 > kMaxStack) return Status::Err(GPT_ERR_CAPACITY, "Binary BVH deeper than the traversal stack");
@@ -223,13 +246,10 @@ namespace pt
         }
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->materials.get<void>(), d.materials, static_cast<size_t>(d.material_count) * sizeof(MaterialDev), cudaMemcpyHostToDevice, stream));
         // Vertex attributes go up once; shading records, lights and the alias table are built on the device.
-        DeviceBuffer pos, nrm, tan, uv, mid;
-        PT_TRY(pos.allocate(static_cast<size_t>(n) * 9 * 4));
         PT_TRY(nrm.allocate(static_cast<size_t>(n) * 9 * 4));
         PT_TRY(tan.allocate(static_cast<size_t>(n) * 12 * 4));
         PT_TRY(uv.allocate(static_cast<size_t>(n) * 6 * 4));
         PT_TRY(mid.allocate(static_cast<size_t>(n) * 4));
-        PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(pos.get<void>(), d.positions, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(nrm.get<void>(), d.normals, static_cast<size_t>(n) * 36, cudaMemcpyHostToDevice, stream));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(tan.get<void>(), d.tangents, static_cast<size_t>(n) * 48, cudaMemcpyHostToDevice, stream));
         PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(uv.get<void>(), d.uvs, static_cast<size_t>(n) * 24, cudaMemcpyHostToDevice, stream));
@@ -404,7 +424,7 @@ namespace pt
             if (rendering_.load()) return Status::Err(GPT_ERR_STATE, "Cannot upload a scene while rendering");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             std::unique_ptr<SceneGpu> scene;
-            PT_TRY(BuildScene(d, stream_, scene, true));
+            PT_TRY(BuildScene(d, stream_, scene, true, bvhBuild_ == GPT_BVH_BUILD_DEVICE));
             releaseGraph();
             scene->version = ++sceneVersion_;
             scene_ = std::move(scene);
@@ -986,6 +1006,7 @@ namespace pt
         mutable std::mutex errorMutex_;
         std::string lastError_;
         bool hasError_ = false;
+        uint32_t bvhBuild_ = GPT_BVH_BUILD_HOST;  // where the next scene upload builds its BVH8
     };
 }
 
@@ -1242,6 +1263,43 @@ extern "C"
         if (!r->impl->scene_) return GPT_ERR_NO_SCENE;
         if (bvh_build_seconds) *bvh_build_seconds = r->impl->scene_->bvhSeconds;
         if (upload_seconds) *upload_seconds = r->impl->scene_->uploadSeconds;
+        return GPT_OK;
+    }
+
+    int gpt_set_bvh_build(gpt_renderer* r, uint32_t build)
+    {
+        if (!r) return GPT_ERR_INVALID_ARGUMENT;
+        if (build > GPT_BVH_BUILD_DEVICE) return Report(r, pt::Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown BVH build"));
+        r->impl->bvhBuild_ = build;
+        return GPT_OK;
+    }
+
+    int gpt_check_bvh(gpt_renderer* r, const float* positions, uint32_t triangle_count, uint64_t* containment_violations,
+                      uint64_t* triangles_not_exactly_once, uint64_t* leaf_triangles)
+    {
+        if (!r || !positions) return GPT_ERR_INVALID_ARGUMENT;
+        const pt::SceneGpu* sc = r->impl->scene_.get();
+        if (!sc) return GPT_ERR_NO_SCENE;
+        if (triangle_count != sc->triangleCount)
+            return Report(r, pt::Status::Err(GPT_ERR_INVALID_ARGUMENT, "Triangle count differs from the uploaded scene"));
+        pt::Bvh8 b;
+        b.nodes.resize(sc->nodeCount);
+        b.tris.resize(static_cast<size_t>(sc->triangleCount) * pt::kTriangleVec4);
+        b.depth = sc->depth;
+        cudaError_t e = cudaSetDevice(r->impl->device_);
+        if (e == cudaSuccess) e = cudaMemcpy(b.nodes.data(), sc->nodes.get<void>(), b.nodes.size() * sizeof(pt::Node8), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(b.tris.data(), sc->tris.get<void>(), b.tris.size() * sizeof(float4), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return Report(r, pt::CudaStatus("cudaMemcpy", e));
+        b.order.resize(sc->triangleCount);
+        for (uint32_t k = 0; k < sc->triangleCount; k++)
+        {
+            const float w = b.tris[static_cast<size_t>(k) * pt::kTriangleVec4].w;  // input index of leaf position k
+            std::memcpy(&b.order[k], &w, 4);
+        }
+        const pt::Bvh8Check c = pt::CheckBvh8(b, positions, triangle_count);
+        if (containment_violations) *containment_violations = c.containmentViolations;
+        if (triangles_not_exactly_once) *triangles_not_exactly_once = c.trianglesNotExactlyOnce;
+        if (leaf_triangles) *leaf_triangles = c.leafTriangles;
         return GPT_OK;
     }
 

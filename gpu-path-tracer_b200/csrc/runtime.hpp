@@ -108,7 +108,8 @@ namespace pt
         uint32_t nodeCount2 = 0, depth2 = 0;  // binary FP32 BVH, built when the scene is uploaded with it
         bool modelPresent[kModelCount] = {};
         uint64_t version = 0;
-        double bvhSeconds = 0.0, uploadSeconds = 0.0;  // host BVH build; whole upload (wall clock)
+        double bvhSeconds = 0.0, uploadSeconds = 0.0;  // BVH build (host or device); whole upload (wall clock)
+        bool deviceBvh = false;                         // the BVH8 was built on the device
         SceneView view() const
         {
             SceneView v{};
@@ -132,7 +133,9 @@ namespace pt
 
     // Minimal PNG writer (zlib deflate) for SaveRenderedFrame (Renderer.cpp:649-675): RGBA8, rows
     // flipped vertically like Import::FlipVertically.
-    // Validates a scene description and builds its device copy: image textures, BVH8 (host build),
-    // shading records, light list and alias table; with `withBinary` also the binary FP32 BVH.
-    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary = false);
+    // Validates a scene description and builds its device copy: image textures, BVH8, shading records,
+    // light list and alias table. The BVH8 is built on the host (binned SAH), with `withBinary` also the
+    // binary FP32 BVH, or with `deviceBvh` on the device (clustering; no binary BVH).
+    Status BuildScene(const gpt_scene_desc& d, cudaStream_t stream, std::unique_ptr<SceneGpu>& out, bool withBinary = false,
+                      bool deviceBvh = false);
 }

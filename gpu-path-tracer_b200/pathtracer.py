@@ -80,6 +80,7 @@ LOOP_GRAPH, LOOP_HOST = 0, 1
 RNG_PHILOX, RNG_PCG32 = 0, 1
 LIGHTS_AREA, LIGHTS_POWER = 0, 1
 BVH8_Q8, BVH2_FP32 = 0, 1
+BVH_BUILD_HOST, BVH_BUILD_DEVICE = 0, 1
 WAVEFRONT_B200, WAVEFRONT_QUEUES = 0, 1
 SCHEDULE_SHORTEST_FIRST, SCHEDULE_OLDEST_FIRST, SCHEDULE_DEADLINE, SCHEDULE_TWO_CLASS = 1, 2, 3, 4
 NODE_BYTES = {BVH8_Q8: 64 + 4, BVH2_FP32: 64}  # bytes a node visit reads: BVH8 header + its child reference; the whole binary node
@@ -178,6 +179,9 @@ _SIGNATURES = [
                                              ctypes.POINTER(ctypes.c_uint32)]),
     ("gpt_scene_upload_times", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                               ctypes.POINTER(ctypes.c_double)]),
+    ("gpt_set_bvh_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("gpt_check_bvh", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64),
+                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     ("gpt_read_alias_table", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_read_alias_table_power", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_inject_allocation_failure", ctypes.c_int, [ctypes.c_uint32]),
@@ -305,10 +309,22 @@ class Renderer:
                     binary_depth=d2.value)
 
     def upload_times(self) -> dict:
-        """Seconds of the last upload: host BVH build, and the whole upload."""
+        """Seconds of the last upload: the BVH build (host or device), and the whole upload."""
         b, u = ctypes.c_double(), ctypes.c_double()
         self._check(self.L.gpt_scene_upload_times(self.h, ctypes.byref(b), ctypes.byref(u)), "gpt_scene_upload_times")
         return dict(bvh_build_s=b.value, upload_s=u.value)
+
+    def set_bvh_build(self, build: int):
+        """Where the next upload_scene builds the BVH8: BVH_BUILD_HOST (default) or BVH_BUILD_DEVICE."""
+        self._check(self.L.gpt_set_bvh_build(self.h, build), "gpt_set_bvh_build")
+
+    def check_bvh(self, scene) -> dict:
+        """Host check of the uploaded BVH8 against the scene's positions (gpt_check_bvh)."""
+        pos = np.ascontiguousarray(scene.positions, dtype=np.float32)
+        a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+        self._check(self.L.gpt_check_bvh(self.h, _ptr(pos), pos.shape[0], ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                    "gpt_check_bvh")
+        return dict(containment_violations=a.value, triangles_not_exactly_once=b.value, leaf_triangles=c.value)
 
     def alias_table(self, power: bool = False) -> np.ndarray:
         """[lights, 4] words (q, p, alias, value): the area-weighted table, or with power=True the

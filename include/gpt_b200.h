@@ -296,11 +296,27 @@ int gpt_scene_info(const gpt_renderer* renderer, uint32_t* node_count, uint32_t*
 /* Node count and depth of the scene's binary FP32 BVH (HostBvh.cpp:22-100 builds the reference's
  * binary tree by median splits; this one is the binned-SAH tree the BVH8 is collapsed from). */
 int gpt_scene_info_binary(const gpt_renderer* renderer, uint32_t* node_count, uint32_t* depth);
-/* Wall-clock seconds of the last scene upload: the host BVH build (binned SAH, 8-wide collapse,
- * quantisation; all host threads) and the whole gpt_init_scene_buffers call, which adds validation,
+/* Wall-clock seconds of the last scene upload: the BVH build (on the host: binned SAH, 8-wide
+ * collapse, quantisation on all host threads; or on the device, gpt_set_bvh_build) and the whole
+ * gpt_init_scene_buffers call, which adds validation,
  * textures, host-to-device copies and the device-built shading records, lights and alias tables
  * (Renderer.cpp:292-306 is the reference's upload; it reports no timings). */
 int gpt_scene_upload_times(const gpt_renderer* renderer, double* bvh_build_seconds, double* upload_seconds);
+
+/* Where the next gpt_init_scene_buffers builds the BVH8 (the reference builds it on the host,
+ * HostBvh.cpp, with median splits). GPT_BVH_BUILD_HOST (default): binned SAH on all host threads,
+ * plus the binary FP32 BVH of GPT_BVH2_FP32. GPT_BVH_BUILD_DEVICE: on the GPU (Morton order,
+ * clustering of nearest neighbours, the same 8-wide collapse and quantisation), no binary BVH (frames
+ * with GPT_BVH2_FP32 are refused). Hits, and so frames, do not depend on the builder; traversal work
+ * does. */
+#define GPT_BVH_BUILD_HOST 0u
+#define GPT_BVH_BUILD_DEVICE 1u
+int gpt_set_bvh_build(gpt_renderer* renderer, uint32_t build);
+/* Structural check of the uploaded BVH8 against the scene's positions ([n][3][3], the ones uploaded),
+ * on the host: quantised child boxes not containing their subtree (exact arithmetic), triangles not
+ * referenced exactly once, and triangles in leaves. */
+int gpt_check_bvh(gpt_renderer* renderer, const float* positions, uint32_t triangle_count, uint64_t* containment_violations,
+                  uint64_t* triangles_not_exactly_once, uint64_t* leaf_triangles);
 /* The light alias table built on the device, [lights][4] words (q, p, alias, value)
  * (AliasTableView.hpp:8-14). */
 int gpt_read_alias_table(gpt_renderer* renderer, uint32_t* bins, uint32_t count);
