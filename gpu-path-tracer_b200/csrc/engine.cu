@@ -279,6 +279,7 @@ namespace pt
         Status Init()
         {
             if (cfg_.schedule > GPT_SCHEDULE_TWO_CLASS) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown schedule");
+            if (cfg_.bvh_build > GPT_BVH_BUILD_DEVICE) return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown BVH build");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
             PT_CUDA("cudaStreamCreateWithFlags", cudaStreamCreateWithFlags(&copyStream_, cudaStreamNonBlocking));
@@ -341,7 +342,7 @@ namespace pt
             if (!pending_.empty() || !active_.empty()) return Status::Err(GPT_ERR_STATE, "Scenes are added while no job is queued or running");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             std::unique_ptr<SceneGpu> scene;
-            PT_TRY(BuildScene(d, stream_, scene));
+            PT_TRY(BuildScene(d, stream_, scene, false, cfg_.bvh_build == GPT_BVH_BUILD_DEVICE));
             PT_TRY(AppendScene(pack_, *scene, stream_));
             releaseGraph();
             id = static_cast<uint32_t>(pack_.entry.size() - 1);

@@ -100,7 +100,7 @@ class gpt_server_config(ctypes.Structure):
                 ("ring_passes", ctypes.c_uint32), ("hbm_budget_bytes", ctypes.c_uint64), ("trace_block", ctypes.c_uint32),
                 ("trace_refill", ctypes.c_uint32), ("trace_occupancy", ctypes.c_uint32),
                 ("max_slice_iterations", ctypes.c_uint32), ("schedule", ctypes.c_uint32), ("deadline_slowdown", ctypes.c_float),
-                ("short_job_seconds", ctypes.c_float)]
+                ("short_job_seconds", ctypes.c_float), ("bvh_build", ctypes.c_uint32)]
 
 
 class gpt_job_desc(ctypes.Structure):
@@ -651,12 +651,12 @@ class Server:
     def __init__(self, device: int = 0, pool_size: int = 0, max_jobs: int = 0, max_active_jobs: int = 0,
                  ring_passes: int = 0, hbm_budget_bytes: int = 0, trace_block: int = 0, trace_refill: int = 0,
                  trace_occupancy: int = 0, max_slice_iterations: int = 0, schedule: int = 0, deadline_slowdown: float = 0.0,
-                 short_job_seconds: float = 0.0,
+                 short_job_seconds: float = 0.0, bvh_build: int = 0,
                  variant: str = "product"):
         self.L = lib(variant)
         cfg = gpt_server_config(pool_size, max_jobs, max_active_jobs, ring_passes, hbm_budget_bytes, trace_block,
                                 trace_refill, trace_occupancy, max_slice_iterations, schedule, deadline_slowdown,
-                                short_job_seconds)
+                                short_job_seconds, bvh_build)
         h = ctypes.c_void_p()
         rc = self.L.gpt_server_create(ctypes.byref(h), device, ctypes.byref(cfg))
         if rc != 0:

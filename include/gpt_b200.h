@@ -427,6 +427,8 @@ typedef struct gpt_server_config {
                                       first, and a large job is not passed over past its deadline) */
     float deadline_slowdown;       /* GPT_SCHEDULE_DEADLINE: deadline in units of the job's own render time (0 = 4) */
     float short_job_seconds;       /* GPT_SCHEDULE_TWO_CLASS: render time alone below which a job is short (0 = 0.05) */
+    uint32_t bvh_build;            /* where gpt_server_add_scene builds a scene's BVH8: GPT_BVH_BUILD_HOST (0) or
+                                      GPT_BVH_BUILD_DEVICE (see gpt_set_bvh_build) */
 } gpt_server_config;
 
 #define GPT_SCHEDULE_SHORTEST_FIRST 1u

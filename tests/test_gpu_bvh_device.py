@@ -111,6 +111,33 @@ def test_device_bvh_of_a_few_triangles(device_renderer, host_renderer, scene_fac
     assert np.array_equal(uvt_d.view(np.uint32), uvt_h.view(np.uint32))
 
 
+def test_job_server_with_device_built_scenes(host_renderer, scene_factory):
+    """The job server building its scenes' BVH8 on the device: jobs over two resident scenes give the
+    frame renderer's (host-built BVH) images bit for bit."""
+    names = ["cornell-all", "spheres-small"]
+    srv = P.Server(0, pool_size=1 << 16, bvh_build=P.BVH_BUILD_DEVICE, hbm_budget_bytes=1 << 30, variant="det")
+    try:
+        ids = {n: srv.add_scene(scene_factory(n)) for n in names}
+        jobs = [("cornell-all", 40, 30, 4, 6), ("spheres-small", 64, 40, 4, 12), ("spheres-small", 31, 29, 1, 10)]
+        jids = []
+        for name, w, h, spp, depth in jobs:
+            cam = scenes.scene_camera(scene_factory(name), w, h)
+            jids.append(srv.submit(ids[name], cam, w, h, spp, depth, True, keep_accumulation=True))
+        for jid, (name, w, h, spp, depth) in zip(jids, jobs):
+            st = srv.wait(jid, 300)
+            assert st["state"] == "done", (name, st)
+            fb, acc = srv.result(jid, accumulation=True)
+            s = scene_factory(name)
+            host_renderer.upload_scene(s)
+            host_renderer.render_frame(scenes.scene_camera(s, w, h), w, h, spp, depth, True)
+            assert np.array_equal(acc.view(np.uint32), host_renderer.accumulation().reshape(-1, 4).view(np.uint32))
+            assert np.array_equal(fb, host_renderer.framebuffer().reshape(-1))
+    finally:
+        srv.close()
+    with pytest.raises(P.GptError):
+        P.Server(0, bvh_build=2)
+
+
 def test_device_bvh_at_benchmark_scale(device_renderer, host_renderer, scene_factory):
     """The 1.31M-triangle headline scene: a valid tree whose hits on 2^20 rays equal the host BVH's."""
     s = scene_factory("spheres-1m")
