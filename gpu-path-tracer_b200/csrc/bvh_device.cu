@@ -102,24 +102,39 @@ namespace pt
             return v;
         }
 
-        // Bounds of the partial bounds (one block), then the Morton code of every centroid.
-        __global__ void morton_kernel(const float4* cent, uint32_t n, const float4* partLo, const float4* partHi, uint32_t parts, uint32_t* keys,
-                                      uint32_t* values)
+        // One block of 256 threads: the bounds of the per-block bounds, into entry 0.
+        __global__ void bounds_final_kernel(float4* partLo, float4* partHi, uint32_t parts)
         {
-            __shared__ float4 bounds[2];
+            __shared__ float4 sLo[256], sHi[256];
+            float4 lo = partLo[0], hi = partHi[0];
+            for (uint32_t i = threadIdx.x; i < parts; i += blockDim.x)
+            {
+                lo = fmin4(lo, partLo[i]);
+                hi = fmax4(hi, partHi[i]);
+            }
+            sLo[threadIdx.x] = lo;
+            sHi[threadIdx.x] = hi;
+            __syncthreads();
+            for (uint32_t s = blockDim.x / 2; s > 0; s >>= 1)
+            {
+                if (threadIdx.x < s)
+                {
+                    sLo[threadIdx.x] = fmin4(sLo[threadIdx.x], sLo[threadIdx.x + s]);
+                    sHi[threadIdx.x] = fmax4(sHi[threadIdx.x], sHi[threadIdx.x + s]);
+                }
+                __syncthreads();
+            }
             if (threadIdx.x == 0)
             {
-                float4 lo = partLo[0], hi = partHi[0];
-                for (uint32_t i = 1; i < parts; i++)
-                {
-                    lo = fmin4(lo, partLo[i]);
-                    hi = fmax4(hi, partHi[i]);
-                }
-                bounds[0] = lo;
-                bounds[1] = hi;
+                partLo[0] = sLo[0];
+                partHi[0] = sHi[0];
             }
-            __syncthreads();
-            const float4 lo = bounds[0], hi = bounds[1];
+        }
+
+        // The Morton code of every centroid within the centroids' bounds.
+        __global__ void morton_kernel(const float4* cent, uint32_t n, const float4* boundsLo, const float4* boundsHi, uint32_t* keys, uint32_t* values)
+        {
+            const float4 lo = boundsLo[0], hi = boundsHi[0];
             const float ex = hi.x - lo.x, ey = hi.y - lo.y, ez = hi.z - lo.z;
             const float sx = ex > 0.0f ? 1023.0f / ex : 0.0f, sy = ey > 0.0f ? 1023.0f / ey : 0.0f, sz = ez > 0.0f ? 1023.0f / ez : 0.0f;
             for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
@@ -615,7 +630,9 @@ namespace pt
         triangle_boxes_kernel<<<parts, 256, 0, s>>>(positions, n, triLo.get<float4>(), triHi.get<float4>(), cent.get<float4>(), partLo.get<float4>(),
                                                     partHi.get<float4>());
         PT_CUDA("triangle boxes", cudaGetLastError());
-        morton_kernel<<<grid_for(n, 256, 4096), 256, 0, s>>>(cent.get<float4>(), n, partLo.get<float4>(), partHi.get<float4>(), parts,
+        bounds_final_kernel<<<1, 256, 0, s>>>(partLo.get<float4>(), partHi.get<float4>(), parts);
+        PT_CUDA("centroid bounds", cudaGetLastError());
+        morton_kernel<<<grid_for(n, 256, 4096), 256, 0, s>>>(cent.get<float4>(), n, partLo.get<float4>(), partHi.get<float4>(),
                                                              keys.get<uint32_t>(), values.get<uint32_t>());
         PT_CUDA("morton codes", cudaGetLastError());
         size_t tb = temp.bytes();

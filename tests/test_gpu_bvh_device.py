@@ -138,9 +138,11 @@ def test_job_server_with_device_built_scenes(host_renderer, scene_factory):
         P.Server(0, bvh_build=2)
 
 
-def test_device_bvh_at_benchmark_scale(device_renderer, host_renderer, scene_factory):
-    """The 1.31M-triangle headline scene: a valid tree whose hits on 2^20 rays equal the host BVH's."""
-    s = scene_factory("spheres-1m")
+@pytest.mark.parametrize("name", ["spheres-1m", "spheres-8m"])
+def test_device_bvh_at_benchmark_scale(device_renderer, host_renderer, scene_factory, name):
+    """The 1.31M-triangle headline scene and the 8.19M-triangle precision scene: valid trees whose hits
+    on 2^20 rays equal the host BVH's."""
+    s = scene_factory(name)
     device_renderer.upload_scene(s)
     t_device = device_renderer.upload_times()["bvh_build_s"]
     host_renderer.upload_scene(s)
