@@ -475,6 +475,9 @@ namespace pt
             return Status::Ok();
         }
 
+        // GPT_LOOP_GRAPH or GPT_LOOP_HOST for the slices launched from now on.
+        void SetLoopMode(uint32_t mode) { loopMode_.store(mode); }
+
         Status Cancel(uint64_t id)
         {
             std::scoped_lock lock(mu_);
@@ -570,6 +573,34 @@ namespace pt
             graph_ = nullptr;
         }
 
+        // The launch parameters of one engine iteration: inside the slice graph's WHILE node
+        // (graphLoop, with its conditional handle) or launched from the host (GPT_LOOP_HOST).
+        EngineLaunch iterationLaunch(int sms, bool graphLoop, cudaGraphConditionalHandle handle)
+        {
+            EngineLaunch L{};
+            L.scene = pack_.view();
+            L.wf = wavefront();
+            L.ev = engineView();
+            L.handle = handle;
+            for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = pack_.modelPresent[m];
+            L.anyLights = pack_.lightCount > 0;
+            L.traceThreads = threads_;
+            L.occupancy = occupancy_;
+            L.traceBlocks = trace_grid_blocks(device_, threads_, pack_.depth, occupancy_);
+            L.refill = refill_;
+            L.refillShadow = refillShadow_;
+            L.shadeBlocks = sms * 8;
+            L.sms = sms;
+            L.graphLoop = graphLoop;
+            L.shadeFork = shadeFork_;
+            for (uint32_t m = 0; m < kModelCount; m++)
+            {
+                L.shadeJoin[m] = shadeJoin_[m];
+                L.shadeStreams[m] = shadeStreams_[m];
+            }
+            return L;
+        }
+
         Status buildGraph()
         {
             releaseGraph();
@@ -586,27 +617,7 @@ namespace pt
             cudaGraphNode_t whileNode;
             PT_CUDA("cudaGraphAddNode", cudaGraphAddNode(&whileNode, graph_, nullptr, 0, &cp));
             cudaGraph_t body = cp.conditional.phGraph_out[0];
-            EngineLaunch L{};
-            L.scene = pack_.view();
-            L.wf = wavefront();
-            L.ev = engineView();
-            L.handle = handle;
-            for (uint32_t m = 0; m < kModelCount; m++) L.modelPresent[m] = pack_.modelPresent[m];
-            L.anyLights = pack_.lightCount > 0;
-            L.traceThreads = threads_;
-            L.occupancy = occupancy_;
-            L.traceBlocks = trace_grid_blocks(device_, threads_, pack_.depth, occupancy_);
-            L.refill = refill_;
-            L.refillShadow = refillShadow_;
-            L.shadeBlocks = sms * 8;
-            L.sms = sms;
-            L.graphLoop = true;
-            L.shadeFork = shadeFork_;
-            for (uint32_t m = 0; m < kModelCount; m++)
-            {
-                L.shadeJoin[m] = shadeJoin_[m];
-                L.shadeStreams[m] = shadeStreams_[m];
-            }
+            const EngineLaunch L = iterationLaunch(sms, true, handle);
             PT_CUDA("cudaStreamBeginCaptureToGraph", cudaStreamBeginCaptureToGraph(stream_, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             const cudaError_t le = launch_engine_iteration(L, stream_);
             const cudaError_t ce = cudaStreamEndCapture(stream_, &body);
@@ -774,12 +785,24 @@ namespace pt
         }
 
         // Under mu_: one graph launch, then the counters and the job table come back (queued on the
-        // render stream; waitSlice collects them).
+        // render stream; waitSlice collects them). With GPT_LOOP_HOST the slice's iterations are
+        // launched one by one by waitSlice instead.
         Status launchSlice()
         {
+            hostSlice_ = loopMode_.load() == GPT_LOOP_HOST;
+            if (hostSlice_)
+            {
+                PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
+                return Status::Ok();
+            }
             if (!graphExec_) PT_TRY(buildGraph());
             PT_CUDA("cudaEventRecord", cudaEventRecord(startEvent_, stream_));
             PT_CUDA("cudaGraphLaunch", cudaGraphLaunch(graphExec_, stream_));
+            return readBack();
+        }
+
+        Status readBack()
+        {
             PT_CUDA("cudaEventRecord", cudaEventRecord(stopEvent_, stream_));
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(hostCounters_, counters_.get<void>(), sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(hostCtl_, ctl_.get<void>(), sizeof(EngineCtl), cudaMemcpyDeviceToHost, stream_));
@@ -787,9 +810,29 @@ namespace pt
             return Status::Ok();
         }
 
+        // Without mu_, GPT_LOOP_HOST: the slice's iterations as ordinary launches, the loop condition
+        // read after each (the graph's WHILE node reads it on the device). ncu profiles these kernels;
+        // it does not profile kernel nodes of graphs with conditional nodes.
+        Status hostLoopSlice()
+        {
+            int sms = 0;
+            PT_CUDA("cudaDeviceGetAttribute", cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device_));
+            const EngineLaunch L = iterationLaunch(sms, false, 0);
+            const uint64_t cap = uint64_t(cfg_.max_slice_iterations) + 1;
+            for (uint64_t it = 0; it < cap; it++)
+            {
+                PT_CUDA("engine iteration", launch_engine_iteration(L, stream_));
+                PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(&hostCounters_->done, &counters_.get<Counters>()->done, 4, cudaMemcpyDeviceToHost, stream_));
+                PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
+                if (hostCounters_->done) break;
+            }
+            return readBack();
+        }
+
         // Without mu_: waits for the slice launched by launchSlice.
         Status waitSlice()
         {
+            if (hostSlice_) PT_TRY(hostLoopSlice());
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
             float ms = 0.0f;
             PT_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, startEvent_, stopEvent_));
@@ -965,6 +1008,8 @@ namespace pt
         gpt_server_config cfg_;
         int threads_ = 128, occupancy_ = 10;
         uint32_t schedule_ = GPT_SCHEDULE_TWO_CLASS;
+        std::atomic<uint32_t> loopMode_{GPT_LOOP_GRAPH};  // slices as one graph launch, or iterations launched by the host
+        bool hostSlice_ = false;                          // the slice in flight runs its iterations from the host
         std::atomic<double> rateEstimate_{1e9};  // paths per second, smoothed (initial guess: one B200 on a mid-size scene); read by Submit
         uint64_t lastSliceSamples_ = 0;
         uint64_t rateSamples_ = 0;         // samples launched in the current rate window
@@ -1093,6 +1138,14 @@ extern "C"
     {
         if (!s) return GPT_ERR_INVALID_ARGUMENT;
         return ServerReport(s, s->impl->Cancel(id));
+    }
+
+    int gpt_server_set_loop_mode(gpt_server* s, uint32_t mode)
+    {
+        if (!s) return GPT_ERR_INVALID_ARGUMENT;
+        if (mode > GPT_LOOP_HOST) return ServerReport(s, pt::Status::Err(GPT_ERR_INVALID_ARGUMENT, "Unknown loop mode"));
+        s->impl->SetLoopMode(mode);
+        return GPT_OK;
     }
 
     int gpt_server_get_stats(gpt_server* s, gpt_server_stats* out)

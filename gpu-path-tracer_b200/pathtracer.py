@@ -209,6 +209,7 @@ _SIGNATURES = [
     ("gpt_server_read", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p]),
     ("gpt_server_release", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     ("gpt_server_cancel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("gpt_server_set_loop_mode", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
     ("gpt_server_get_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(gpt_server_stats)]),
     ("gpt_server_peek_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
 ]
@@ -723,6 +724,10 @@ class Server:
 
     def cancel(self, job: int):
         self._check(self.L.gpt_server_cancel(self.h, job), "gpt_server_cancel")
+
+    def set_loop_mode(self, mode: int):
+        """LOOP_GRAPH (default): a slice is one graph launch; LOOP_HOST: iterations launched by the host."""
+        self._check(self.L.gpt_server_set_loop_mode(self.h, mode), "gpt_server_set_loop_mode")
 
     def stats(self) -> dict:
         st = gpt_server_stats()

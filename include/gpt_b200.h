@@ -492,6 +492,12 @@ int gpt_server_release(gpt_server* server, uint64_t job_id);
 /* A queued job is dropped; a running one launches no more samples and ends as GPT_JOB_CANCELLED
  * (without an image) once its paths in flight finish. */
 int gpt_server_cancel(gpt_server* server, uint64_t job_id);
+/* How the server runs a slice: GPT_LOOP_GRAPH (default) as one CUDA graph whose conditional WHILE node
+ * repeats the engine iteration on the device, GPT_LOOP_HOST as one launch per kernel with the loop
+ * condition read on the host after every iteration (slower; for profilers, which do not profile kernel
+ * nodes of graphs with conditional nodes). Takes effect from the next slice; results do not change.
+ * No counterpart in the reference, which has no job server. */
+int gpt_server_set_loop_mode(gpt_server* server, uint32_t mode);
 int gpt_server_get_stats(gpt_server* server, gpt_server_stats* stats);
 int gpt_server_peek_last_error(gpt_server* server, char* buffer, size_t length);
 

@@ -109,6 +109,23 @@ def test_mixed_jobs_match_alone(resident, frame_renderers):
         srv.close()
 
 
+def test_host_loop_slices_match_frame_renderer(resident, frame_renderers):
+    """Slices whose iterations the host launches one by one (GPT_LOOP_HOST, the mode profilers can
+    see) give the same images as the graph slices, i.e. the frame renderer's."""
+    srv, ids = make_server(resident, pool_size=1 << 16)
+    try:
+        srv.set_loop_mode(pathtracer.LOOP_HOST)
+        jids = [submit(srv, ids, resident, job) for job in JOBS]
+        for jid, job in zip(jids, JOBS):
+            check_job(srv, jid, frame_renderers, resident, job)
+        srv.set_loop_mode(pathtracer.LOOP_GRAPH)
+        check_job(srv, submit(srv, ids, resident, JOBS[0]), frame_renderers, resident, JOBS[0])
+        with pytest.raises(pathtracer.GptError):
+            srv.set_loop_mode(7)
+    finally:
+        srv.close()
+
+
 @pytest.mark.parametrize("schedule", [pathtracer.SCHEDULE_SHORTEST_FIRST, pathtracer.SCHEDULE_OLDEST_FIRST,
                                       pathtracer.SCHEDULE_DEADLINE, pathtracer.SCHEDULE_TWO_CLASS])
 def test_schedule_orders_completion_not_images(resident, frame_renderers, schedule):
