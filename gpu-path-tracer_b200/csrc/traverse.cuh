@@ -12,7 +12,8 @@ namespace pt
     {
         float3 o, invd;
         float tmin;
-        uint32_t oct;   // bit k set when the ray's k-th direction component is negative
+        uint32_t oct;   // child visiting order: bit k set when the ray's k-th direction component is negative
+                        // (near to far); the any-hit kernel flips all three bits (far to near)
     };
 
     PT_HD float safe_inv(float dk)
