@@ -20,10 +20,11 @@ On one GPU the line also carries (--sections, default all):
   cornell    the Cornell box at 512x512, 16 spp, depth 8, NEE
   batched    64 uneven jobs over 4 resident scenes (10k-2M triangles) through the job server in one
              device loop, against the same jobs one at a time (server, frame renderer, plain form)
-  serving    open-loop Poisson arrivals (20, 50, 100 jobs/s) over 8 resident scenes (50k-4M
-             triangles): p50/p99 latency, paths/s and admitted-bytes high-water mark, served
-             (continuous batching: short jobs first, then the others in submission order; and shortest
-             remaining work first) against one job at a time
+  serving    open-loop Poisson arrivals (20, 50, 100 jobs/s; 200 per rate) over 8 resident scenes
+             (50k-4M triangles): p50/p99 latency, per-job slowdown, paths/s and admitted-bytes
+             high-water mark, served (continuous batching: short jobs first, then the others in
+             submission order; with --serve-shortest-first also shortest remaining work first) against
+             one job at a time in submission order
   precision  8M-triangle scene at 3840x2160, 16 spp, depth 10: BVH8 with 8-bit quantised boxes
              against the binary FP32 BVH (node bytes per ray, traversal Mrays/s), and the FP32 Kahan
              accumulation against FP64 accumulation of the same per-sample radiance (RMSE)

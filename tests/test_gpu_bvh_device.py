@@ -47,6 +47,7 @@ def test_device_bvh_is_valid_and_hits_equal_the_host_bvh(device_renderer, host_r
     device_renderer.upload_scene(s)
     host_renderer.upload_scene(s)
     check(device_renderer, s)
+    check(host_renderer, s)  # the same checker holds for the host-built tree
     info, host_info = device_renderer.scene_info(), host_renderer.scene_info()
     assert info["binary_nodes"] == 0 and host_info["binary_nodes"] > 0  # no binary FP32 BVH from the device build
     assert 0 < info["depth"] <= 64 and info["nodes"] > 0
