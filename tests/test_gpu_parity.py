@@ -439,3 +439,57 @@ def test_imported_obj_scene_renders_like_the_oracle(gpu_renderer, tmp_path):
     assert np.array_equal(gpu_renderer.queue_log(), ref["queue_log"])
     assert np.array_equal(gpu_renderer.sample_radiance().view(np.uint32), ref["sample_radiance"].view(np.uint32))
     assert np.array_equal(gpu_renderer.framebuffer(), ref["framebuffer"])
+
+
+def test_yaml_scene_file_renders_like_the_oracle(gpu_renderer, tmp_path):
+    """A scene file in the reference's YAML format (two OBJ models, a rotated parent, a scaled child,
+    a look-at camera) through scene_file.load_scene: the deterministic build renders it as the oracle
+    does, bit for bit."""
+    import scene_file
+    from test_obj_import import write_obj
+    root = tmp_path / "Assets"
+    for d in ("Models/Room", "Models/Ball", "Scenes"):
+        (root / d).mkdir(parents=True)
+    write_obj(scenes.cornell_all_models(1), str(root / "Models/Room"))
+    write_obj(scenes.sphere_field(1, 2, 2, 3, name="ball"), str(root / "Models/Ball"))
+    (root / "Scenes/room.yaml").write_text("""
+scene:
+    - components:
+        - type: Transform
+          translation: [0.5, 0.5, 2.2]
+          target: [0.5, 0.45, 0.0]
+          scale: [1.0, 1.0, 1.0]
+        - type: Camera
+          fov-y: 40.0
+          near-plane: 0.1
+          far-plane: 100.0
+    - components:
+        - type: Transform
+          translation: [0.5, 0.0, 0.5]
+          euler-degrees: [0.0, 10.0, 0.0]
+          scale: [1.0, 1.0, 1.0]
+      children:
+        - components:
+            - type: Transform
+              translation: [-0.5, 0.0, -0.5]
+              scale: [1.0, 1.0, 1.0]
+            - type: Model
+              path: Models/Room/scene.obj
+        - components:
+            - type: Transform
+              translation: [-0.2, 0.15, 0.1]
+              scale: [0.01, 0.01, 0.01]
+            - type: Model
+              path: Models/Ball/scene.obj
+""")
+    s = scene_file.load_scene(str(root / "Scenes/room.yaml"))
+    o = oracle.OracleScene(s)
+    gpu_renderer.upload_scene(s)
+    cam = scene_file.device_camera(s, 64, 48)
+    st = gpu_renderer.render_frame(cam, 64, 48, 4, 10, True)
+    ref = o.render(cam, 64, 48, 4, 10, True)
+    assert st["iterations"] == ref["iterations"]
+    assert np.array_equal(gpu_renderer.queue_log(), ref["queue_log"])
+    assert np.array_equal(gpu_renderer.sample_radiance().view(np.uint32), ref["sample_radiance"].view(np.uint32))
+    assert np.array_equal(gpu_renderer.framebuffer(), ref["framebuffer"])
+    assert np.count_nonzero(ref["framebuffer"]) > 0
