@@ -246,8 +246,16 @@ def _parse(root):
         if comps is not None:
             if not isinstance(comps, list):
                 raise SceneFileError("Entity 'components' must be a sequence")
+            seen = set()
             for c in comps:
                 kind = _get(c, "type", "str", e.index)
+                # The reference's registry holds one component of a type per entity, and Model and
+                # Grid both give the entity its Children list: a second one is not a defined scene.
+                slot = "Children" if kind in ("Model", "Grid") else kind
+                if slot in ("Transform", "Camera", "Children"):
+                    if slot in seen:
+                        raise SceneFileError(f"entity {e.index}: more than one {'Model or Grid' if slot == 'Children' else kind} component")
+                    seen.add(slot)
                 if kind == "Transform":
                     e.local = _transform(c, e.index)
                 elif kind == "Camera":
@@ -272,6 +280,9 @@ def _parse(root):
         if kids is not None:
             if not isinstance(kids, list):
                 raise SceneFileError("Entity 'children' must be a sequence")
+            if e.models or e.children:
+                raise SceneFileError(f"entity {e.index}: a Model or Grid entity cannot also list 'children' "
+                                     "(both would be its Children list)")
             for k in kids:
                 e.children.append(build(k, e))
         return e

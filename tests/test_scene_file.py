@@ -110,9 +110,10 @@ scene:
           translation: [0.0, 0.0, 0.0]
           euler-degrees: [0.0, 30.0, 0.0]
           scale: [1.0, 1.0, 1.0]
-        - type: Model
-          path: Models/Room/scene.obj
       children:
+        - components:
+            - type: Model
+              path: Models/Room/scene.obj
         - components:
             - type: Transform
               translation: [0.25, 0.1, 0.5]
@@ -197,9 +198,13 @@ scene:
             - type: Model
               path: Models/Ball/scene.obj
     - components:
-        - type: Model
-          path: Models/Ball/scene.obj
+        - type: Light
+          color: [1.0, 1.0, 1.0]
+          intensity: 1.0
       children:
+        - components:
+            - type: Model
+              path: Models/Ball/scene.obj
         - components:
             - type: Transform
               translation: [0.0, 3.0, 0.0]
@@ -251,6 +256,12 @@ MODEL = """    - components:
     ("scene:\n" + CAMERA + MODEL.replace("Ball", "Missing"), "not found"),
     ("scripts:\n    - phase: Late\n      name: X\nscene:\n" + CAMERA + MODEL, "Invalid script phase"),
     ("scene: {}\n", "scene root sequence"),
+    ("scene:\n" + CAMERA + MODEL.replace("scale: [1.0, 1.0, 1.0]", "scale: [1.0, 1.0, 1.0]\n        - type: Transform\n"
+                                         "          translation: [0.0, 0.0, 0.0]\n          scale: [1.0, 1.0, 1.0]"),
+     "more than one Transform"),
+    ("scene:\n" + CAMERA + MODEL + "        - type: Model\n          path: Models/Ball/scene.obj\n", "more than one Model or Grid"),
+    ("scene:\n" + CAMERA + MODEL + "      children:\n" + MODEL.replace("    - ", "        - ", 1).replace("\n    ", "\n        "),
+     "cannot also list 'children'"),
 ])
 def test_scene_file_errors(assets, text, message):
     with pytest.raises(sf.SceneFileError, match=message):
