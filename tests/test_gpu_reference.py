@@ -7,7 +7,7 @@ oracle/_ref/ and driven through their launchers (oracle/ref_harness), GPU agains
   hit triangle ids and (u, v, t) bit-exact on 2^20 rays except at exact ties (two triangles at the
   bit-identical t: the reference keeps the first its DFS visits, the product the smaller input
   index; such rays are counted), per-iteration queue counts bit-exact, and every path's radiance
-  within 1e-4 relative at spp = 1.
+  within 1e-4 relative at spp = 1, with constant and with image-textured materials.
 * The oracle's pin: against the reference built with -fmad=false (the oracle's operator-by-operator
   rounding) the oracle's hits are bit-exact except exact ties; its deterministic transcendentals
   differ from CUDA's in the last bits, so its frames agree with the reference's statistically, with
@@ -178,3 +178,27 @@ def test_textured_materials_against_reference_kernels(gpu_renderer, nee):
     assert within >= (0.999 if not nee else 0.995)
     assert np.all(np.abs(a.mean(0) - b.mean(0)) <= 1e-4 * np.abs(b.mean(0)) + 1e-6)
     assert np.all(np.isfinite(a)) and a.mean() > 0
+
+
+@pytest.mark.parametrize("nee", [False, True])
+def test_product_textured_frames_against_reference_build(gpu_renderer_product, nee):
+    """Image textures in every slot, the product build against the reference built with its own
+    flags: identical per-iteration queue counts and every path within 1e-4 relative at spp = 1."""
+    s = scenes.config_scene("cornell-textured")
+    R = ref_harness.RefScene(s, fma=True)
+    decoded = with_materials(s, R.decoded_materials())
+    decoded.textures, decoded.material_textures = s.textures, s.material_textures
+    r = gpu_renderer_product
+    r.upload_scene(decoded)
+    W = H = 192
+    cam = scenes.scene_camera(s, W, H)
+    st = r.render_frame(cam, W, H, 1, 10, nee, pool_size=1 << 20)
+    rr = R.render(cam, W, H, 1, 10, nee)
+    R.close()
+    assert st["iterations"] == rr["iterations"]
+    assert np.array_equal(r.queue_log(), rr["queue_log"][:len(r.queue_log())])
+    a = r.sample_radiance().astype(np.float64)
+    b = rr["accumulation"][:, :3].astype(np.float64)
+    rel = np.abs(a - b) / np.maximum(np.abs(b), 1e-6)
+    assert np.all(rel <= 1e-4), (int(np.sum(np.any(rel > 1e-4, axis=1))), float(rel.max()))
+    assert a.mean() > 0
