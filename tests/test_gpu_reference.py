@@ -79,7 +79,8 @@ def test_product_hits_bit_exact_against_reference_build(gpu_renderer_product, na
     assert ties <= 1e-3 * rays.shape[0]
 
 
-@pytest.mark.parametrize("name,w,h", [("cornell-all", 256, 256), ("spheres-small", 192, 128), ("spheres-1m", 240, 135)])
+@pytest.mark.parametrize("name,w,h", [("cornell-all", 256, 256), ("spheres-small", 192, 128), ("spheres-1m", 240, 135),
+                                      ("spheres-8m", 256, 144)])
 @pytest.mark.parametrize("nee", [False, True])
 def test_product_frames_against_reference_build(gpu_renderer_product, name, w, h, nee):
     """spp = 1 (one path per pixel, so the reference's float-atomic pixel sum is that path's
