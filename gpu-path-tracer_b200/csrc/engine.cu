@@ -654,6 +654,7 @@ namespace pt
         // cleared accumulator); the caller removes it from the waiting list.
         Status admit(JobRecord& J, size_t offset)
         {
+            NvtxRange range("gpt server admit");
             J.arenaOffset = offset;
             J.tableIndex = freeTable_.back();
             freeTable_.pop_back();
@@ -832,6 +833,7 @@ namespace pt
         // Without mu_: waits for the slice launched by launchSlice.
         Status waitSlice()
         {
+            NvtxRange range("gpt server slice");
             if (hostSlice_) PT_TRY(hostLoopSlice());
             PT_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(stream_));
             float ms = 0.0f;

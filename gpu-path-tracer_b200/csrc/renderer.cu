@@ -144,6 +144,7 @@ namespace pt
         if (d.triangle_count == 0 || !d.positions || !d.normals || !d.tangents || !d.uvs || !d.material_ids || !d.materials ||
             d.material_count == 0)
             return Status::Err(GPT_ERR_INVALID_ARGUMENT, "Scene description is incomplete");
+        NvtxRange rangeUpload("gpt scene upload");
         const auto tUpload = std::chrono::steady_clock::now();
         const uint32_t n = d.triangle_count;
         std::vector<uint32_t> models(n);
@@ -197,6 +198,7 @@ namespace pt
         scene->materialCount = d.material_count;
         scene->deviceBvh = deviceBvh;
         const auto tBvh = std::chrono::steady_clock::now();
+        NvtxRange rangeBvh(deviceBvh ? "gpt bvh8 build (device)" : "gpt bvh8 build (host)");
         Bvh8 bvh;
         if (deviceBvh)
         {
@@ -233,6 +235,7 @@ namespace pt
             PT_CUDA("cudaMemcpyAsync", cudaMemcpyAsync(scene->tris.get<void>(), bvh.tris.data(), bvh.tris.size() * sizeof(float4), cudaMemcpyHostToDevice, stream));
         }
         scene->bvhSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - tBvh).count();
+        rangeBvh.end();
         PT_TRY(scene->shading.allocate(static_cast<size_t>(n) * 9 * sizeof(float4)));
         PT_TRY(scene->materials.allocate(static_cast<size_t>(d.material_count) * sizeof(MaterialDev)));
         if (withBinary)
@@ -635,6 +638,7 @@ namespace pt
         Status RenderFrame(const gpt_device_camera& cam, const gpt_render_settings& s, gpt_frame_stats* stats, bool copyToHost = true)
         {
             if (!scene_) return Status::Err(GPT_ERR_NO_SCENE, "No scene has been uploaded");
+            NvtxRange range("gpt render frame");
             PT_CUDA("cudaSetDevice", cudaSetDevice(device_));
             FrameConfig c;
             PT_TRY(resolveConfig(s, c));
@@ -722,6 +726,7 @@ namespace pt
                         uint32_t& tried)
         {
             if (!scene_) return Status::Err(GPT_ERR_NO_SCENE, "No scene has been uploaded");
+            NvtxRange range("gpt autotune");
             gpt_render_settings trial = base;
             trial.max_samples = 0;
             trial.loop_mode = GPT_LOOP_GRAPH;

@@ -2,6 +2,7 @@
 // status values, RAII device buffers, texture objects and device-resident scenes.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <memory>
@@ -38,6 +39,28 @@ namespace pt
         if (!_s.ok()) return _s;          \
     } while (0)
 #define PT_CUDA(op, expr) PT_TRY(CudaStatus(op, (expr)))
+
+    // A named host range on the calling thread's NVTX stack (scene upload and its stages, frames,
+    // the autotuner, job-server slices), so a profiler's timeline shows which host step issued the
+    // kernels under it (ncu: --nvtx --nvtx-include "gpt render frame/"). NVTX is header-only: with
+    // no tool attached a push or pop is one predictable branch. end() closes the range early; the
+    // destructor closes it on every return path otherwise.
+    class NvtxRange
+    {
+    public:
+        explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+        ~NvtxRange() { end(); }
+        NvtxRange(const NvtxRange&) = delete;
+        NvtxRange& operator=(const NvtxRange&) = delete;
+        void end()
+        {
+            if (open_) nvtxRangePop();
+            open_ = false;
+        }
+
+    private:
+        bool open_ = true;
+    };
 
     // True when this device allocation is the one gpt_inject_allocation_failure chose to fail.
     bool InjectedAllocationFailure();
